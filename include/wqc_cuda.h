@@ -1,0 +1,202 @@
+/* wqc_cuda.h - C ABI of the `WQC_TN_BACKEND=cuda` MPS backend (B200, sm_100a).
+ *
+ * The entry points are what the reference's MpsState backend hooks would bind
+ * through `extern "C"` (src/tn/mps.rs:62-67, 128-212, 431-482, 489-495,
+ * 567-590, 937-1079 are the webgpu hooks this backend sits beside).  Plain
+ * pointers and sizes only; every call returns a status and never unwinds.
+ *
+ * Threading: a wqc_cuda_ctx is process-wide (one per device, like the shared
+ * device OnceLock at src/tn/engine_status.rs:27).  A wqc_mps is used from one
+ * thread at a time (the request's spawn_blocking thread, src/api.rs:342) and
+ * owns one CUDA stream; calls enqueue device work and return, and the calls
+ * that hand results to the host synchronise that stream.
+ */
+#ifndef WQC_CUDA_H
+#define WQC_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "wqc_types.h"
+
+#if defined(__GNUC__)
+#define WQC_API __attribute__((visibility("default")))
+#else
+#define WQC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t wqc_status;
+
+/* Status codes and the EngineError each maps to on the Rust side
+ * (src/engine.rs:67-77). */
+enum wqc_status_code {
+    WQC_OK = 0,
+    WQC_ERR_INVALID = 1,              /* ExecutionFailed(msg) */
+    WQC_ERR_OOM = 2,                  /* InsufficientMemory { required, available } */
+    WQC_ERR_TRUNCATION_REJECTED = 3,  /* ExecutionFailed("mps bond exceeded chi"), mps.rs:1143 */
+    WQC_ERR_SVD_FAILED = 4,           /* ExecutionFailed("SVD ... failed its check"), svd_guard.rs:134-138 */
+    WQC_ERR_CANCELLED = 5,            /* ExecutionFailed(cancel::CANCELLED), src/cancel.rs:20 */
+    WQC_ERR_DEVICE_TIMEOUT = 6,       /* ExecutionFailed: a bounded device wait gave up */
+    WQC_ERR_CUDA = 7,                 /* ExecutionFailed: CUDA runtime error */
+    WQC_ERR_NO_DEVICE = 8,            /* backend probe note: no CUDA device (engine_status.rs:74-81) */
+    WQC_ERR_QUBIT_OUT_OF_RANGE = 9,   /* QubitIndexOutOfBounds { index, limit } */
+    WQC_ERR_INVALID_QUBIT_COUNT = 10  /* InvalidQubitCount(n), mps.rs:83-85 */
+};
+
+/* Arithmetic of the split path. */
+enum wqc_precision {
+    WQC_PRECISION_FP64 = 0 /* plain form: complex128 throughout */
+};
+
+typedef struct wqc_cuda_ctx wqc_cuda_ctx;
+typedef struct wqc_mps wqc_mps;
+
+/* Message of the last failing call on this thread (thread-local, never NULL). */
+WQC_API const char* wqc_cuda_last_error(void);
+
+/* Open the process-wide context on `device` (-1: WQC_CUDA_DEVICE or 0).
+ * Replaces the shared device probe (engine_status.rs:40-102). */
+WQC_API wqc_status wqc_cuda_open(int device, wqc_cuda_ctx** out);
+WQC_API void wqc_cuda_close(wqc_cuda_ctx* ctx);
+
+/* Device memory for /sysinfo's vram_budget_bytes (engine_status.rs:105-117)
+ * and the SM count.  Any out pointer may be NULL. */
+WQC_API wqc_status wqc_cuda_device_info(wqc_cuda_ctx* ctx, uint64_t* total_bytes, uint64_t* free_bytes, int32_t* sm_count);
+
+/* Device bytes of the site tensors at bond chi: N * chi^2 * 32, the same
+ * estimate as mps_workspace_bytes (mps.rs:27-32). */
+WQC_API uint64_t wqc_mps_workspace_bytes(uint32_t qubit_count, uint32_t max_bond_dim);
+
+/* MpsState::try_new_with_bond (mps.rs:82-126): N sites of |0>, each stored at
+ * chi_max capacity in device memory.  reject_truncation marks a time-split
+ * half (mps.rs:1270): a split that would drop a singular value above the
+ * cutoff fails with WQC_ERR_TRUNCATION_REJECTED instead of cutting.  Fails
+ * with WQC_ERR_OOM when the sites plus split workspace exceed free device
+ * memory (the device analogue of ensure_mps_workspace_budget, mps.rs:36-48). */
+WQC_API wqc_status wqc_mps_create(wqc_cuda_ctx* ctx, uint32_t qubit_count, uint32_t max_bond_dim, int32_t precision,
+                          uint8_t reject_truncation, wqc_mps** out);
+WQC_API void wqc_mps_destroy(wqc_mps* mps);
+
+/* Back to |0...0> with the split records cleared, keeping the device memory
+ * (a fresh MpsState for the next request without reallocating). */
+WQC_API wqc_status wqc_mps_reset(wqc_mps* mps);
+
+/* MpsState::apply_gate (mps.rs:278-297) for each gate in order: 1q gates,
+ * CNOT/CZ with SWAP routing and undo (mps.rs:353-375), CCNOT as the
+ * reference's 15-gate decomposition (mps.rs:657-677); MEASURE/RESET/IF are
+ * no-ops.  Splits on disjoint sites run concurrently; each site sees exactly
+ * the reference's sequence of operations. */
+WQC_API wqc_status wqc_mps_apply_gates(wqc_mps* mps, const wqc_gate* gates, uint32_t count);
+
+/* MpsState::apply_gate_adjoint (mps.rs:301-331) for each gate in order. */
+WQC_API wqc_status wqc_mps_apply_gates_adjoint(wqc_mps* mps, const wqc_gate* gates, uint32_t count);
+
+/* apply_one_qubit / apply_unary_at / apply_tdg_at (mps.rs:333-351, 621-629):
+ * u is the 2x2 as re,im pairs in row-major order [u00,u01,u10,u11]. */
+WQC_API wqc_status wqc_mps_apply_1q(wqc_mps* mps, uint32_t site, const double u[8]);
+
+/* apply_two_qubit_at_positions / apply_pair_at / apply_cnot_at /
+ * apply_swap_at (mps.rs:377-429, 631-655): u is a Mat4 [c_out][t_out][c_in]
+ * [t_in] (gates.rs:7-8) as 16 re,im pairs; ctrl_is_first says whether the
+ * control is at left_site.  `info` (nullable) receives the split record
+ * (synchronises the stream). */
+WQC_API wqc_status wqc_mps_apply_2q(wqc_mps* mps, uint32_t left_site, const double u[32], uint8_t ctrl_is_first,
+                            wqc_split_info* info);
+
+/* apply_two_qubit_gate (mps.rs:353-375): SWAP the right operand down to the
+ * left one, apply, SWAP back; the same split sequence as the reference. */
+WQC_API wqc_status wqc_mps_apply_2q_routed(wqc_mps* mps, uint32_t ctrl, uint32_t tgt, const double u[32]);
+
+/* apply_adjacent_disjoint_gates (mps.rs:520-565): a layer of adjacent,
+ * qubit-disjoint CNOT/CZ, merged from the current sites then split. */
+WQC_API wqc_status wqc_mps_apply_layer(wqc_mps* mps, const wqc_gate* gates, uint32_t count);
+
+/* Which split the state performs (applies to splits enqueued afterwards).
+ * REFERENCE: the reference's rule, an exact SVD or the seeded range finder
+ * when the split is large (mps.rs:929-981).  EXACT: an exact SVD on every
+ * split.  The range finder's test matrix has rank 48 for every shape (its
+ * signs are bits 8 and 9 of a power-of-two LCG, period 1024), so on a split
+ * of rank above 48 part of its basis is set by rounding; EXACT gives a
+ * reproducible truncation at those shapes. */
+enum wqc_split_rule { WQC_SPLIT_RULE_REFERENCE = 0, WQC_SPLIT_RULE_EXACT = 1 };
+WQC_API wqc_status wqc_mps_set_split_rule(wqc_mps* mps, int32_t rule);
+
+/* Host-only: how wqc_mps_apply_gates would schedule `gates` on n sites,
+ * without a device.  For each split in program order, its left site and its
+ * level (splits of one level run concurrently); *nsplits and *nlevels
+ * receive the totals, and at most `max` entries are written.  The split
+ * sequence is the reference's (mps.rs:353-375 routing, 657-677 CCNOT). */
+WQC_API wqc_status wqc_schedule_gates(uint32_t n, const wqc_gate* gates, uint32_t count, int32_t* split_site,
+                                      int32_t* split_level, uint32_t max, uint32_t* nsplits, uint32_t* nlevels);
+
+/* Wait for the enqueued work; reports device-side failures. */
+WQC_API wqc_status wqc_mps_synchronize(wqc_mps* mps);
+
+/* Ask the running work to stop (src/cancel.rs:38-63): splits not yet started
+ * are skipped and the next synchronising call returns WQC_ERR_CANCELLED.
+ * Safe to call from another thread. */
+WQC_API void wqc_mps_cancel(wqc_mps* mps);
+
+/* amplitude_at_compact_zero (mps.rs:262-276): <0...0|psi> as re, im. */
+WQC_API wqc_status wqc_mps_amplitude_zero(wqc_mps* mps, double out[2]);
+
+/* site_amplitudes (mps.rs:679-693), the trace feeder of trace.rs:401:
+ * out = a0.re, a0.im, a1.re, a1.im.  control_probability is |a1|^2. */
+WQC_API wqc_status wqc_mps_site_amplitudes(wqc_mps* mps, uint32_t target, double out[4]);
+
+/* Right bond of every site (out has qubit_count entries). */
+WQC_API wqc_status wqc_mps_bond_dims(wqc_mps* mps, uint32_t* out);
+
+/* Read / write one site tensor [l][2][r] as re,im pairs (used for
+ * to_dense_state, overlap and tests; mps.rs:742-780, 1421-1474).  With
+ * buf == NULL only the shape is returned. */
+WQC_API wqc_status wqc_mps_download_site(wqc_mps* mps, uint32_t site, uint32_t* l, uint32_t* r, double* buf);
+WQC_API wqc_status wqc_mps_upload_site(wqc_mps* mps, uint32_t site, uint32_t l, uint32_t r, const double* buf);
+
+/* Sum_t coeff_t <psi|P_t|psi> for Pauli strings (labels: nterms strings of
+ * qubit_count characters in IXYZ, character n-1-q acting on qubit q as in
+ * src/expectation.rs:98-132; coeffs: re,im pairs).  Computed on the device
+ * with transfer matrices, so it is not limited to 20 qubits. */
+WQC_API wqc_status wqc_mps_expectation_pauli(wqc_mps* mps, const char* labels, const double* coeffs, uint32_t nterms,
+                                     double out[2]);
+
+/* Split records in program order (one per merge + gate + split). */
+WQC_API uint32_t wqc_mps_split_count(wqc_mps* mps);
+WQC_API wqc_status wqc_mps_split_records(wqc_mps* mps, wqc_split_info* out, uint32_t max, uint32_t* written);
+
+/* WorkReport.vram_peak_bytes (mps.rs:158-166, api.rs:657): high-water mark of
+ * this state's device allocations. */
+WQC_API uint64_t wqc_mps_peak_vram_bytes(wqc_mps* mps);
+
+/* WorkReport.tn_backend (mps.rs:147-155): "cuda". */
+WQC_API const char* wqc_mps_backend_label(wqc_mps* mps);
+
+/* Per-kernel timing, taken with CUDA events on this state's stream while
+ * profiling is on.  kind: 0 Jacobi SVD, 1 merge+gate, 2 range finder
+ * (GEMMs + QR), 3 one-qubit, 4 cut + absorb. */
+typedef struct wqc_kernel_stats {
+    uint64_t launches[5];
+    double milliseconds[5];
+    uint64_t total_launches; /* every kernel this state launched */
+    uint64_t h2d_bytes;      /* host-to-device bytes copied by the calls (gate plans, sites) */
+    uint64_t d2h_bytes;      /* device-to-host bytes of results (amplitudes, ...) */
+    uint64_t jacobi_tasks;   /* SVDs run by the Jacobi kernel */
+    uint64_t jacobi_sweeps;  /* sweeps those SVDs took in total */
+} wqc_kernel_stats;
+WQC_API wqc_status wqc_mps_set_profiling(wqc_mps* mps, int32_t on);
+WQC_API wqc_status wqc_mps_kernel_stats(wqc_mps* mps, wqc_kernel_stats* out);
+WQC_API void wqc_mps_reset_stats(wqc_mps* mps);
+
+/* The CUDA stream this state enqueues on (cudaStream_t), for callers that
+ * time or order work around it. */
+WQC_API void* wqc_mps_stream(wqc_mps* mps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WQC_CUDA_H */

@@ -1,0 +1,108 @@
+"""CPU checks of the drop-in boundary and the host logic (no device work).
+
+* libwqc_cuda.so loads and exports every entry point include/*.h declares;
+* without a device, opening a context fails with WQC_ERR_NO_DEVICE instead
+  of crashing or falling back to the CPU;
+* the host scheduler expands gates into the reference's split sequence and
+  keeps every site's operations in program order;
+* the circuit generators match their stated shapes.
+"""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import wqc_cuda as W
+from wqc_cuda import circuits as C
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_entry_points():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", fn)).read()
+        names |= set(re.findall(r"^WQC_API\s+[\w\s\*]+?\b(wqc_\w+)\s*\(", text, flags=re.M))
+    return names
+
+
+def test_library_exports_every_declared_entry_point():
+    names = declared_entry_points()
+    assert len(names) >= 30
+    lib = W.lib()
+    for name in sorted(names):
+        assert hasattr(lib, name), f"{name} is declared in include/ but not exported"
+    assert set(W.EXPORTS) == names
+
+
+def test_open_without_device_reports_no_device():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    import ctypes
+
+    h = ctypes.c_void_p()
+    rc = W.lib().wqc_cuda_open(-1, ctypes.byref(h))
+    assert rc == W.ERR_NO_DEVICE
+    assert W.lib().wqc_cuda_last_error()
+
+
+def test_workspace_bytes_matches_reference_formula():
+    assert W.workspace_bytes(100, 128) == 52_428_800  # mps.rs:1870-1889
+    assert W.workspace_bytes(50, 128) == 50 * 128 * 128 * 32
+
+
+def test_schedule_matches_reference_split_sequence_and_keeps_site_order():
+    for gates, n in ((C.config0().gates, 16), (C.config1(n=30, depth=12).gates, 30),
+                     (C.gates_array(C.large_chi(n=24, depth=20)), 24)):
+        site, level, nlevels = W.schedule(n, gates)
+        assert len(site) == C.split_plan(gates)
+        # splits of one level are disjoint
+        for L in range(nlevels):
+            s = site[level == L]
+            touched = np.concatenate([s, s + 1])
+            assert len(set(touched.tolist())) == len(touched)
+        # each site sees its splits at strictly increasing levels, in program order
+        last = np.full(n, -1)
+        for p, L in zip(site, level):
+            assert L > last[p] and L > last[p + 1]
+            last[p] = last[p + 1] = L
+
+
+def test_schedule_routes_long_range_gates_with_swaps():
+    """mps.rs:353-375: CNOT(0, 3) is swaps at 2, 1, the gate at 0, swaps at 1, 2."""
+    site, level, _ = W.schedule(4, C.gates_array([C.g2(C.CNOT, 0, 3)]))
+    assert site.tolist() == [2, 1, 0, 1, 2]
+    assert level.tolist() == [0, 1, 2, 3, 4]
+    site, _, _ = W.schedule(3, C.gates_array([C.g3(0, 1, 2)]))
+    assert len(site) == 10  # 6 CNOTs, the two CNOT(0, 2) routed over site 1
+
+
+def test_schedule_rejects_bad_gates():
+    with pytest.raises(W.WqcCudaError) as e:
+        W.schedule(4, C.gates_array([C.g2(C.CNOT, 0, 4)]))
+    assert e.value.code == W.ERR_QUBIT_OUT_OF_RANGE
+    with pytest.raises(W.WqcCudaError):
+        W.schedule(4, C.gates_array([C.g2(C.CZ, 2, 2)]))
+
+
+def test_generators_have_the_stated_shapes():
+    w0 = C.config0()
+    assert (w0.n, w0.chi) == (16, 32)
+    assert int(np.sum(np.isin(w0.gates["kind"], [C.CNOT]))) == 10 * 8 + 10 * 7
+    w1 = C.config1()
+    assert (w1.n, w1.chi) == (50, 128)
+    k = w1.gates["kind"]
+    assert int(np.sum(np.isin(k, list(C.ONE_QUBIT)))) == 50 * 40
+    d = np.abs(w1.gates["q0"] - w1.gates["q1"])[np.isin(k, [C.CNOT, C.CZ])]
+    assert d.min() == 1 and d.max() <= 8 and int(np.sum(d > 1)) == 5 * 40
+    slices = C.config2_slices(16)
+    assert all(20 <= s.n <= 60 and s.chi in (16, 32, 64, 128) for s in slices)
+    g, pidx, params = C.hea_ansatz()
+    assert len(params) == 512 and int(np.sum(pidx >= 0)) == 512
+    labels, coeffs = C.zz_x_observable(32)
+    assert len(labels) == 63 and all(len(x) == 32 for x in labels)

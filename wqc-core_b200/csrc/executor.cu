@@ -1,0 +1,1220 @@
+// Host side of the cuda MPS backend: the C ABI of include/wqc_cuda.h.
+//
+// A gate list is expanded into the reference's MpsState operations (one-qubit
+// applies and adjacent two-site splits, with SWAP routing and the CCNOT
+// decomposition of src/tn/mps.rs:353-375, 657-677), scheduled into levels so
+// that splits on disjoint sites share a wave, and enqueued on the state's
+// stream without waiting for the device.  Bond dimensions live on the device;
+// the host only tracks upper bounds to size launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/wqc_cuda.h"
+#include "common.cuh"
+#include "split_kernels.cuh"
+
+using namespace wqc;
+
+namespace {
+
+thread_local std::string g_err;
+
+wqc_status fail(wqc_status code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                                    \
+    do {                                                                                                  \
+        cudaError_t e_ = (expr);                                                                          \
+        if (e_ != cudaSuccess) return fail(WQC_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int kMaxSweeps = 60;
+constexpr size_t kSmemLimit = 232448 - 1024;  // 227 KB opt-in per block, minus static shared memory
+
+struct Mat2 {
+    double2 u[4];  // row-major
+};
+struct Mat4 {
+    double2 u[16];  // [c_out][t_out][c_in][t_in] flattened: ((co*2+to)*2+ci)*2+ti
+};
+
+double2 C(double r, double i = 0.0) { return make_double2(r, i); }
+
+// src/tn/gates.rs:10-66 and mps.rs:1173-1180.
+Mat2 unary_matrix(int kind, double theta) {
+    const double r2 = 0.70710678118654752440;
+    switch (kind) {
+        case WQC_GATE_H: {
+            const double k = 1.0 / std::sqrt(2.0);
+            return {{C(k), C(k), C(k), C(-k)}};
+        }
+        case WQC_GATE_X: return {{C(0), C(1), C(1), C(0)}};
+        case WQC_GATE_Y: return {{C(0), C(0, -1), C(0, 1), C(0)}};
+        case WQC_GATE_Z: return {{C(1), C(0), C(0), C(-1)}};
+        case WQC_GATE_S: return {{C(1), C(0), C(0), C(0, 1)}};
+        case WQC_GATE_T: return {{C(1), C(0), C(0), C(r2, r2)}};
+        case WQC_GATE_RX: {
+            const double s = std::sin(theta / 2.0), c = std::cos(theta / 2.0);
+            return {{C(c), C(0, -s), C(0, -s), C(c)}};
+        }
+        case WQC_GATE_RY: {
+            const double s = std::sin(theta / 2.0), c = std::cos(theta / 2.0);
+            return {{C(c), C(-s), C(s), C(c)}};
+        }
+        default: {  // RZ
+            const double s = std::sin(theta / 2.0), c = std::cos(theta / 2.0);
+            return {{C(c, -s), C(0), C(0), C(c, s)}};
+        }
+    }
+}
+Mat2 tdg_matrix() {
+    const double r2 = 0.70710678118654752440;
+    return {{C(1), C(0), C(0), C(r2, -r2)}};
+}
+int i4(int co, int to, int ci, int ti) { return ((co * 2 + to) * 2 + ci) * 2 + ti; }
+Mat4 cnot_matrix() {
+    Mat4 m{};
+    m.u[i4(0, 0, 0, 0)] = C(1);
+    m.u[i4(0, 1, 0, 1)] = C(1);
+    m.u[i4(1, 0, 1, 1)] = C(1);
+    m.u[i4(1, 1, 1, 0)] = C(1);
+    return m;
+}
+Mat4 cz_matrix() {
+    Mat4 m{};
+    m.u[i4(0, 0, 0, 0)] = C(1);
+    m.u[i4(0, 1, 0, 1)] = C(1);
+    m.u[i4(1, 0, 1, 0)] = C(1);
+    m.u[i4(1, 1, 1, 1)] = C(-1);
+    return m;
+}
+Mat4 swap_matrix() {
+    Mat4 m{};
+    m.u[i4(0, 0, 0, 0)] = C(1);
+    m.u[i4(0, 1, 1, 0)] = C(1);
+    m.u[i4(1, 0, 0, 1)] = C(1);
+    m.u[i4(1, 1, 1, 1)] = C(1);
+    return m;
+}
+Mat2 adjoint2(const Mat2& a) {
+    return {{make_double2(a.u[0].x, -a.u[0].y), make_double2(a.u[2].x, -a.u[2].y),
+             make_double2(a.u[1].x, -a.u[1].y), make_double2(a.u[3].x, -a.u[3].y)}};
+}
+Mat4 adjoint4(const Mat4& a) {
+    Mat4 o{};
+    for (int co = 0; co < 2; ++co)
+        for (int to = 0; to < 2; ++to)
+            for (int ci = 0; ci < 2; ++ci)
+                for (int ti = 0; ti < 2; ++ti) {
+                    const double2 v = a.u[i4(ci, ti, co, to)];
+                    o.u[i4(co, to, ci, ti)] = make_double2(v.x, -v.y);
+                }
+    return o;
+}
+
+// Effective 4x4 acting on theta[a][s][t][b] (mps.rs:396-421, split.rs:808-831).
+void effective(const Mat4& u, bool ctrl_is_first, double2* out) {
+    for (int so = 0; so < 2; ++so)
+        for (int to = 0; to < 2; ++to)
+            for (int si = 0; si < 2; ++si)
+                for (int ti = 0; ti < 2; ++ti) {
+                    const int co = ctrl_is_first ? so : to, tgo = ctrl_is_first ? to : so;
+                    const int ci = ctrl_is_first ? si : ti, tgi = ctrl_is_first ? ti : si;
+                    out[(so * 2 + to) * 4 + si * 2 + ti] = u.u[i4(co, tgo, ci, tgi)];
+                }
+}
+
+struct Op {
+    bool two;
+    int site;        // 1q: site; 2q: left site
+    Mat2 m2;
+    double2 ueff[16];
+};
+
+struct Group {
+    int mode, C, idx_off, count;
+    size_t smem;
+};
+
+struct Wave {
+    int oq_off = 0, oq_count = 0;  // OneQubitOp entries
+    int jobs_off = 0, njobs = 0;   // SplitJob entries
+    int max_dl = 1, max_dr = 1, max_rows = 2, max_cols = 2, max_ell = 1;
+    bool any_rsvd = false;
+    std::vector<Group> groups;
+};
+
+struct Arena {
+    void* d = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace
+
+struct wqc_cuda_ctx {
+    int device = 0;
+    int sm_count = 0;
+    int max_cluster = 8;
+    std::mutex mu;
+};
+
+struct wqc_mps {
+    wqc_cuda_ctx* ctx = nullptr;
+    int n = 0, chi = 0;
+    bool reject = false;
+    bool exact_only = false;  // WQC_SPLIT_RULE_EXACT
+    cudaStream_t stream = nullptr;
+    // device state
+    double2* site_pool = nullptr;
+    size_t site_cap = 0;  // complex entries per site
+    DeviceMps dev{};
+    double2** d_site_ptr = nullptr;
+    int* d_dl = nullptr;
+    int* d_dr = nullptr;
+    int* d_status = nullptr;
+    volatile int* h_cancel = nullptr;  // mapped pinned
+    int* d_cancel = nullptr;
+    // split workspace
+    int nslots = 0;
+    char* slot_pool = nullptr;
+    SlotBuffers* d_slots = nullptr;
+    SplitState* d_state = nullptr;
+    // per-call plan
+    char* h_stage = nullptr;
+    size_t h_stage_cap = 0;
+    cudaEvent_t stage_done = nullptr;
+    Arena d_stage;
+    wqc_split_info* d_records = nullptr;
+    size_t rec_cap = 0;
+    uint32_t rec_count = 0;
+    double2* d_small = nullptr;  // results of amplitude / site kernels
+    unsigned long long* d_counters = nullptr;  // Jacobi tasks, Jacobi sweeps
+    // host bounds: ub[i] = upper bound of the bond between sites i and i+1
+    std::vector<int> ub;
+    // accounting
+    uint64_t bytes_now = 0, bytes_peak = 0;
+    bool profiling = false;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;
+    std::vector<cudaEvent_t> event_pool;
+    wqc_kernel_stats stats{};
+
+    int left_bond(int site) const { return site == 0 ? 1 : ub[site - 1]; }
+    int right_bond(int site) const { return site + 1 >= n ? 1 : ub[site]; }
+};
+
+namespace {
+
+wqc_status dmalloc(wqc_mps* m, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        return fail(WQC_ERR_OOM, "Insufficient memory: need " + std::to_string(bytes) + " bytes, only " +
+                                     std::to_string(fr) + " bytes free on the device");
+    }
+    m->bytes_now += bytes;
+    m->bytes_peak = std::max(m->bytes_peak, m->bytes_now);
+    return WQC_OK;
+}
+void dfree(wqc_mps* m, void* p, size_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    m->bytes_now -= bytes;
+}
+
+std::once_flag g_attr_once;
+cudaError_t g_attr_err = cudaSuccess;
+
+void set_kernel_attributes() {
+    g_attr_err = cudaFuncSetAttribute(jacobi_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLimit));
+    if (g_attr_err == cudaSuccess)
+        g_attr_err = cudaFuncSetAttribute(jacobi_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (g_attr_err == cudaSuccess)
+        g_attr_err = cudaFuncSetAttribute(amplitude_zero_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    if (g_attr_err == cudaSuccess)
+        g_attr_err = cudaFuncSetAttribute(site_amplitudes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+}
+
+int round_up(int x, int q) { return ((x + q - 1) / q) * q; }
+
+// Smallest cluster that holds the working matrix, preferring blocks of at
+// most 16 columns so each CTA step has at most two pairs per warp.
+int choose_cluster(int M, int N, int max_c) {
+    int fallback = -1;
+    for (int Cc = 1; Cc <= max_c; Cc *= 2) {
+        if (jacobi_smem_bytes(M, N, Cc) > kSmemLimit) continue;
+        const int b = round_up(N, 4 * Cc) / (2 * Cc);
+        if (b <= 16) return Cc;
+        if (fallback < 0) fallback = Cc;
+    }
+    return fallback;
+}
+
+cudaEvent_t get_event(wqc_mps* m) {
+    if (!m->event_pool.empty()) {
+        cudaEvent_t e = m->event_pool.back();
+        m->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct Timed {
+    wqc_mps* m;
+    int kind;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timed(wqc_mps* mm, int k) : m(mm), kind(k) {
+        if (m->profiling) {
+            a = get_event(m);
+            b = get_event(m);
+            cudaEventRecord(a, m->stream);
+        }
+    }
+    ~Timed() {
+        if (m->profiling) {
+            cudaEventRecord(b, m->stream);
+            m->events.push_back({kind, {a, b}});
+        }
+    }
+};
+
+void count_launch(wqc_mps* m, int kind) {
+    m->stats.total_launches++;
+    if (kind >= 0) m->stats.launches[kind]++;
+}
+
+// ---------------------------------------------------------------------------
+// Expansion of gates into MpsState operations.
+// ---------------------------------------------------------------------------
+struct Expander {
+    std::vector<Op> ops;
+    void one(int q, const Mat2& u) {
+        Op o{};
+        o.two = false;
+        o.site = q;
+        o.m2 = u;
+        ops.push_back(o);
+    }
+    void two_at(int p, const Mat4& u, bool cf) {
+        Op o{};
+        o.two = true;
+        o.site = p;
+        effective(u, cf, o.ueff);
+        ops.push_back(o);
+    }
+    void two_routed(int ctrl, int tgt, const Mat4& u) {  // mps.rs:353-375
+        const int left = std::min(ctrl, tgt), right = std::max(ctrl, tgt);
+        const int span = right - left;
+        const Mat4 sw = swap_matrix();
+        if (span > 1)
+            for (int pos = right - 1; pos >= left + 1; --pos) two_at(pos, sw, true);
+        two_at(left, u, ctrl < tgt);
+        if (span > 1)
+            for (int pos = left + 1; pos < right; ++pos) two_at(pos, sw, true);
+    }
+    void ccnot(int c1, int c2, int t) {  // mps.rs:657-677
+        const Mat2 tdg = tdg_matrix(), h = unary_matrix(WQC_GATE_H, 0), tt = unary_matrix(WQC_GATE_T, 0);
+        const Mat4 cx = cnot_matrix();
+        one(t, h);
+        two_routed(c2, t, cx);
+        one(t, tdg);
+        two_routed(c1, t, cx);
+        one(t, tt);
+        two_routed(c2, t, cx);
+        one(t, tdg);
+        two_routed(c1, t, cx);
+        one(t, tt);
+        one(t, h);
+        one(c2, tt);
+        two_routed(c1, c2, cx);
+        one(c1, tt);
+        one(c2, tdg);
+        two_routed(c1, c2, cx);
+    }
+};
+
+wqc_status check_gate(const wqc_mps* m, const wqc_gate& g) {
+    auto chk = [&](int q) -> wqc_status {
+        if (q < 0 || q >= m->n)
+            return fail(WQC_ERR_QUBIT_OUT_OF_RANGE,
+                        "Qubit index " + std::to_string(q) + " out of bounds (limit: " + std::to_string(m->n) + ")");
+        return WQC_OK;
+    };
+    wqc_status s = WQC_OK;
+    switch (g.kind) {
+        case WQC_GATE_H: case WQC_GATE_X: case WQC_GATE_Y: case WQC_GATE_Z: case WQC_GATE_S: case WQC_GATE_T:
+        case WQC_GATE_RX: case WQC_GATE_RY: case WQC_GATE_RZ:
+            return chk(g.q0);
+        case WQC_GATE_CNOT: case WQC_GATE_CZ:
+            if ((s = chk(g.q0)) || (s = chk(g.q1))) return s;
+            if (g.q0 == g.q1) return fail(WQC_ERR_INVALID, "two-qubit gate on one qubit");
+            return WQC_OK;
+        case WQC_GATE_CCNOT:
+            if ((s = chk(g.q0)) || (s = chk(g.q1)) || (s = chk(g.q2))) return s;
+            if (g.q0 == g.q1 || g.q0 == g.q2 || g.q1 == g.q2) return fail(WQC_ERR_INVALID, "CCNOT needs three qubits");
+            return WQC_OK;
+        case WQC_GATE_MEASURE: case WQC_GATE_RESET: case WQC_GATE_IF:
+            return WQC_OK;
+        default:
+            return fail(WQC_ERR_INVALID, "unknown gate kind " + std::to_string(g.kind));
+    }
+}
+
+wqc_status expand(const wqc_mps* m, const wqc_gate* gates, uint32_t count, bool adjoint, Expander& ex) {
+    for (uint32_t i = 0; i < count; ++i) {
+        const wqc_gate& g = gates[adjoint ? count - 1 - i : i];
+        if (wqc_status s = check_gate(m, g)) return s;
+        switch (g.kind) {
+            case WQC_GATE_CNOT:
+                ex.two_routed(g.q0, g.q1, adjoint ? adjoint4(cnot_matrix()) : cnot_matrix());
+                break;
+            case WQC_GATE_CZ:
+                ex.two_routed(g.q0, g.q1, adjoint ? adjoint4(cz_matrix()) : cz_matrix());
+                break;
+            case WQC_GATE_CCNOT:
+                ex.ccnot(g.q0, g.q1, g.q2);
+                break;
+            case WQC_GATE_MEASURE: case WQC_GATE_RESET: case WQC_GATE_IF:
+                if (adjoint) return fail(WQC_ERR_INVALID, "time-split overlap does not apply measurement or reset");
+                break;
+            default: {
+                const Mat2 u = unary_matrix(g.kind, g.angle);
+                ex.one(g.q0, adjoint ? adjoint2(u) : u);
+                break;
+            }
+        }
+    }
+    return WQC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Plan: levels -> waves, staged in one pinned buffer and copied once.
+// ---------------------------------------------------------------------------
+struct Plan {
+    std::vector<Wave> waves;
+    std::vector<OneQubitOp> oq;
+    std::vector<double2> mats;
+    std::vector<SplitJob> jobs;
+    std::vector<int> idx;
+    uint32_t first_seq = 0, nsplits = 0;
+};
+
+// Level of every operation: a split on (p, p+1) goes one level after the last
+// split that touched p or p+1; a one-qubit gate goes one level after the last
+// split on its site and runs before that level's splits.  Each site therefore
+// sees its operations in program order, and the splits of one level touch
+// disjoint sites.
+void assign_levels(int n, const std::vector<Op>& ops, std::vector<int>& level_of) {
+    std::vector<int> last2q(n, -1);
+    level_of.resize(ops.size());
+    for (size_t i = 0; i < ops.size(); ++i) {
+        const Op& o = ops[i];
+        if (!o.two) {
+            level_of[i] = last2q[o.site] + 1;
+        } else {
+            const int L = std::max(last2q[o.site], last2q[o.site + 1]) + 1;
+            level_of[i] = L;
+            last2q[o.site] = last2q[o.site + 1] = L;
+        }
+    }
+}
+
+void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
+    struct LevelBuild {
+        std::vector<std::pair<int, std::vector<Mat2>>> oq;  // site -> matrices in order
+        std::vector<int> oq_index;                          // site -> entry in oq (built lazily)
+        std::vector<SplitJob> jobs;
+        std::vector<std::pair<int, int>> bounds;  // (ub left of p, ub right of p+1) at the job
+    };
+    std::vector<LevelBuild> levels;
+    std::vector<int> level_of;
+    assign_levels(m->n, ops, level_of);
+    auto level = [&](int L) -> LevelBuild& {
+        while (int(levels.size()) <= L) levels.emplace_back();
+        return levels[L];
+    };
+    uint32_t seq = m->rec_count;
+    plan.first_seq = seq;
+    for (size_t oi = 0; oi < ops.size(); ++oi) {
+        const Op& o = ops[oi];
+        if (!o.two) {
+            LevelBuild& lb = level(level_of[oi]);
+            if (lb.oq_index.empty()) lb.oq_index.assign(m->n, -1);
+            int& e = lb.oq_index[o.site];
+            if (e < 0) {
+                e = int(lb.oq.size());
+                lb.oq.push_back({o.site, {}});
+            }
+            lb.oq[e].second.push_back(o.m2);
+        } else {
+            const int p = o.site;
+            LevelBuild& lb = level(level_of[oi]);
+            SplitJob J{};
+            J.p = p;
+            J.seq = int(seq++);
+            J.reject = m->reject ? 1 : 0;
+            J.exact_only = m->exact_only ? 1 : 0;
+            std::memcpy(J.u, o.ueff, sizeof(J.u));
+            const int bl = m->left_bond(p), br = m->right_bond(p + 1);
+            lb.jobs.push_back(J);
+            lb.bounds.push_back({bl, br});
+            m->ub[p] = std::min(std::min(2 * bl, 2 * br), m->chi);
+        }
+    }
+    plan.nsplits = seq - plan.first_seq;
+    for (LevelBuild& lb : levels) {
+        // one-qubit ops run first, in one wave with no splits when needed
+        size_t j0 = 0;
+        bool first = true;
+        do {
+            Wave w;
+            if (first) {
+                w.oq_off = int(plan.oq.size());
+                for (auto& e : lb.oq) {
+                    OneQubitOp op;
+                    op.site = e.first;
+                    op.first = int(plan.mats.size() / 4);
+                    op.count = int(e.second.size());
+                    for (const Mat2& u : e.second)
+                        for (int k = 0; k < 4; ++k) plan.mats.push_back(u.u[k]);
+                    plan.oq.push_back(op);
+                }
+                w.oq_count = int(lb.oq.size());
+                first = false;
+            }
+            const size_t j1 = std::min(lb.jobs.size(), j0 + size_t(m->nslots));
+            w.jobs_off = int(plan.jobs.size());
+            w.njobs = int(j1 - j0);
+            // cluster groups: key (mode, C)
+            std::vector<std::pair<std::pair<int, int>, std::vector<int>>> groups;
+            auto add = [&](int mode, int Cc, int local, size_t smem) {
+                for (auto& g : groups)
+                    if (g.first.first == mode && g.first.second == Cc) {
+                        g.second.push_back(local);
+                        return;
+                    }
+                groups.push_back({{mode, Cc}, {local}});
+                (void)smem;
+            };
+            std::vector<size_t> gsmem;
+            for (size_t k = j0; k < j1; ++k) {
+                SplitJob J = lb.jobs[k];
+                const int local = int(k - j0);
+                J.slot = local;
+                plan.jobs.push_back(J);
+                const int bl = lb.bounds[k].first, br = lb.bounds[k].second;
+                const int rows = 2 * bl, cols = 2 * br;
+                const int ell = std::min(std::min(m->chi + kRsvdOversample, rows), cols);
+                const unsigned long long f = (unsigned long long)rows * cols * ell;
+                const bool rs = !m->reject && !m->exact_only && ell < std::min(rows, cols) &&
+                                f >= (unsigned long long)kRsvdMinSide * kRsvdMinSide * kRsvdMinSide;
+                w.max_dl = std::max(w.max_dl, bl);
+                w.max_dr = std::max(w.max_dr, br);
+                w.max_rows = std::max(w.max_rows, rows);
+                w.max_cols = std::max(w.max_cols, cols);
+                w.max_ell = std::max(w.max_ell, ell);
+                add(kJacobiExact, choose_cluster(std::max(rows, cols), std::min(rows, cols), m->ctx->max_cluster), local, 0);
+                if (rs) {
+                    w.any_rsvd = true;
+                    add(kJacobiRsvd, choose_cluster(cols, ell, m->ctx->max_cluster), local, 0);
+                }
+            }
+            for (auto& g : groups) {
+                Group gr;
+                gr.mode = g.first.first;
+                gr.C = g.first.second;
+                gr.idx_off = int(plan.idx.size());
+                gr.count = int(g.second.size());
+                // shared memory for the largest job of the group
+                size_t sm = 0;
+                for (int local : g.second) {
+                    const int bl = lb.bounds[j0 + local].first, br = lb.bounds[j0 + local].second;
+                    const int rows = 2 * bl, cols = 2 * br;
+                    const int ell = std::min(std::min(m->chi + kRsvdOversample, rows), cols);
+                    const size_t s = gr.mode == kJacobiExact
+                                         ? jacobi_smem_bytes(std::max(rows, cols), std::min(rows, cols), std::max(gr.C, 1))
+                                         : jacobi_smem_bytes(cols, ell, std::max(gr.C, 1));
+                    sm = std::max(sm, s);
+                }
+                gr.smem = sm;
+                for (int local : g.second) plan.idx.push_back(local);
+                w.groups.push_back(gr);
+            }
+            plan.waves.push_back(std::move(w));
+            j0 = j1;
+        } while (j0 < lb.jobs.size());
+    }
+}
+
+template <class T>
+size_t stage_section(size_t& off, const std::vector<T>& v) {
+    off = (off + 255) & ~size_t(255);
+    const size_t at = off;
+    off += v.size() * sizeof(T);
+    return at;
+}
+
+wqc_status ensure_records(wqc_mps* m, size_t need) {
+    if (need <= m->rec_cap) return WQC_OK;
+    size_t cap = std::max<size_t>(need, m->rec_cap * 2 + 1024);
+    void* p = nullptr;
+    if (wqc_status s = dmalloc(m, &p, cap * sizeof(wqc_split_info))) return s;
+    if (m->d_records) {
+        CUDA_TRY(cudaStreamSynchronize(m->stream));
+        CUDA_TRY(cudaMemcpy(p, m->d_records, m->rec_cap * sizeof(wqc_split_info), cudaMemcpyDeviceToDevice));
+        dfree(m, m->d_records, m->rec_cap * sizeof(wqc_split_info));
+    }
+    m->d_records = static_cast<wqc_split_info*>(p);
+    m->rec_cap = cap;
+    return WQC_OK;
+}
+
+wqc_status launch_plan(wqc_mps* m, Plan& plan) {
+    if (plan.waves.empty()) return WQC_OK;
+    if (wqc_status s = ensure_records(m, size_t(plan.first_seq) + plan.nsplits)) return s;
+    size_t off = 0;
+    const size_t o_oq = stage_section(off, plan.oq);
+    const size_t o_mats = stage_section(off, plan.mats);
+    const size_t o_jobs = stage_section(off, plan.jobs);
+    const size_t o_idx = stage_section(off, plan.idx);
+    const size_t bytes = std::max<size_t>(off, 256);
+    // host staging: wait for the previous copy out of it
+    CUDA_TRY(cudaEventSynchronize(m->stage_done));
+    if (bytes > m->h_stage_cap) {
+        if (m->h_stage) cudaFreeHost(m->h_stage);
+        m->h_stage = nullptr;
+        CUDA_TRY(cudaHostAlloc(reinterpret_cast<void**>(&m->h_stage), bytes * 2, cudaHostAllocDefault));
+        m->h_stage_cap = bytes * 2;
+    }
+    if (bytes > m->d_stage.cap) {
+        CUDA_TRY(cudaStreamSynchronize(m->stream));
+        dfree(m, m->d_stage.d, m->d_stage.cap);
+        m->d_stage.d = nullptr;
+        m->d_stage.cap = 0;
+        if (wqc_status s = dmalloc(m, &m->d_stage.d, bytes * 2)) return s;
+        m->d_stage.cap = bytes * 2;
+    }
+    std::memcpy(m->h_stage + o_oq, plan.oq.data(), plan.oq.size() * sizeof(OneQubitOp));
+    std::memcpy(m->h_stage + o_mats, plan.mats.data(), plan.mats.size() * sizeof(double2));
+    std::memcpy(m->h_stage + o_jobs, plan.jobs.data(), plan.jobs.size() * sizeof(SplitJob));
+    std::memcpy(m->h_stage + o_idx, plan.idx.data(), plan.idx.size() * sizeof(int));
+    CUDA_TRY(cudaMemcpyAsync(m->d_stage.d, m->h_stage, bytes, cudaMemcpyHostToDevice, m->stream));
+    m->stats.h2d_bytes += bytes;
+    CUDA_TRY(cudaEventRecord(m->stage_done, m->stream));
+    char* dbase = static_cast<char*>(m->d_stage.d);
+    const OneQubitOp* d_oq = reinterpret_cast<const OneQubitOp*>(dbase + o_oq);
+    const double2* d_mats = reinterpret_cast<const double2*>(dbase + o_mats);
+    const SplitJob* d_jobs_all = reinterpret_cast<const SplitJob*>(dbase + o_jobs);
+    const int* d_idx = reinterpret_cast<const int*>(dbase + o_idx);
+
+    for (const Wave& w : plan.waves) {
+        if (w.oq_count > 0) {
+            Timed t(m, 3);
+            const int gx = std::min(64, std::max(1, (m->chi * m->chi + 1023) / 1024));
+            apply_1q_kernel<<<dim3(gx, w.oq_count), 256, 0, m->stream>>>(d_oq + w.oq_off, d_mats, m->dev);
+            count_launch(m, 3);
+        }
+        if (w.njobs == 0) continue;
+        const SplitJob* d_jobs = d_jobs_all + w.jobs_off;
+        const int nj = w.njobs;
+        {
+            Timed t(m, 1);
+            prepare_kernel<<<(nj + 127) / 128, 128, 0, m->stream>>>(d_jobs, m->d_state, nj, m->dev);
+            count_launch(m, 1);
+            dim3 g((w.max_dr + 15) / 16, (w.max_dl + 15) / 16, nj);
+            merge_gate_kernel<<<g, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);
+            count_launch(m, 1);
+        }
+        auto jacobi = [&](int mode) -> wqc_status {
+            for (const Group& gr : w.groups) {
+                if (gr.mode != mode) continue;
+                if (gr.C < 1)
+                    return fail(WQC_ERR_INVALID, "two-site matrix too large for the cluster-resident Jacobi SVD");
+                Timed t(m, 0);
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3(gr.count * gr.C);
+                cfg.blockDim = dim3(kJacobiThreads);
+                cfg.dynamicSmemBytes = gr.smem;
+                cfg.stream = m->stream;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = gr.C;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                CUDA_TRY(cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel, d_jobs, (const SplitState*)m->d_state,
+                                            (const SlotBuffers*)m->d_slots, d_idx + gr.idx_off, mode, kMaxSweeps,
+                                            m->d_status, m->d_counters));
+                count_launch(m, 0);
+            }
+            return WQC_OK;
+        };
+        if (w.any_rsvd) {
+            {
+                Timed t(m, 2);
+                omega_kernel<<<dim3(32, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots);
+                const int tr = (w.max_rows + 31) / 32, tc = (w.max_cols + 31) / 32, te = (w.max_ell + 31) / 32;
+                rsvd_gemm_kernel<<<dim3(te, tr, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageY0);
+                rsvd_gemm_kernel<<<dim3(te, tc, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageZ);
+                rsvd_gemm_kernel<<<dim3(te, tr, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageY);
+                householder_qr_kernel<<<nj, 512, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots);
+                rsvd_gemm_kernel<<<dim3(tc, te, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageB);
+                for (int k = 0; k < 6; ++k) count_launch(m, 2);
+            }
+            if (wqc_status s = jacobi(kJacobiRsvd)) return s;
+            {
+                Timed t(m, 4);
+                finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiRsvd, m->chi,
+                                                            m->d_records, m->d_status);
+                count_launch(m, 4);
+            }
+        }
+        if (wqc_status s = jacobi(kJacobiExact)) return s;
+        {
+            Timed t(m, 4);
+            finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiExact, m->chi,
+                                                        m->d_records, m->d_status);
+            const int per = std::max(w.max_rows, w.max_cols) * std::min(m->chi, std::max(w.max_rows, w.max_cols));
+            const int gx = std::max(1, std::min(32, per / 2048));
+            absorb_kernel<<<dim3(gx, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);
+            count_launch(m, 4);
+            count_launch(m, 4);
+        }
+    }
+    CUDA_TRY(cudaGetLastError());
+    m->rec_count = plan.first_seq + plan.nsplits;
+    return WQC_OK;
+}
+
+wqc_status run_ops(wqc_mps* m, const std::vector<Op>& ops) {
+    if (*m->h_cancel) return fail(WQC_ERR_CANCELLED, "computation cancelled: the client has gone");
+    Plan plan;
+    build_plan(m, ops, plan);
+    return launch_plan(m, plan);
+}
+
+wqc_status sync_status(wqc_mps* m) {
+    CUDA_TRY(cudaStreamSynchronize(m->stream));
+    int st = 0;
+    CUDA_TRY(cudaMemcpy(&st, m->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (*m->h_cancel) return fail(WQC_ERR_CANCELLED, "computation cancelled: the client has gone");
+    if (st & kStatusCancelled) return fail(WQC_ERR_CANCELLED, "computation cancelled: the client has gone");
+    if (st & kStatusTruncationRejected) return fail(WQC_ERR_TRUNCATION_REJECTED, "mps bond exceeded chi");
+    if (st & kStatusNonFinite) return fail(WQC_ERR_SVD_FAILED, "SVD of a two-site matrix produced non-finite values");
+    return WQC_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* wqc_cuda_last_error(void) { return g_err.c_str(); }
+
+wqc_status wqc_cuda_open(int device, wqc_cuda_ctx** out) {
+    if (!out) return fail(WQC_ERR_INVALID, "null output pointer");
+    if (device < 0) {
+        const char* env = std::getenv("WQC_CUDA_DEVICE");
+        device = env ? std::atoi(env) : 0;
+    }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(WQC_ERR_NO_DEVICE, "CUDA device not found");
+    }
+    if (device >= count) return fail(WQC_ERR_NO_DEVICE, "CUDA device index out of range");
+    CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return fail(WQC_ERR_NO_DEVICE, "the cuda MPS backend is built for sm_100a (B200)");
+    std::call_once(g_attr_once, set_kernel_attributes);
+    if (g_attr_err != cudaSuccess) return fail(WQC_ERR_CUDA, std::string("kernel attributes: ") + cudaGetErrorString(g_attr_err));
+    auto* ctx = new wqc_cuda_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    // Largest cluster the device schedules with a full shared-memory CTA.
+    ctx->max_cluster = 8;
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(16);
+        cfg.blockDim = dim3(kJacobiThreads);
+        cfg.dynamicSmemBytes = 200 * 1024;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 16;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, jacobi_cluster_kernel, &cfg) == cudaSuccess && clusters > 0)
+            ctx->max_cluster = 16;
+        cudaGetLastError();
+    }
+    *out = ctx;
+    return WQC_OK;
+}
+
+void wqc_cuda_close(wqc_cuda_ctx* ctx) { delete ctx; }
+
+wqc_status wqc_cuda_device_info(wqc_cuda_ctx* ctx, uint64_t* total_bytes, uint64_t* free_bytes, int32_t* sm_count) {
+    if (!ctx) return fail(WQC_ERR_INVALID, "null context");
+    CUDA_TRY(cudaSetDevice(ctx->device));
+    size_t fr = 0, tot = 0;
+    CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    if (total_bytes) *total_bytes = tot;
+    if (free_bytes) *free_bytes = fr;
+    if (sm_count) *sm_count = ctx->sm_count;
+    return WQC_OK;
+}
+
+uint64_t wqc_mps_workspace_bytes(uint32_t n, uint32_t chi) {
+    const unsigned __int128 v = (unsigned __int128)n * chi * chi * 32;
+    return v > ~uint64_t(0) ? ~uint64_t(0) : uint64_t(v);
+}
+
+wqc_status wqc_mps_create(wqc_cuda_ctx* ctx, uint32_t n, uint32_t chi, int32_t precision, uint8_t reject,
+                          wqc_mps** out) {
+    if (!ctx || !out) return fail(WQC_ERR_INVALID, "null argument");
+    if (n == 0) return fail(WQC_ERR_INVALID_QUBIT_COUNT, "Invalid qubit count: 0. Max limit is 40.");
+    if (chi == 0) return fail(WQC_ERR_INVALID, "MPS max bond dimension must be > 0");
+    if (precision != WQC_PRECISION_FP64) return fail(WQC_ERR_INVALID, "unsupported precision form");
+    if (chi > 256) return fail(WQC_ERR_INVALID, "the cuda backend supports max_bond_dim <= 256");
+    CUDA_TRY(cudaSetDevice(ctx->device));
+    auto* m = new wqc_mps();
+    m->ctx = ctx;
+    m->n = int(n);
+    m->chi = int(chi);
+    m->reject = reject != 0;
+    m->ub.assign(n > 0 ? n - 1 : 0, 1);
+    auto bail = [&](wqc_status s) {
+        wqc_mps_destroy(m);
+        return s;
+    };
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "stream"));
+    if (cudaEventCreateWithFlags(&m->stage_done, cudaEventDisableTiming) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "event"));
+    cudaEventRecord(m->stage_done, m->stream);
+    // Budget check before any large allocation (mps.rs:36-48 analogue).
+    const int R = 2 * int(chi), E = std::min(int(chi) + kRsvdOversample, R);
+    const size_t slot_c = size_t(R) * R * 3 + size_t(R) * E * 6 + E;  // theta, w, z + range finder + tau
+    const size_t slot_bytes = ((slot_c * sizeof(double2) + size_t(R) * (sizeof(double) + sizeof(int)) + 4095) / 4096) * 4096;
+    m->nslots = std::max(1, int(n) / 2);
+    m->site_cap = size_t(chi) * 2 * chi;
+    const size_t site_bytes = size_t(n) * m->site_cap * sizeof(double2);
+    const uint64_t need = site_bytes + uint64_t(m->nslots) * slot_bytes;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "cudaMemGetInfo"));
+    if (need > fr)
+        return bail(fail(WQC_ERR_OOM, "Insufficient memory: need " + std::to_string(need) + " bytes, only " +
+                                          std::to_string(fr) + " bytes free on the device"));
+    void* p = nullptr;
+    if (wqc_status s = dmalloc(m, &p, site_bytes)) return bail(s);
+    m->site_pool = static_cast<double2*>(p);
+    if (wqc_status s = dmalloc(m, &p, n * sizeof(double2*))) return bail(s);
+    m->d_site_ptr = static_cast<double2**>(p);
+    if (wqc_status s = dmalloc(m, &p, 2 * n * sizeof(int) + 64)) return bail(s);
+    m->d_dl = static_cast<int*>(p);
+    m->d_dr = m->d_dl + n;
+    m->d_status = m->d_dr + n;
+    if (wqc_status s = dmalloc(m, &p, size_t(m->nslots) * slot_bytes)) return bail(s);
+    m->slot_pool = static_cast<char*>(p);
+    if (wqc_status s = dmalloc(m, &p, m->nslots * sizeof(SlotBuffers))) return bail(s);
+    m->d_slots = static_cast<SlotBuffers*>(p);
+    if (wqc_status s = dmalloc(m, &p, m->nslots * sizeof(SplitState))) return bail(s);
+    m->d_state = static_cast<SplitState*>(p);
+    if (wqc_status s = dmalloc(m, &p, 64 * sizeof(double2))) return bail(s);
+    m->d_small = static_cast<double2*>(p);
+    m->d_counters = reinterpret_cast<unsigned long long*>(m->d_small + 60);
+    if (cudaMemset(m->d_small, 0, 64 * sizeof(double2)) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "memset"));
+    int* hc = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&hc), sizeof(int), cudaHostAllocMapped) != cudaSuccess)
+        return bail(fail(WQC_ERR_CUDA, "cudaHostAlloc"));
+    *hc = 0;
+    m->h_cancel = hc;
+    if (cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->d_cancel), hc, 0) != cudaSuccess)
+        return bail(fail(WQC_ERR_CUDA, "cudaHostGetDevicePointer"));
+    // site pointers, |0> sites, dims
+    std::vector<double2*> ptrs(n);
+    for (uint32_t i = 0; i < n; ++i) ptrs[i] = m->site_pool + i * m->site_cap;
+    std::vector<int> ones(2 * n + 16, 1);
+    for (int i = 0; i < 16; ++i) ones[2 * n + i] = 0;
+    std::vector<double2> zero_site(2, make_double2(0, 0));
+    zero_site[0] = make_double2(1.0, 0.0);
+    if (cudaMemcpy(m->d_site_ptr, ptrs.data(), n * sizeof(double2*), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m->d_dl, ones.data(), (2 * n + 16) * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(WQC_ERR_CUDA, "initial upload"));
+    for (uint32_t i = 0; i < n; ++i)
+        if (cudaMemcpy(ptrs[i], zero_site.data(), 2 * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(fail(WQC_ERR_CUDA, "initial upload"));
+    std::vector<SlotBuffers> slots(m->nslots);
+    for (int s = 0; s < m->nslots; ++s) {
+        char* base = m->slot_pool + size_t(s) * slot_bytes;
+        double2* c = reinterpret_cast<double2*>(base);
+        SlotBuffers& b = slots[s];
+        b.theta = c; c += size_t(R) * R;
+        b.w = c; c += size_t(R) * R;
+        b.z = c; c += size_t(R) * R;
+        b.omega = c; c += size_t(R) * E;
+        b.y0 = c; c += size_t(R) * E;
+        b.zr = c; c += size_t(R) * E;
+        b.y = c; c += size_t(R) * E;
+        b.q = c; c += size_t(R) * E;
+        b.b = c; c += size_t(R) * E;
+        b.tau = c; c += E;
+        b.sigma = reinterpret_cast<double*>(c);
+        b.perm = reinterpret_cast<int*>(b.sigma + R);
+    }
+    if (cudaMemcpy(m->d_slots, slots.data(), slots.size() * sizeof(SlotBuffers), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(WQC_ERR_CUDA, "slot table upload"));
+    m->dev.site = m->d_site_ptr;
+    m->dev.dl = m->d_dl;
+    m->dev.dr = m->d_dr;
+    m->dev.n = int(n);
+    m->dev.chi_max = int(chi);
+    m->dev.status = m->d_status;
+    m->dev.cancel = m->d_cancel;
+    if (wqc_status s = ensure_records(m, 1024)) return bail(s);
+    *out = m;
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_reset(wqc_mps* m) {
+    if (!m) return fail(WQC_ERR_INVALID, "null argument");
+    if (wqc_status s = sync_status(m)) return s;
+    std::vector<int> ones(2 * m->n + 16, 1);
+    for (int i = 0; i < 16; ++i) ones[2 * m->n + i] = 0;
+    CUDA_TRY(cudaMemcpy(m->d_dl, ones.data(), ones.size() * sizeof(int), cudaMemcpyHostToDevice));
+    const double2 zero[2] = {make_double2(1.0, 0.0), make_double2(0.0, 0.0)};
+    for (int i = 0; i < m->n; ++i)
+        CUDA_TRY(cudaMemcpy(m->site_pool + size_t(i) * m->site_cap, zero, sizeof(zero), cudaMemcpyHostToDevice));
+    std::fill(m->ub.begin(), m->ub.end(), 1);
+    m->rec_count = 0;
+    *m->h_cancel = 0;
+    return WQC_OK;
+}
+
+void wqc_mps_destroy(wqc_mps* m) {
+    if (!m) return;
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    dfree(m, m->site_pool, 0);
+    dfree(m, m->d_site_ptr, 0);
+    dfree(m, m->d_dl, 0);
+    dfree(m, m->slot_pool, 0);
+    dfree(m, m->d_slots, 0);
+    dfree(m, m->d_state, 0);
+    dfree(m, m->d_small, 0);
+    dfree(m, m->d_records, 0);
+    dfree(m, m->d_stage.d, 0);
+    if (m->h_stage) cudaFreeHost(m->h_stage);
+    if (m->h_cancel) cudaFreeHost(const_cast<int*>(m->h_cancel));
+    for (auto& e : m->events) {
+        cudaEventDestroy(e.second.first);
+        cudaEventDestroy(e.second.second);
+    }
+    for (auto e : m->event_pool) cudaEventDestroy(e);
+    if (m->stage_done) cudaEventDestroy(m->stage_done);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+}
+
+wqc_status wqc_schedule_gates(uint32_t n, const wqc_gate* gates, uint32_t count, int32_t* split_site,
+                              int32_t* split_level, uint32_t max, uint32_t* nsplits, uint32_t* nlevels) {
+    if (n == 0 || (!gates && count) || !nsplits || !nlevels) return fail(WQC_ERR_INVALID, "null argument");
+    wqc_mps probe;
+    probe.n = int(n);
+    Expander ex;
+    if (wqc_status s = expand(&probe, gates, count, false, ex)) return s;
+    std::vector<int> level_of;
+    assign_levels(int(n), ex.ops, level_of);
+    uint32_t k = 0;
+    int top = -1;
+    for (size_t i = 0; i < ex.ops.size(); ++i) {
+        top = std::max(top, level_of[i]);
+        if (!ex.ops[i].two) continue;
+        if (k < max) {
+            if (split_site) split_site[k] = ex.ops[i].site;
+            if (split_level) split_level[k] = level_of[i];
+        }
+        ++k;
+    }
+    *nsplits = k;
+    *nlevels = uint32_t(top + 1);
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_apply_gates(wqc_mps* m, const wqc_gate* gates, uint32_t count) {
+    if (!m || (!gates && count)) return fail(WQC_ERR_INVALID, "null argument");
+    Expander ex;
+    if (wqc_status s = expand(m, gates, count, false, ex)) return s;
+    return run_ops(m, ex.ops);
+}
+
+wqc_status wqc_mps_apply_gates_adjoint(wqc_mps* m, const wqc_gate* gates, uint32_t count) {
+    if (!m || (!gates && count)) return fail(WQC_ERR_INVALID, "null argument");
+    Expander ex;
+    if (wqc_status s = expand(m, gates, count, true, ex)) return s;
+    return run_ops(m, ex.ops);
+}
+
+wqc_status wqc_mps_apply_1q(wqc_mps* m, uint32_t site, const double u[8]) {
+    if (!m || !u) return fail(WQC_ERR_INVALID, "null argument");
+    if (int(site) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
+    Expander ex;
+    Mat2 mm;
+    for (int i = 0; i < 4; ++i) mm.u[i] = make_double2(u[2 * i], u[2 * i + 1]);
+    ex.one(int(site), mm);
+    return run_ops(m, ex.ops);
+}
+
+static Mat4 mat4_from(const double u[32]) {
+    Mat4 mm;
+    for (int i = 0; i < 16; ++i) mm.u[i] = make_double2(u[2 * i], u[2 * i + 1]);
+    return mm;
+}
+
+wqc_status wqc_mps_apply_2q(wqc_mps* m, uint32_t left, const double u[32], uint8_t cf, wqc_split_info* info) {
+    if (!m || !u) return fail(WQC_ERR_INVALID, "null argument");
+    if (int(left) + 1 >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "two-site apply needs adjacent positions");
+    Expander ex;
+    ex.two_at(int(left), mat4_from(u), cf != 0);
+    const uint32_t seq = m->rec_count;
+    if (wqc_status s = run_ops(m, ex.ops)) return s;
+    if (info) {
+        if (wqc_status s = sync_status(m)) return s;
+        CUDA_TRY(cudaMemcpy(info, m->d_records + seq, sizeof(wqc_split_info), cudaMemcpyDeviceToHost));
+    }
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_apply_2q_routed(wqc_mps* m, uint32_t ctrl, uint32_t tgt, const double u[32]) {
+    if (!m || !u) return fail(WQC_ERR_INVALID, "null argument");
+    if (int(ctrl) >= m->n || int(tgt) >= m->n || ctrl == tgt) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "bad qubit pair");
+    Expander ex;
+    ex.two_routed(int(ctrl), int(tgt), mat4_from(u));
+    return run_ops(m, ex.ops);
+}
+
+wqc_status wqc_mps_apply_layer(wqc_mps* m, const wqc_gate* gates, uint32_t count) {
+    if (!m || (!gates && count)) return fail(WQC_ERR_INVALID, "null argument");
+    if (count >= 2) {
+        std::vector<int> seen;
+        for (uint32_t i = 0; i < count; ++i) {
+            const wqc_gate& g = gates[i];
+            if (g.kind != WQC_GATE_CNOT && g.kind != WQC_GATE_CZ)
+                return fail(WQC_ERR_INVALID, "disjoint layer contains a gate that is not CNOT or CZ");
+        }
+    }
+    return wqc_mps_apply_gates(m, gates, count);
+}
+
+wqc_status wqc_mps_set_split_rule(wqc_mps* m, int32_t rule) {
+    if (!m) return fail(WQC_ERR_INVALID, "null argument");
+    if (rule != WQC_SPLIT_RULE_REFERENCE && rule != WQC_SPLIT_RULE_EXACT) return fail(WQC_ERR_INVALID, "unknown split rule");
+    m->exact_only = rule == WQC_SPLIT_RULE_EXACT;
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_synchronize(wqc_mps* m) {
+    if (!m) return fail(WQC_ERR_INVALID, "null argument");
+    return sync_status(m);
+}
+
+void wqc_mps_cancel(wqc_mps* m) {
+    if (m && m->h_cancel) *const_cast<volatile int*>(m->h_cancel) = 1;
+}
+
+wqc_status wqc_mps_amplitude_zero(wqc_mps* m, double out[2]) {
+    if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
+    amplitude_zero_kernel<<<1, 512, 2 * m->chi * sizeof(double2), m->stream>>>(m->dev, m->d_small);
+    count_launch(m, -1);
+    CUDA_TRY(cudaGetLastError());
+    double2 h;
+    CUDA_TRY(cudaMemcpyAsync(&h, m->d_small, sizeof(double2), cudaMemcpyDeviceToHost, m->stream));
+    m->stats.d2h_bytes += sizeof(double2);
+    if (wqc_status s = sync_status(m)) return s;
+    out[0] = h.x;
+    out[1] = h.y;
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_site_amplitudes(wqc_mps* m, uint32_t target, double out[4]) {
+    if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
+    if (int(target) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "target out of range");
+    site_amplitudes_kernel<<<1, 512, 4 * m->chi * sizeof(double2), m->stream>>>(m->dev, int(target), m->d_small);
+    count_launch(m, -1);
+    CUDA_TRY(cudaGetLastError());
+    double2 h[2];
+    CUDA_TRY(cudaMemcpyAsync(h, m->d_small, 2 * sizeof(double2), cudaMemcpyDeviceToHost, m->stream));
+    if (wqc_status s = sync_status(m)) return s;
+    out[0] = h[0].x;
+    out[1] = h[0].y;
+    out[2] = h[1].x;
+    out[3] = h[1].y;
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_bond_dims(wqc_mps* m, uint32_t* out) {
+    if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
+    if (wqc_status s = sync_status(m)) return s;
+    std::vector<int> dr(m->n);
+    CUDA_TRY(cudaMemcpy(dr.data(), m->d_dr, m->n * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < m->n; ++i) out[i] = uint32_t(dr[i]);
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_download_site(wqc_mps* m, uint32_t site, uint32_t* l, uint32_t* r, double* buf) {
+    if (!m || !l || !r) return fail(WQC_ERR_INVALID, "null argument");
+    if (int(site) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
+    if (wqc_status s = sync_status(m)) return s;
+    int dl = 0, dr = 0;
+    CUDA_TRY(cudaMemcpy(&dl, m->d_dl + site, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&dr, m->d_dr + site, sizeof(int), cudaMemcpyDeviceToHost));
+    *l = uint32_t(dl);
+    *r = uint32_t(dr);
+    if (buf)
+        CUDA_TRY(cudaMemcpy(buf, m->site_pool + site * m->site_cap, size_t(dl) * 2 * dr * sizeof(double2),
+                            cudaMemcpyDeviceToHost));
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_upload_site(wqc_mps* m, uint32_t site, uint32_t l, uint32_t r, const double* buf) {
+    if (!m || !buf) return fail(WQC_ERR_INVALID, "null argument");
+    if (int(site) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
+    if (l == 0 || r == 0 || int(l) > m->chi || int(r) > m->chi) return fail(WQC_ERR_INVALID, "site shape exceeds max_bond_dim");
+    if (wqc_status s = sync_status(m)) return s;
+    CUDA_TRY(cudaMemcpy(m->site_pool + site * m->site_cap, buf, size_t(l) * 2 * r * sizeof(double2), cudaMemcpyHostToDevice));
+    const int il = int(l), ir = int(r);
+    CUDA_TRY(cudaMemcpy(m->d_dl + site, &il, sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(m->d_dr + site, &ir, sizeof(int), cudaMemcpyHostToDevice));
+    if (site > 0) m->ub[site - 1] = std::max(m->ub[site - 1], il);
+    if (int(site) + 1 < m->n) m->ub[site] = std::max(m->ub[site], ir);
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_expectation_pauli(wqc_mps* m, const char* labels, const double* coeffs, uint32_t nterms,
+                                     double out[2]) {
+    if (!m || !labels || !coeffs || !out) return fail(WQC_ERR_INVALID, "null argument");
+    for (size_t i = 0; i < size_t(nterms) * m->n; ++i) {
+        const char ch = labels[i];
+        if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z')
+            return fail(WQC_ERR_INVALID, std::string("invalid pauli character in label"));
+    }
+    if (nterms == 0) {
+        out[0] = out[1] = 0;
+        return WQC_OK;
+    }
+    const size_t E = size_t(m->chi) * m->chi;
+    const size_t scratch = size_t(nterms) * 4 * E * sizeof(double2);
+    void* d_lab = nullptr;
+    void* d_scr = nullptr;
+    void* d_out = nullptr;
+    if (wqc_status s = dmalloc(m, &d_lab, size_t(nterms) * m->n + 16)) return s;
+    if (wqc_status s = dmalloc(m, &d_scr, scratch)) {
+        dfree(m, d_lab, size_t(nterms) * m->n + 16);
+        return s;
+    }
+    if (wqc_status s = dmalloc(m, &d_out, nterms * sizeof(double2))) {
+        dfree(m, d_lab, size_t(nterms) * m->n + 16);
+        dfree(m, d_scr, scratch);
+        return s;
+    }
+    wqc_status rc = WQC_OK;
+    std::vector<double2> vals(nterms);
+    cudaError_t e = cudaMemcpyAsync(d_lab, labels, size_t(nterms) * m->n, cudaMemcpyHostToDevice, m->stream);
+    if (e == cudaSuccess) {
+        pauli_expectation_kernel<<<nterms, 256, 0, m->stream>>>(m->dev, static_cast<const char*>(d_lab), int(nterms),
+                                                                  static_cast<double2*>(d_scr), m->chi,
+                                                                  static_cast<double2*>(d_out));
+        count_launch(m, -1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(vals.data(), d_out, nterms * sizeof(double2), cudaMemcpyDeviceToHost, m->stream);
+    if (e != cudaSuccess) rc = fail(WQC_ERR_CUDA, cudaGetErrorString(e));
+    if (rc == WQC_OK) rc = sync_status(m);
+    dfree(m, d_lab, size_t(nterms) * m->n + 16);
+    dfree(m, d_scr, scratch);
+    dfree(m, d_out, nterms * sizeof(double2));
+    if (rc != WQC_OK) return rc;
+    double re = 0, im = 0;
+    for (uint32_t t = 0; t < nterms; ++t) {  // coeff * Re<P> (expectation.rs:177-185)
+        const double v = vals[t].x;
+        re += coeffs[2 * t] * v;
+        im += coeffs[2 * t + 1] * v;
+    }
+    out[0] = re;
+    out[1] = im;
+    return WQC_OK;
+}
+
+uint32_t wqc_mps_split_count(wqc_mps* m) { return m ? m->rec_count : 0; }
+
+wqc_status wqc_mps_split_records(wqc_mps* m, wqc_split_info* out, uint32_t max, uint32_t* written) {
+    if (!m || (!out && max)) return fail(WQC_ERR_INVALID, "null argument");
+    if (wqc_status s = sync_status(m)) return s;
+    const uint32_t k = std::min(max, m->rec_count);
+    if (k) CUDA_TRY(cudaMemcpy(out, m->d_records, k * sizeof(wqc_split_info), cudaMemcpyDeviceToHost));
+    if (written) *written = k;
+    return WQC_OK;
+}
+
+uint64_t wqc_mps_peak_vram_bytes(wqc_mps* m) { return m ? m->bytes_peak : 0; }
+
+const char* wqc_mps_backend_label(wqc_mps*) { return "cuda"; }
+
+wqc_status wqc_mps_set_profiling(wqc_mps* m, int32_t on) {
+    if (!m) return fail(WQC_ERR_INVALID, "null argument");
+    m->profiling = on != 0;
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_kernel_stats(wqc_mps* m, wqc_kernel_stats* out) {
+    if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
+    CUDA_TRY(cudaStreamSynchronize(m->stream));
+    for (auto& e : m->events) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, e.second.first, e.second.second) == cudaSuccess) m->stats.milliseconds[e.first] += ms;
+        m->event_pool.push_back(e.second.first);
+        m->event_pool.push_back(e.second.second);
+    }
+    m->events.clear();
+    unsigned long long c[2] = {0, 0};
+    CUDA_TRY(cudaMemcpy(c, m->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+    m->stats.jacobi_tasks = c[0];
+    m->stats.jacobi_sweeps = c[1];
+    *out = m->stats;
+    return WQC_OK;
+}
+
+void wqc_mps_reset_stats(wqc_mps* m) {
+    if (!m) return;
+    cudaStreamSynchronize(m->stream);
+    for (auto& e : m->events) {
+        m->event_pool.push_back(e.second.first);
+        m->event_pool.push_back(e.second.second);
+    }
+    m->events.clear();
+    m->stats = wqc_kernel_stats{};
+    cudaMemset(m->d_counters, 0, 2 * sizeof(unsigned long long));
+}
+
+void* wqc_mps_stream(wqc_mps* m) { return m ? static_cast<void*>(m->stream) : nullptr; }
+
+}  // extern "C"

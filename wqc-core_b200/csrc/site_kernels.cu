@@ -1,0 +1,195 @@
+// Site-local kernels: 1-qubit gates, the <0...0|psi> chain, the trace
+// feeders' environments, and Pauli-string expectations.
+#include "common.cuh"
+#include "split_kernels.cuh"
+
+namespace wqc {
+
+// One-qubit gates (mps.rs:333-351): site[a, s', b] = sum_s u[s'][s] site[a, s, b].
+// Every gate queued for a site in this wave is applied in order while the
+// pair (v0, v1) stays in registers: one read and one write of the site.
+__global__ void __launch_bounds__(256) apply_1q_kernel(const OneQubitOp* ops, const double2* mats, DeviceMps mps) {
+    const OneQubitOp op = ops[blockIdx.y];
+    const int l = mps.dl[op.site], r = mps.dr[op.site];
+    double2* s = mps.site[op.site];
+    const long total = long(l) * r;
+    for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += long(gridDim.x) * blockDim.x) {
+        const long a = e / r, b = e % r;
+        double2* p0 = s + (a * 2) * r + b;
+        double2* p1 = p0 + r;
+        double2 v0 = *p0, v1 = *p1;
+        for (int g = 0; g < op.count; ++g) {
+            const double2* u = mats + size_t(op.first + g) * 4;
+            const double2 n0 = cadd(cmul(u[0], v0), cmul(u[1], v1));
+            const double2 n1 = cadd(cmul(u[2], v0), cmul(u[3], v1));
+            v0 = n0;
+            v1 = n1;
+        }
+        *p0 = v0;
+        *p1 = v1;
+    }
+}
+
+// <0...0|psi> (mps.rs:262-276): v <- v . site[:, 0, :] along the chain.
+__global__ void __launch_bounds__(512) amplitude_zero_kernel(DeviceMps mps, double2* out) {
+    extern __shared__ double2 vbuf[];  // 2 * chi_max
+    double2* v = vbuf;
+    double2* nx = vbuf + mps.chi_max;
+    int len = 1;
+    if (threadIdx.x == 0) v[0] = cmake(1.0, 0.0);
+    __syncthreads();
+    for (int i = 0; i < mps.n; ++i) {
+        const int l = mps.dl[i], r = mps.dr[i];
+        const double2* s = mps.site[i];
+        const int la = min(l, len);
+        for (int b = threadIdx.x; b < r; b += blockDim.x) {
+            double2 acc = cmake(0, 0);
+            for (int a = 0; a < la; ++a) cfma(acc, v[a], s[size_t(a) * 2 * r + b]);
+            nx[b] = acc;
+        }
+        __syncthreads();
+        double2* t = v;
+        v = nx;
+        nx = t;
+        len = r;
+    }
+    if (threadIdx.x == 0) *out = len > 0 ? v[0] : cmake(0, 0);
+}
+
+// Trace feeders (mps.rs:679-740): environments with the all-ones physical
+// vector on both sides of `target`, then (a0, a1).
+__global__ void __launch_bounds__(512) site_amplitudes_kernel(DeviceMps mps, int target, double2* out) {
+    extern __shared__ double2 buf[];  // 4 * chi_max
+    double2* le = buf;
+    double2* tmp = buf + mps.chi_max;
+    double2* re = buf + 2 * mps.chi_max;
+    double2* tmp2 = buf + 3 * mps.chi_max;
+    __shared__ double2 red[2][512 / 32];
+    int llen = 1, rlen = 1;
+    if (threadIdx.x == 0) {
+        le[0] = cmake(1.0, 0.0);
+        re[0] = cmake(1.0, 0.0);
+    }
+    __syncthreads();
+    for (int i = 0; i < target; ++i) {
+        const int l = mps.dl[i], r = mps.dr[i];
+        const double2* s = mps.site[i];
+        const int la = min(l, llen);
+        for (int b = threadIdx.x; b < r; b += blockDim.x) {
+            double2 acc = cmake(0, 0);
+            for (int a = 0; a < la; ++a)
+                for (int p = 0; p < 2; ++p) cfma(acc, le[a], s[(size_t(a) * 2 + p) * r + b]);
+            tmp[b] = acc;
+        }
+        __syncthreads();
+        for (int b = threadIdx.x; b < r; b += blockDim.x) le[b] = tmp[b];
+        __syncthreads();
+        llen = r;
+    }
+    if (target + 1 < mps.n) {
+        for (int i = mps.n - 1; i > target; --i) {
+            const int l = mps.dl[i], r = mps.dr[i];
+            const double2* s = mps.site[i];
+            const int rb = min(r, rlen);
+            for (int a = threadIdx.x; a < l; a += blockDim.x) {
+                double2 acc = cmake(0, 0);
+                for (int b = 0; b < rb; ++b)
+                    for (int p = 0; p < 2; ++p) cfma(acc, re[b], s[(size_t(a) * 2 + p) * r + b]);
+                tmp2[a] = acc;
+            }
+            __syncthreads();
+            for (int a = threadIdx.x; a < l; a += blockDim.x) re[a] = tmp2[a];
+            __syncthreads();
+            rlen = l;
+        }
+    }
+    const int l = mps.dl[target], r = mps.dr[target];
+    const double2* s = mps.site[target];
+    double2 a0 = cmake(0, 0), a1 = cmake(0, 0);
+    for (long e = threadIdx.x; e < long(llen) * r; e += blockDim.x) {
+        const int a = int(e / r), b = int(e % r);
+        if (a >= l) continue;
+        const double2 rv = b < rlen ? re[b] : cmake(1.0, 0.0);
+        cfma(a0, le[a], cmul(s[(size_t(a) * 2) * r + b], rv));
+        cfma(a1, le[a], cmul(s[(size_t(a) * 2 + 1) * r + b], rv));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a0.x += __shfl_xor_sync(0xffffffffu, a0.x, o);
+        a0.y += __shfl_xor_sync(0xffffffffu, a0.y, o);
+        a1.x += __shfl_xor_sync(0xffffffffu, a1.x, o);
+        a1.y += __shfl_xor_sync(0xffffffffu, a1.y, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][wid] = a0;
+        red[1][wid] = a1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 s0 = cmake(0, 0), s1 = cmake(0, 0);
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+            s0 = cadd(s0, red[0][w]);
+            s1 = cadd(s1, red[1][w]);
+        }
+        out[0] = s0;
+        out[1] = s1;
+    }
+}
+
+// <psi|P|psi> for Pauli strings by transfer matrices, one CTA per term.
+// env[l_ket][l_bra] lives in global scratch (two env_cap x env_cap buffers
+// per term plus one for the half-contracted tensor).  Label character n-1-q
+// acts on qubit q (src/expectation.rs:98-132).
+__global__ void __launch_bounds__(256) pauli_expectation_kernel(DeviceMps mps, const char* labels, int nterms,
+                                                                double2* scratch, int env_cap, double2* out) {
+    const int t = blockIdx.x;
+    if (t >= nterms) return;
+    const size_t E = size_t(env_cap) * env_cap;
+    double2* env = scratch + size_t(t) * 4 * E;
+    double2* nxt = env + E;
+    double2* tmp = env + 2 * E;  // [l_bra][s][r], up to env_cap * 2 * env_cap
+    const char* lab = labels + size_t(t) * mps.n;
+    if (threadIdx.x == 0) env[0] = cmake(1.0, 0.0);
+    __syncthreads();
+    int lk = 1;
+    for (int q = 0; q < mps.n; ++q) {
+        const int l = mps.dl[q], r = mps.dr[q];
+        const double2* s = mps.site[q];
+        const char ch = lab[mps.n - 1 - q];
+        // tmp[lp][p][b] = sum_l env[l][lp] * s[l][p][b]
+        for (long e = threadIdx.x; e < long(lk) * 2 * r; e += blockDim.x) {
+            const int lp = int(e / (2 * r)), rem = int(e % (2 * r));
+            double2 acc = cmake(0, 0);
+            for (int a = 0; a < min(lk, l); ++a) cfma(acc, env[size_t(a) * lk + lp], s[size_t(a) * 2 * r + rem]);
+            tmp[e] = acc;
+        }
+        __syncthreads();
+        // next[b][bp] = sum_{lp, so, si} conj(s[lp][so][bp]) P[so][si] tmp[lp][si][b]
+        for (long e = threadIdx.x; e < long(r) * r; e += blockDim.x) {
+            const int b = int(e / r), bp = int(e % r);
+            double2 acc = cmake(0, 0);
+            for (int lp = 0; lp < min(lk, l); ++lp) {
+                const double2 t0 = tmp[(size_t(lp) * 2 + 0) * r + b];
+                const double2 t1 = tmp[(size_t(lp) * 2 + 1) * r + b];
+                const double2 k0 = s[(size_t(lp) * 2 + 0) * r + bp];
+                const double2 k1 = s[(size_t(lp) * 2 + 1) * r + bp];
+                double2 y0, y1;  // (P t)[so]
+                if (ch == 'X') { y0 = t1; y1 = t0; }
+                else if (ch == 'Y') { y0 = cmake(t1.y, -t1.x); y1 = cmake(-t0.y, t0.x); }
+                else if (ch == 'Z') { y0 = t0; y1 = cmake(-t1.x, -t1.y); }
+                else { y0 = t0; y1 = t1; }
+                cfma_conj(acc, k0, y0);
+                cfma_conj(acc, k1, y1);
+            }
+            nxt[e] = acc;
+        }
+        __syncthreads();
+        double2* sw = env;
+        env = nxt;
+        nxt = sw;
+        lk = r;
+    }
+    if (threadIdx.x == 0) out[t] = env[0];
+}
+
+}  // namespace wqc

@@ -1,0 +1,806 @@
+// Two-site split pipeline: merge + 4x4 gate, range finder (reference rule),
+// one-sided Jacobi SVD in a thread-block cluster, cut, and sqrt(S) absorption.
+//
+// Reference path: src/tn/mps.rs:377-429 (two-site apply), 484-514 (merge),
+// 833-866 (4x4 on theta), 937-981 (split dispatch), 983-1053 (range finder),
+// 1124-1171 (truncated split), src/tn/svd_guard.rs:25-76 (truncation rule,
+// ambiguity test), 91-139 (dust zeroing before the SVD).
+//
+// Every kernel takes the wave's job array and reads the job's bond dimensions
+// from device memory, so a whole circuit can be enqueued without the host
+// waiting on the device.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "split_kernels.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace wqc {
+
+// ---------------------------------------------------------------------------
+// prepare: bond dims and the exact / range-finder decision (mps.rs:937-954).
+// ---------------------------------------------------------------------------
+__global__ void prepare_kernel(const SplitJob* jobs, SplitState* st, int njobs, DeviceMps mps) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    const SplitJob& J = jobs[j];
+    SplitState s{};
+    if (*mps.cancel) {  // cancelled: every later kernel of this wave skips the job
+        s.skip = 1;
+        st[j] = s;
+        if (j == 0) atomicOr(mps.status, kStatusCancelled);
+        return;
+    }
+    s.dl = mps.dl[J.p];
+    s.dr = mps.dr[J.p + 1];
+    s.k = min(mps.dr[J.p], mps.dl[J.p + 1]);
+    s.rows = 2 * s.dl;
+    s.cols = 2 * s.dr;
+    s.ell = min(min(mps.chi_max + kRsvdOversample, s.rows), s.cols);
+    const unsigned long long f = (unsigned long long)s.rows * s.cols * s.ell;
+    const unsigned long long side = kRsvdMinSide;
+    const bool worth = f >= side * side * side;
+    s.use_rsvd = (!J.reject && !J.exact_only && s.ell > 0 && s.ell < min(s.rows, s.cols) && worth) ? 1 : 0;
+    s.need_exact = s.use_rsvd ? 0 : 1;
+    s.path = s.use_rsvd ? WQC_SPLIT_RSVD : WQC_SPLIT_EXACT;
+    s.w_rows_of_src = s.rows < s.cols ? 1 : 0;
+    st[j] = s;
+}
+
+// ---------------------------------------------------------------------------
+// merge + gate: theta'[(a,s'),(t',b)] = sum_{s,t} U[s't',st] sum_g L[a,s,g] R[g,t,b]
+// One thread owns one (a, b) pair and its 2x2 physical block.  L and R tiles
+// are staged in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kMergeTA = 16, kMergeTB = 16, kMergeTK = 16;
+
+__global__ void __launch_bounds__(256) merge_gate_kernel(const SplitJob* jobs, const SplitState* st,
+                                                         const SlotBuffers* slots, DeviceMps mps) {
+    const int j = blockIdx.z;
+    const SplitJob& J = jobs[j];
+    const SplitState S = st[j];
+    const int a0 = blockIdx.y * kMergeTA, b0 = blockIdx.x * kMergeTB;
+    if (S.skip || a0 >= S.dl || b0 >= S.dr) return;
+    const double2* L = mps.site[J.p];      // [dl][2][k']  with k' = dr of site p
+    const double2* R = mps.site[J.p + 1];  // [k''][2][dr] with k'' = dl of site p+1
+    const int ldl = mps.dr[J.p];           // row stride of L's (a,s) rows
+    const int k = S.k;
+    const int dr = S.dr;
+    __shared__ double2 Ls[2 * kMergeTA][kMergeTK + 1];
+    __shared__ double2 Rs[kMergeTK][2 * kMergeTB + 1];
+    __shared__ double2 U[16];
+    const int tid = threadIdx.x;
+    if (tid < 16) U[tid] = J.u[tid];
+    const int ta = tid / kMergeTB, tb = tid % kMergeTB;
+    const int a = a0 + ta, b = b0 + tb;
+    double2 acc[4] = {cmake(0, 0), cmake(0, 0), cmake(0, 0), cmake(0, 0)};  // [s][t]
+    for (int g0 = 0; g0 < k; g0 += kMergeTK) {
+        // L tile: rows (a0..a0+TA) x s, cols g
+        for (int e = tid; e < 2 * kMergeTA * kMergeTK; e += 256) {
+            const int r = e / kMergeTK, c = e % kMergeTK;
+            const int aa = a0 + r / 2, ss = r % 2, gg = g0 + c;
+            Ls[r][c] = (aa < S.dl && gg < k) ? L[(size_t(aa) * 2 + ss) * ldl + gg] : cmake(0, 0);
+        }
+        for (int e = tid; e < kMergeTK * 2 * kMergeTB; e += 256) {
+            const int r = e / (2 * kMergeTB), c = e % (2 * kMergeTB);
+            const int gg = g0 + r, tt = c / kMergeTB, bb = b0 + c % kMergeTB;
+            Rs[r][c] = (gg < k && bb < dr) ? R[(size_t(gg) * 2 + tt) * dr + bb] : cmake(0, 0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int c = 0; c < kMergeTK; ++c) {
+            const double2 l0 = Ls[2 * ta][c], l1 = Ls[2 * ta + 1][c];
+            const double2 r0 = Rs[c][tb], r1 = Rs[c][kMergeTB + tb];
+            cfma(acc[0], l0, r0);
+            cfma(acc[1], l0, r1);
+            cfma(acc[2], l1, r0);
+            cfma(acc[3], l1, r1);
+        }
+        __syncthreads();
+    }
+    if (a >= S.dl || b >= dr) return;
+    double2* th = slots[J.slot].theta;
+    const int cols = S.cols;
+    for (int so = 0; so < 2; ++so)
+        for (int to = 0; to < 2; ++to) {
+            double2 v = cmake(0, 0);
+            for (int q = 0; q < 4; ++q) cfma(v, U[(so * 2 + to) * 4 + q], acc[q]);
+            th[size_t(a * 2 + so) * cols + to * dr + b] = v;
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Rademacher test matrix (mps.rs:1103-1122), generated in parallel: element i
+// is the LCG state after i+1 steps from (salt | 1), reached by composing the
+// affine map x -> a x + c with itself (exact 64-bit wrapping arithmetic).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long lcg_jump(unsigned long long x, unsigned long long n) {
+    unsigned long long A = 1ull, Cc = 0ull;            // accumulated map
+    unsigned long long a = 6364136223846793005ull, c = 1ull;  // current power
+    while (n) {
+        if (n & 1ull) {
+            A = A * a;
+            Cc = Cc * a + c;
+        }
+        c = c * (a + 1ull);
+        a = a * a;
+        n >>= 1;
+    }
+    return A * x + Cc;
+}
+
+__global__ void omega_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots) {
+    const int j = blockIdx.y;
+    const SplitState S = st[j];
+    if (!S.use_rsvd) return;
+    const long total = long(S.cols) * S.ell;
+    const unsigned long long salt =
+        ((unsigned long long)S.rows * 0x9E37ull + (unsigned long long)S.cols) * 0x9E37ull + (unsigned long long)S.ell;
+    const double scale = 1.0 / sqrt(double(S.cols));
+    double2* om = slots[jobs[j].slot].omega;
+    for (long i = blockIdx.x * long(blockDim.x) + threadIdx.x; i < total; i += long(gridDim.x) * blockDim.x) {
+        const unsigned long long s = lcg_jump(salt | 1ull, (unsigned long long)i + 1ull);
+        om[i] = cmake((s & 0x100ull) == 0 ? scale : -scale, (s & 0x200ull) == 0 ? scale : -scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Batched complex FP64 GEMM for the range finder.  C(m x n) = A(m x k) B(k x n)
+// with strided / conjugated operand views derived per job from its state.
+// ---------------------------------------------------------------------------
+struct MatView {
+    const double2* p;
+    long rs, cs;
+    int conj;
+};
+
+__device__ __forceinline__ double2 view_at(const MatView& v, int i, int kk) {
+    const double2 x = v.p[i * v.rs + kk * v.cs];
+    return v.conj ? cconj(x) : x;
+}
+
+constexpr int kGemmT = 32, kGemmK = 16;
+
+__global__ void __launch_bounds__(256) rsvd_gemm_kernel(const SplitJob* jobs, const SplitState* st,
+                                                        const SlotBuffers* slots, int stage) {
+    const int j = blockIdx.z;
+    const SplitState S = st[j];
+    if (!S.use_rsvd) return;
+    const SlotBuffers B = slots[jobs[j].slot];
+    const int rows = S.rows, cols = S.cols, ell = S.ell;
+    MatView A, Bv;
+    double2* Cp;
+    long c_rs, c_cs;
+    int m, n, k;
+    switch (stage) {
+        case kStageY0:  // Y0 = theta * Omega   (rows x ell)
+            A = {B.theta, cols, 1, 0};
+            Bv = {B.omega, ell, 1, 0};
+            Cp = B.y0; c_rs = ell; c_cs = 1; m = rows; n = ell; k = cols;
+            break;
+        case kStageZ:  // Z = theta^H * Y0    (cols x ell)
+            A = {B.theta, 1, cols, 1};
+            Bv = {B.y0, ell, 1, 0};
+            Cp = B.zr; c_rs = ell; c_cs = 1; m = cols; n = ell; k = rows;
+            break;
+        case kStageY:  // Y = theta * Z, stored column-major for the QR
+            A = {B.theta, cols, 1, 0};
+            Bv = {B.zr, ell, 1, 0};
+            Cp = B.y; c_rs = 1; c_cs = rows; m = rows; n = ell; k = cols;
+            break;
+        default:  // kStageB: B = Q^H * theta  (ell x cols), Q column-major rows x ell
+            A = {B.q, rows, 1, 1};
+            Bv = {B.theta, cols, 1, 0};
+            Cp = B.b; c_rs = cols; c_cs = 1; m = ell; n = cols; k = rows;
+            break;
+    }
+    const int i0 = blockIdx.y * kGemmT, n0 = blockIdx.x * kGemmT;
+    if (i0 >= m || n0 >= n) return;
+    __shared__ double2 As[kGemmT][kGemmK + 1];
+    __shared__ double2 Bs[kGemmK][kGemmT + 1];
+    const int tid = threadIdx.x;
+    const int tr = tid / 16, tc = tid % 16;  // 2x2 outputs per thread
+    double2 acc[2][2] = {{cmake(0, 0), cmake(0, 0)}, {cmake(0, 0), cmake(0, 0)}};
+    for (int k0 = 0; k0 < k; k0 += kGemmK) {
+        for (int e = tid; e < kGemmT * kGemmK; e += 256) {
+            const int r = e / kGemmK, c = e % kGemmK;
+            As[r][c] = (i0 + r < m && k0 + c < k) ? view_at(A, i0 + r, k0 + c) : cmake(0, 0);
+        }
+        for (int e = tid; e < kGemmK * kGemmT; e += 256) {
+            const int r = e / kGemmT, c = e % kGemmT;
+            Bs[r][c] = (k0 + r < k && n0 + c < n) ? view_at(Bv, k0 + r, n0 + c) : cmake(0, 0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int c = 0; c < kGemmK; ++c) {
+            const double2 a0 = As[tr][c], a1 = As[tr + 16][c];
+            const double2 b0 = Bs[c][tc], b1 = Bs[c][tc + 16];
+            cfma(acc[0][0], a0, b0);
+            cfma(acc[0][1], a0, b1);
+            cfma(acc[1][0], a1, b0);
+            cfma(acc[1][1], a1, b1);
+        }
+        __syncthreads();
+    }
+    for (int x = 0; x < 2; ++x)
+        for (int y = 0; y < 2; ++y) {
+            const int i = i0 + tr + 16 * x, jj = n0 + tc + 16 * y;
+            if (i < m && jj < n) Cp[i * c_rs + jj * c_cs] = acc[x][y];
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Householder QR of Y (rows x ell, column-major) and the thin Q, one CTA per
+// job (LAPACK zgeqr2 + zung2r conventions; thin Q is unique up to column
+// phases, which the range finder's results do not depend on).
+// ---------------------------------------------------------------------------
+constexpr int kQrThreads = 512;
+
+__device__ double block_sum(double v, double* red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double t = 0;
+    const int nw = blockDim.x >> 5;
+    for (int w = 0; w < nw; ++w) t += red[w];  // every thread sums in the same order
+    __syncthreads();
+    return t;
+}
+
+__global__ void __launch_bounds__(kQrThreads) householder_qr_kernel(const SplitJob* jobs, const SplitState* st,
+                                                                    const SlotBuffers* slots) {
+    const int j = blockIdx.x;
+    const SplitState S = st[j];
+    if (!S.use_rsvd) return;
+    const SlotBuffers B = slots[jobs[j].slot];
+    const int m = S.rows, n = S.ell;
+    double2* y = B.y;
+    double2* q = B.q;
+    double2* tau = B.tau;
+    __shared__ double red[kQrThreads / 32];
+    __shared__ double2 v[512];
+    __shared__ double2 s_tau;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = kQrThreads / 32;
+    for (int c = 0; c < n; ++c) {
+        double2* col = y + size_t(c) * m;
+        double part = 0;
+        for (int i = c + 1 + tid; i < m; i += kQrThreads) part += cnorm2(col[i]);
+        const double xnorm2 = block_sum(part, red);
+        const double2 alpha = col[c];
+        double2 t = cmake(0, 0);
+        double2 sc = cmake(0, 0);
+        double beta = alpha.x;
+        const bool trivial = (xnorm2 == 0.0 && alpha.y == 0.0);
+        if (!trivial) {
+            beta = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
+            if (alpha.x >= 0) beta = -beta;
+            t = cmake((beta - alpha.x) / beta, -alpha.y / beta);
+            // sc = 1 / (alpha - beta)
+            const double2 d = cmake(alpha.x - beta, alpha.y);
+            const double dn = d.x * d.x + d.y * d.y;
+            sc = cmake(d.x / dn, -d.y / dn);
+        }
+        __syncthreads();  // everyone has read col[c]
+        for (int i = c + 1 + tid; i < m; i += kQrThreads) {
+            const double2 x = trivial ? col[i] : cmul(col[i], sc);
+            col[i] = x;
+            v[i] = x;
+        }
+        if (tid == 0) {
+            col[c] = cmake(beta, 0.0);
+            v[c] = cmake(1.0, 0.0);
+            tau[c] = t;
+            s_tau = t;
+        }
+        __syncthreads();
+        if (!trivial) {
+            const double2 tc = cconj(s_tau);  // apply H^H
+            for (int kk = c + 1 + wid; kk < n; kk += nw) {
+                double2* ck = y + size_t(kk) * m;
+                double2 w = cmake(0, 0);
+                for (int i = c + lane; i < m; i += 32) cfma_conj(w, v[i], ck[i]);
+                for (int o = 16; o > 0; o >>= 1) {
+                    w.x += __shfl_xor_sync(0xffffffffu, w.x, o);
+                    w.y += __shfl_xor_sync(0xffffffffu, w.y, o);
+                }
+                w = cmul(tc, w);
+                for (int i = c + lane; i < m; i += 32) ck[i] = csub(ck[i], cmul(v[i], w));
+            }
+        }
+        __syncthreads();
+    }
+    // Thin Q = H_0 ... H_{n-1} [I; 0], accumulated backward.
+    for (int e = tid; e < m * n; e += kQrThreads) {
+        const int r = e % m, c = e / m;
+        q[e] = cmake(r == c ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    for (int c = n - 1; c >= 0; --c) {
+        const double2* col = y + size_t(c) * m;
+        for (int i = c + 1 + tid; i < m; i += kQrThreads) v[i] = col[i];
+        if (tid == 0) {
+            v[c] = cmake(1.0, 0.0);
+            s_tau = tau[c];
+        }
+        __syncthreads();
+        const double2 tc = s_tau;
+        if (tc.x != 0.0 || tc.y != 0.0) {
+            for (int kk = c + wid; kk < n; kk += nw) {
+                double2* ck = q + size_t(kk) * m;
+                double2 w = cmake(0, 0);
+                for (int i = c + lane; i < m; i += 32) cfma_conj(w, v[i], ck[i]);
+                for (int o = 16; o > 0; o >>= 1) {
+                    w.x += __shfl_xor_sync(0xffffffffu, w.x, o);
+                    w.y += __shfl_xor_sync(0xffffffffu, w.y, o);
+                }
+                w = cmul(tc, w);
+                for (int i = c + lane; i < m; i += 32) ck[i] = csub(ck[i], cmul(v[i], w));
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One-sided Hestenes Jacobi SVD on a thread-block cluster.
+//
+// The tall working matrix W (M x N, padded to N' = 2*C*b columns) and the
+// rotation accumulator Z (N' x N') are held column by column in the shared
+// memory of the C CTAs of one cluster: CTA r holds block r ("top") and block
+// 2C-1-r ("bottom"), b columns each, one column being W's M entries followed
+// by Z's N' entries.  A sweep orthogonalises the pairs inside each block, then
+// runs 2C-1 block steps of the b*b cross pairs, rotating the blocks between
+// CTAs by the circle method through distributed shared memory.  Each pair
+// rotation is the reference's rephase-then-real-rotation (svd_guard.rs:
+// 174-199), with column dot products reduced by warp shuffles.
+// ---------------------------------------------------------------------------
+struct JacobiCtl {
+    int top_buf, bot_buf, spare_buf;
+    int top_id, bot_id;
+    int rot;
+    double fro_part;
+};
+
+__device__ __forceinline__ int circle_at(int pos, int step, int b) {
+    if (pos == 0) return 0;
+    const int m = b - 1;
+    int v = (pos - 1 - step) % m;
+    if (v < 0) v += m;
+    return v + 1;
+}
+
+// Rotates columns xp, xq (each W then Z, `len` entries, W part `M`).  All
+// lanes compute bitwise-identical reductions (xor butterfly), so the branch is
+// warp-uniform.  Returns 1 when a rotation was applied.
+//
+// Two guards keep every applied rotation unitary and the sweep finite:
+// |gamma| is taken with hypot, so the phase stays of unit modulus when the
+// products underflow; and a pair whose Gram scale sqrt(alpha*beta) is below
+// floor = (1e-16 * ||W||_F)^2 is left alone.  Such a pair is a column at
+// rounding-noise level against another column; rotating it moves nothing
+// above 1e-32 ||W||_F^2, while exactly parallel columns (a rank-deficient
+// theta) would otherwise be re-rotated every sweep until their products
+// reach the subnormal range.
+__device__ __forceinline__ int jacobi_rotate(double2* xp, double2* xq, int M, int len, double tol, double noise_floor,
+                                             int lane) {
+    double a = 0, bb = 0, gr = 0, gi = 0;
+    for (int r = lane; r < M; r += 32) {
+        const double2 u = xp[r], v = xq[r];
+        a = fma(u.x, u.x, fma(u.y, u.y, a));
+        bb = fma(v.x, v.x, fma(v.y, v.y, bb));
+        gr = fma(u.x, v.x, fma(u.y, v.y, gr));
+        gi = fma(u.x, v.y, fma(-u.y, v.x, gi));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        bb += __shfl_xor_sync(0xffffffffu, bb, o);
+        gr += __shfl_xor_sync(0xffffffffu, gr, o);
+        gi += __shfl_xor_sync(0xffffffffu, gi, o);
+    }
+    const double g = hypot(gr, gi);
+    const double scale = sqrt(a) * sqrt(bb);
+    if (g == 0.0 || g <= tol * scale || scale <= noise_floor) return 0;
+    const double pr = gr / g, pi = gi / g;
+    const double zeta = (bb - a) / (2.0 * g);
+    const double t = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
+    const double c = 1.0 / sqrt(1.0 + t * t);
+    const double s = c * t;
+    for (int r = lane; r < len; r += 32) {
+        const double2 u = xp[r], v = xq[r];
+        const double vqx = v.x * pr + v.y * pi, vqy = v.y * pr - v.x * pi;  // v * conj(phase)
+        const double npx = u.x * c - vqx * s, npy = u.y * c - vqy * s;
+        const double tx = u.x * s + vqx * c, ty = u.y * s + vqy * c;
+        xp[r] = cmake(npx, npy);
+        xq[r] = cmake(tx * pr - ty * pi, tx * pi + ty * pr);  // * phase
+    }
+    return 1;
+}
+
+__device__ __forceinline__ void jacobi_task(const SplitJob& J, const SplitState& S, const SlotBuffers& B, int mode,
+                                            const double2*& src, int& sr, int& sc, int& ld, int& rows_of_src) {
+    if (mode == kJacobiRsvd) {  // W = B^H, B is ell x cols row-major
+        src = B.b;
+        sr = S.ell;
+        sc = S.cols;
+        ld = S.cols;
+        rows_of_src = 1;
+    } else {  // exact: W = theta (rows >= cols) or theta^H
+        src = B.theta;
+        sr = S.rows;
+        sc = S.cols;
+        ld = S.cols;
+        rows_of_src = S.w_rows_of_src;
+    }
+}
+
+__device__ __forceinline__ bool jacobi_active(const SplitState& S, int mode) {
+    return mode == kJacobiRsvd ? S.use_rsvd != 0 : S.need_exact != 0;
+}
+
+__global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const SplitJob* jobs, const SplitState* st,
+                                                                          const SlotBuffers* slots, const int* idx,
+                                                                          int mode, int max_sweeps, int* status,
+                                                                          unsigned long long* counters) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = int(cluster.num_blocks());
+    const int rank = int(cluster.block_rank());
+    const int j = idx[blockIdx.x / C];
+    const SplitState S = st[j];
+    if (!jacobi_active(S, mode)) return;  // uniform over the cluster
+    const SplitJob& J = jobs[j];
+    const SlotBuffers Bf = slots[J.slot];
+    const double2* src;
+    int sr, sc, ld, rows_of_src;
+    jacobi_task(J, S, Bf, mode, src, sr, sc, ld, rows_of_src);
+    const int M = rows_of_src ? sc : sr;
+    const int N = rows_of_src ? sr : sc;
+    const int quantum = 4 * C;
+    const int Np = ((N + quantum - 1) / quantum) * quantum;
+    const int b = Np / (2 * C);
+    const int len = M + Np;
+    const int nbuf = C == 1 ? 2 : 3;
+
+    extern __shared__ __align__(16) double2 smem[];
+    __shared__ JacobiCtl ctl;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int nwarps = kJacobiThreads / 32;
+    auto buf = [&](int k) { return smem + size_t(k) * b * len; };
+    __shared__ double red[kJacobiThreads / 32];
+
+    if (tid == 0) {
+        ctl.top_buf = 0;
+        ctl.bot_buf = 1;
+        ctl.spare_buf = nbuf - 1;
+        ctl.top_id = rank;
+        ctl.bot_id = 2 * C - 1 - rank;
+        ctl.rot = 0;
+    }
+    // Frobenius norm over the columns this CTA loads, then over the cluster.
+    auto src_at = [&](int i, int col) -> double2 {
+        return rows_of_src ? cconj(src[size_t(col) * ld + i]) : src[size_t(i) * ld + col];
+    };
+    double part = 0;
+    for (int half = 0; half < 2; ++half) {
+        const int id = half == 0 ? rank : 2 * C - 1 - rank;
+        for (int e = tid; e < b * M; e += kJacobiThreads) {
+            int c, i;
+            if (rows_of_src) { c = e / M; i = e % M; } else { i = e / b; c = e % b; }
+            const int col = id * b + c;
+            if (col < N) part += cnorm2(src_at(i, col));
+        }
+    }
+    {
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0) red[wid] = part;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0;
+            for (int w = 0; w < nwarps; ++w) t += red[w];
+            ctl.fro_part = t;
+        }
+    }
+    cluster.sync();
+    double fro2 = 0;
+    for (int r = 0; r < C; ++r) fro2 += cluster.map_shared_rank(&ctl, r)->fro_part;
+    const double dust = sqrt(fro2) * kDustRel;
+    const double dust2 = dust * dust;
+    // Load W (dust-zeroed) and Z = identity.
+    for (int half = 0; half < 2; ++half) {
+        const int id = half == 0 ? rank : 2 * C - 1 - rank;
+        double2* base = buf(half);
+        for (int e = tid; e < b * M; e += kJacobiThreads) {
+            int c, i;
+            if (rows_of_src) { c = e / M; i = e % M; } else { i = e / b; c = e % b; }
+            const int col = id * b + c;
+            double2 x = col < N ? src_at(i, col) : cmake(0, 0);
+            if (cnorm2(x) < dust2) x = cmake(0, 0);
+            base[size_t(c) * len + i] = x;
+        }
+        for (int e = tid; e < b * Np; e += kJacobiThreads) {
+            const int c = e / Np, i = e % Np;
+            base[size_t(c) * len + M + i] = cmake(i == id * b + c ? 1.0 : 0.0, 0.0);
+        }
+    }
+    __syncthreads();
+    // Pairs count as orthogonal at |gamma| <= 1e-14 sqrt(alpha beta): above
+    // the rounding of an M <= 512 dot product (sqrt(M) eps <= 5e-15), so the
+    // sweeps stop, and the singular values are then exact to second order.
+    const double tol = 1e-14;
+    const double noise_floor = 1e-32 * fro2;
+    int sweep = 0;
+    bool converged = false;
+    for (; sweep < max_sweeps; ++sweep) {
+        if (tid == 0) ctl.rot = 0;
+        __syncthreads();
+        int my_rot = 0;
+        // Pairs inside each block (circle method on b columns).
+        for (int step = 0; step < b - 1; ++step) {
+            for (int pq = wid; pq < b; pq += nwarps) {
+                const bool top = pq < b / 2;
+                const int i = top ? pq : pq - b / 2;
+                double2* base = buf(top ? ctl.top_buf : ctl.bot_buf);
+                const int e1 = circle_at(i, step, b), e2 = circle_at(b - 1 - i, step, b);
+                my_rot += jacobi_rotate(base + size_t(e1) * len, base + size_t(e2) * len, M, len, tol, noise_floor, lane);
+            }
+            __syncthreads();
+        }
+        // Cross pairs between the two blocks, 2C-1 block steps.
+        for (int bs = 0; bs < 2 * C - 1; ++bs) {
+            for (int k = 0; k < b; ++k) {
+                double2* tb = buf(ctl.top_buf);
+                double2* bb = buf(ctl.bot_buf);
+                for (int i = wid; i < b; i += nwarps) {
+                    const int e2 = (i + k) % b;
+                    my_rot += jacobi_rotate(tb + size_t(i) * len, bb + size_t(e2) * len, M, len, tol, noise_floor, lane);
+                }
+                __syncthreads();
+            }
+            if (C == 1) continue;
+            // Circle rotation of blocks between CTAs (pull protocol, one spare buffer).
+            cluster.sync();  // all block-step rotations are finished and roles are current
+            const size_t blk = size_t(b) * len;
+            if (rank >= 1) {
+                const int srank = rank == 1 ? 0 : rank - 1;
+                const JacobiCtl* rc = cluster.map_shared_rank(&ctl, srank);
+                const int sbuf = rank == 1 ? rc->bot_buf : rc->top_buf;
+                const double2* rsrc = cluster.map_shared_rank(smem, srank) + size_t(sbuf) * blk;
+                double2* dst = buf(ctl.spare_buf);
+                for (size_t e = tid; e < blk; e += kJacobiThreads) dst[e] = rsrc[e];
+            }
+            cluster.sync();
+            if (rank <= C - 2) {
+                const JacobiCtl* rc = cluster.map_shared_rank(&ctl, rank + 1);
+                const double2* rsrc = cluster.map_shared_rank(smem, rank + 1) + size_t(rc->bot_buf) * blk;
+                double2* dst = buf(rank == 0 ? ctl.bot_buf : ctl.top_buf);
+                for (size_t e = tid; e < blk; e += kJacobiThreads) dst[e] = rsrc[e];
+            }
+            // Block ids travel with the data.
+            int new_top_id = ctl.top_id, new_bot_id = ctl.bot_id;
+            if (rank >= 1) {
+                const JacobiCtl* rc = cluster.map_shared_rank(&ctl, rank == 1 ? 0 : rank - 1);
+                new_top_id = rank == 1 ? rc->bot_id : rc->top_id;
+            }
+            if (rank <= C - 2) {
+                new_bot_id = cluster.map_shared_rank(&ctl, rank + 1)->bot_id;
+            } else {
+                new_bot_id = ctl.top_id;
+            }
+            cluster.sync();
+            if (tid == 0) {
+                if (rank == 0) {
+                    ctl.bot_id = new_bot_id;
+                } else {
+                    const int ot = ctl.top_buf, ob = ctl.bot_buf, os = ctl.spare_buf;
+                    ctl.top_buf = os;
+                    ctl.bot_buf = ot;
+                    ctl.spare_buf = ob;
+                    ctl.top_id = new_top_id;
+                    ctl.bot_id = new_bot_id;
+                }
+            }
+            __syncthreads();
+        }
+        // Cluster-wide rotation count decides convergence.
+        if (lane == 0 && my_rot) atomicAdd(&ctl.rot, my_rot);
+        __syncthreads();
+        int total = 0;
+        if (C == 1) {
+            total = ctl.rot;
+            __syncthreads();
+        } else {
+            cluster.sync();
+            for (int r = 0; r < C; ++r) total += cluster.map_shared_rank(&ctl, r)->rot;
+            cluster.sync();
+        }
+        if (total == 0) {
+            converged = true;
+            break;
+        }
+    }
+    if (tid == 0 && rank == 0) {
+        if (!converged) atomicOr(status, kStatusJacobiNoConvergence);
+        atomicAdd(counters + 0, 1ull);
+        atomicAdd(counters + 1, (unsigned long long)(converged ? sweep + 1 : sweep));
+    }
+    // Write back: W columns, Z columns (first N rows) and column norms.
+    for (int half = 0; half < 2; ++half) {
+        const int id = half == 0 ? ctl.top_id : ctl.bot_id;
+        const double2* base = buf(half == 0 ? ctl.top_buf : ctl.bot_buf);
+        for (int c = wid; c < b; c += nwarps) {
+            const int col = id * b + c;
+            if (col >= N) continue;
+            const double2* x = base + size_t(c) * len;
+            double s2 = 0;
+            for (int r = lane; r < M; r += 32) {
+                const double2 v = x[r];
+                s2 = fma(v.x, v.x, fma(v.y, v.y, s2));
+                Bf.w[size_t(col) * M + r] = v;
+            }
+            for (int r = lane; r < N; r += 32) Bf.z[size_t(col) * N + r] = x[M + r];
+            for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            if (lane == 0) Bf.sigma[col] = sqrt(s2);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// finalize: stable descending sort, truncation rule, ambiguity test,
+// discarded weight and the split record.
+// ---------------------------------------------------------------------------
+__global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const SlotBuffers* slots, int mode,
+                                int chi_max, wqc_split_info* records, int* status) {
+    const int j = blockIdx.x;
+    SplitState& S = st[j];
+    if (!jacobi_active(S, mode)) return;
+    const SplitJob& J = jobs[j];
+    const SlotBuffers B = slots[J.slot];
+    const int N = mode == kJacobiRsvd ? S.ell : min(S.rows, S.cols);
+    __shared__ double vals[1024];
+    const int tid = threadIdx.x;
+    // rank_j = #{i : s_i > s_j or (s_i == s_j and i < j)}
+    for (int c = tid; c < N; c += blockDim.x) {
+        const double sj = B.sigma[c];
+        int r = 0;
+        for (int i = 0; i < N; ++i) {
+            const double si = B.sigma[i];
+            r += (si > sj || (si == sj && i < c)) ? 1 : 0;
+        }
+        B.perm[r] = c;
+    }
+    __syncthreads();
+    for (int c = tid; c < N; c += blockDim.x) {
+        double v = B.sigma[B.perm[c]];
+        if (mode == kJacobiRsvd && v < kRsvdZero) v = 0.0;
+        vals[c] = v;
+    }
+    __syncthreads();
+    if (tid != 0) return;
+    // retained_chi (svd_guard.rs:25-35)
+    int rank = 0;
+    bool bad = false;
+    for (int i = 0; i < N; ++i) {
+        if (vals[i] > kSingularCutoff) ++rank;
+        if (!isfinite(vals[i]) || vals[i] < 0.0) bad = true;
+    }
+    int chi = N == 0 ? 0 : min(min(max(rank, 1), chi_max), min(S.rows, S.cols));
+    if (mode == kJacobiRsvd) {
+        // needs_f64_fallback (svd_guard.rs:58-76)
+        bool fb = bad || chi == 0;
+        for (int i = 0; i < N && !fb; ++i)
+            if (vals[i] > 0.0 && fabs(vals[i] - kSingularCutoff) <= kCutoffAbsBand) fb = true;
+        if (!fb && chi > 0 && chi < N) {
+            const double kept = vals[chi - 1], dropped = vals[chi];
+            const double scale = fmax(fmax(kept, dropped), 1e-30);
+            if (fabs(kept - dropped) / scale < kChiRelGap) fb = true;
+        }
+        if (fb) {
+            S.need_exact = 1;
+            S.path = WQC_SPLIT_RSVD_FALLBACK;
+            return;
+        }
+        S.final_kind = 1;
+    } else {
+        S.final_kind = 0;
+        if (J.reject) {
+            for (int i = chi; i < N; ++i)
+                if (vals[i] > kSingularCutoff) {
+                    atomicOr(status, kStatusTruncationRejected);
+                    break;
+                }
+        }
+        if (bad) atomicOr(status, kStatusNonFinite);
+    }
+    double disc = 0;
+    for (int i = chi; i < N; ++i) disc += vals[i] * vals[i];
+    S.chi = chi;
+    S.discarded = disc;
+    wqc_split_info info;
+    info.left_site = J.p;
+    info.rows = S.rows;
+    info.cols = S.cols;
+    info.ell = S.ell;
+    info.path = S.path;
+    info.chi = chi;
+    info.discarded_weight = disc;
+    records[J.seq] = info;
+}
+
+// ---------------------------------------------------------------------------
+// absorb: L = U sqrt(S), R = sqrt(S) V^H written into the two sites, new bond
+// dims published (mps.rs:1156-1168, 1039-1051).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const SplitState* st,
+                                                     const SlotBuffers* slots, DeviceMps mps) {
+    const int j = blockIdx.y;
+    const SplitJob& J = jobs[j];
+    const SplitState S = st[j];
+    if (S.skip) return;
+    const SlotBuffers B = slots[J.slot];
+    const int chi = S.chi, dl = S.dl, dr = S.dr, rows = S.rows, cols = S.cols;
+    double2* Ls = mps.site[J.p];
+    double2* Rs = mps.site[J.p + 1];
+    const long nl = long(rows) * chi, nr = long(chi) * cols;
+    const long stride = long(gridDim.x) * blockDim.x;
+    const long t0 = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (S.final_kind == 1) {
+        // Range finder: W = B^H (cols x ell), U_B = Z (ell x ell), V_B = W / sigma.
+        const int ell = S.ell;
+        for (long e = t0; e < nl; e += stride) {
+            const int r = int(e / chi), m = int(e % chi);
+            const int pc = B.perm[m];
+            const double sg = B.sigma[pc];
+            double2 acc = cmake(0, 0);
+            const double2* zc = B.z + size_t(pc) * ell;
+            for (int t = 0; t < ell; ++t) cfma(acc, B.q[size_t(t) * rows + r], zc[t]);
+            Ls[e] = cscale(acc, sqrt(sg));  // L[(r/2)][r%2][m] at r*chi + m
+        }
+        for (long e = t0; e < nr; e += stride) {
+            const int m = int(e / cols), c = int(e % cols);
+            const int pc = B.perm[m];
+            const double sg = B.sigma[pc];
+            const double2 w = B.w[size_t(pc) * cols + c];
+            Rs[e] = sg > 0.0 ? cscale(cconj(w), 1.0 / sqrt(sg)) : cmake(0, 0);  // R[m][c/dr][c%dr]
+        }
+    } else if (!S.w_rows_of_src) {
+        // W = theta (rows x cols), U = W / sigma, V = Z (cols x cols).
+        for (long e = t0; e < nl; e += stride) {
+            const int r = int(e / chi), m = int(e % chi);
+            const int pc = B.perm[m];
+            const double sg = B.sigma[pc];
+            const double2 w = B.w[size_t(pc) * rows + r];
+            Ls[e] = sg > 0.0 ? cscale(w, 1.0 / sqrt(sg)) : cmake(0, 0);
+        }
+        for (long e = t0; e < nr; e += stride) {
+            const int m = int(e / cols), c = int(e % cols);
+            const int pc = B.perm[m];
+            const double sg = B.sigma[pc];
+            Rs[e] = cscale(cconj(B.z[size_t(pc) * cols + c]), sqrt(sg));
+        }
+    } else {
+        // W = theta^H (cols x rows), U = Z (rows x rows), V = W / sigma.
+        for (long e = t0; e < nl; e += stride) {
+            const int r = int(e / chi), m = int(e % chi);
+            const int pc = B.perm[m];
+            const double sg = B.sigma[pc];
+            Ls[e] = cscale(B.z[size_t(pc) * rows + r], sqrt(sg));
+        }
+        for (long e = t0; e < nr; e += stride) {
+            const int m = int(e / cols), c = int(e % cols);
+            const int pc = B.perm[m];
+            const double sg = B.sigma[pc];
+            const double2 w = B.w[size_t(pc) * cols + c];
+            Rs[e] = sg > 0.0 ? cscale(cconj(w), 1.0 / sqrt(sg)) : cmake(0, 0);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        mps.dr[J.p] = chi;
+        mps.dl[J.p + 1] = chi;
+        (void)dl;
+        (void)dr;
+    }
+}
+
+}  // namespace wqc

@@ -1,0 +1,48 @@
+// Kernel entry points of the two-site split pipeline and the site kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace wqc {
+
+enum { kStageY0 = 0, kStageZ = 1, kStageY = 2, kStageB = 3 };
+enum { kJacobiRsvd = 0, kJacobiExact = 1 };
+constexpr int kJacobiThreads = 256;
+
+__global__ void prepare_kernel(const SplitJob* jobs, SplitState* st, int njobs, DeviceMps mps);
+__global__ void merge_gate_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
+                                  DeviceMps mps);
+__global__ void omega_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
+__global__ void rsvd_gemm_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots, int stage);
+__global__ void householder_qr_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
+__global__ void jacobi_cluster_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
+                                      const int* idx, int mode, int max_sweeps, int* status,
+                                      unsigned long long* counters);
+__global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const SlotBuffers* slots, int mode,
+                                int chi_max, wqc_split_info* records, int* status);
+__global__ void absorb_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
+                              DeviceMps mps);
+
+// Site kernels (site_kernels.cu).
+struct OneQubitOp {
+    int site;
+    int first;  // first gate in the 2x2 array
+    int count;  // gates applied in order
+};
+__global__ void apply_1q_kernel(const OneQubitOp* ops, const double2* mats, DeviceMps mps);
+__global__ void amplitude_zero_kernel(DeviceMps mps, double2* out);
+__global__ void site_amplitudes_kernel(DeviceMps mps, int target, double2* out);
+__global__ void pauli_expectation_kernel(DeviceMps mps, const char* labels, int nterms, double2* scratch,
+                                         int env_cap, double2* out);
+
+// Jacobi shared-memory footprint for a working matrix of M rows and N columns
+// on a cluster of C CTAs.
+inline size_t jacobi_smem_bytes(int M, int N, int C) {
+    const int quantum = 4 * C;
+    const int Np = ((N + quantum - 1) / quantum) * quantum;
+    const int b = Np / (2 * C);
+    const int nbuf = C == 1 ? 2 : 3;
+    return size_t(nbuf) * b * (M + Np) * sizeof(double2);
+}
+
+}  // namespace wqc

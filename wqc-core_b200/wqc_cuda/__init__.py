@@ -1,0 +1,391 @@
+"""Python binding of the `WQC_TN_BACKEND=cuda` MPS backend (libwqc_cuda.so).
+
+``CudaMps`` mirrors the reference's ``MpsState`` (src/tn/mps.rs:55-781):
+the same operations under the same names, all executed by the sm_100a
+kernels behind the C ABI in include/wqc_cuda.h.  There is no CPU fallback:
+importing this module fails when the shared library is missing, and every
+call raises ``WqcCudaError`` when the device reports an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+from .circuits import GATE_DTYPE, SPLIT_INFO_DTYPE, gates_array  # noqa: F401
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "libwqc_cuda.so")
+
+OK = 0
+ERR_INVALID = 1
+ERR_OOM = 2
+ERR_TRUNCATION_REJECTED = 3
+ERR_SVD_FAILED = 4
+ERR_CANCELLED = 5
+ERR_DEVICE_TIMEOUT = 6
+ERR_CUDA = 7
+ERR_NO_DEVICE = 8
+ERR_QUBIT_OUT_OF_RANGE = 9
+ERR_INVALID_QUBIT_COUNT = 10
+
+PRECISION_FP64 = 0
+SPLIT_RULE_REFERENCE = 0
+SPLIT_RULE_EXACT = 1
+
+# Exported entry points of include/wqc_cuda.h (checked by the ABI tests).
+EXPORTS = (
+    "wqc_cuda_last_error", "wqc_cuda_open", "wqc_cuda_close", "wqc_cuda_device_info", "wqc_mps_workspace_bytes",
+    "wqc_mps_create", "wqc_mps_destroy", "wqc_mps_apply_gates", "wqc_mps_apply_gates_adjoint", "wqc_mps_apply_1q",
+    "wqc_mps_apply_2q", "wqc_mps_apply_2q_routed", "wqc_mps_apply_layer", "wqc_mps_synchronize", "wqc_mps_cancel",
+    "wqc_mps_amplitude_zero", "wqc_mps_site_amplitudes", "wqc_mps_bond_dims", "wqc_mps_download_site",
+    "wqc_mps_upload_site", "wqc_mps_expectation_pauli", "wqc_mps_set_split_rule", "wqc_mps_split_count", "wqc_mps_split_records",
+    "wqc_mps_peak_vram_bytes", "wqc_mps_backend_label", "wqc_mps_set_profiling", "wqc_mps_kernel_stats",
+    "wqc_mps_reset_stats", "wqc_mps_stream", "wqc_schedule_gates", "wqc_mps_reset",
+)
+
+KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
+
+
+class WqcCudaError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class KernelStats(ctypes.Structure):
+    _fields_ = [
+        ("launches", ctypes.c_uint64 * 5),
+        ("milliseconds", ctypes.c_double * 5),
+        ("total_launches", ctypes.c_uint64),
+        ("h2d_bytes", ctypes.c_uint64),
+        ("d2h_bytes", ctypes.c_uint64),
+        ("jacobi_tasks", ctypes.c_uint64),
+        ("jacobi_sweeps", ctypes.c_uint64),
+    ]
+
+
+def build() -> str:
+    """Compile libwqc_cuda.so in place for sm_100a."""
+    subprocess.run(["make", "-s", "-C", _PKG], check=True)
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built (run make -C {_PKG}); the cuda backend has no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, U32, U8, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint8, ctypes.POINTER(ctypes.c_double)
+        L.wqc_cuda_last_error.restype = ctypes.c_char_p
+        L.wqc_cuda_open.argtypes = [I, ctypes.POINTER(P)]
+        L.wqc_cuda_close.argtypes = [P]
+        L.wqc_cuda_device_info.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                           ctypes.POINTER(ctypes.c_int32)]
+        L.wqc_mps_workspace_bytes.argtypes = [U32, U32]
+        L.wqc_mps_workspace_bytes.restype = ctypes.c_uint64
+        L.wqc_mps_create.argtypes = [P, U32, U32, ctypes.c_int32, U8, ctypes.POINTER(P)]
+        L.wqc_mps_destroy.argtypes = [P]
+        L.wqc_mps_reset.argtypes = [P]
+        L.wqc_mps_apply_gates.argtypes = [P, P, U32]
+        L.wqc_mps_apply_gates_adjoint.argtypes = [P, P, U32]
+        L.wqc_mps_apply_1q.argtypes = [P, U32, D]
+        L.wqc_mps_apply_2q.argtypes = [P, U32, D, U8, P]
+        L.wqc_mps_apply_2q_routed.argtypes = [P, U32, U32, D]
+        L.wqc_mps_apply_layer.argtypes = [P, P, U32]
+        L.wqc_mps_set_split_rule.argtypes = [P, ctypes.c_int32]
+        L.wqc_mps_synchronize.argtypes = [P]
+        L.wqc_mps_cancel.argtypes = [P]
+        L.wqc_mps_cancel.restype = None
+        L.wqc_mps_amplitude_zero.argtypes = [P, D]
+        L.wqc_mps_site_amplitudes.argtypes = [P, U32, D]
+        L.wqc_mps_bond_dims.argtypes = [P, ctypes.POINTER(U32)]
+        L.wqc_mps_download_site.argtypes = [P, U32, ctypes.POINTER(U32), ctypes.POINTER(U32), D]
+        L.wqc_mps_upload_site.argtypes = [P, U32, U32, U32, D]
+        L.wqc_mps_expectation_pauli.argtypes = [P, ctypes.c_char_p, D, U32, D]
+        L.wqc_mps_split_count.argtypes = [P]
+        L.wqc_mps_split_count.restype = U32
+        L.wqc_mps_split_records.argtypes = [P, P, U32, ctypes.POINTER(U32)]
+        L.wqc_mps_peak_vram_bytes.argtypes = [P]
+        L.wqc_mps_peak_vram_bytes.restype = ctypes.c_uint64
+        L.wqc_mps_backend_label.argtypes = [P]
+        L.wqc_mps_backend_label.restype = ctypes.c_char_p
+        L.wqc_mps_set_profiling.argtypes = [P, ctypes.c_int32]
+        L.wqc_mps_kernel_stats.argtypes = [P, ctypes.POINTER(KernelStats)]
+        L.wqc_mps_reset_stats.argtypes = [P]
+        L.wqc_mps_reset_stats.restype = None
+        L.wqc_schedule_gates.argtypes = [U32, P, U32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                         U32, ctypes.POINTER(U32), ctypes.POINTER(U32)]
+        L.wqc_mps_stream.argtypes = [P]
+        L.wqc_mps_stream.restype = P
+        _LIB = L
+    return _LIB
+
+
+def _check(rc: int) -> None:
+    if rc != OK:
+        raise WqcCudaError(rc, lib().wqc_cuda_last_error().decode())
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _c128(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+class Context:
+    """The process-wide device context (engine_status.rs:27 shared device)."""
+
+    _shared = None
+
+    def __init__(self, device: int = -1):
+        h = ctypes.c_void_p()
+        _check(lib().wqc_cuda_open(device, ctypes.byref(h)))
+        self._h = h
+
+    @classmethod
+    def shared(cls) -> "Context":
+        if cls._shared is None:
+            cls._shared = Context()
+        return cls._shared
+
+    def device_info(self):
+        tot, fr, sm = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int32()
+        _check(lib().wqc_cuda_device_info(self._h, ctypes.byref(tot), ctypes.byref(fr), ctypes.byref(sm)))
+        return {"total_bytes": tot.value, "free_bytes": fr.value, "sm_count": sm.value}
+
+
+def schedule(n: int, gates: np.ndarray):
+    """Host-only: (left site per split, level per split, number of levels)
+    of the schedule wqc_mps_apply_gates uses; needs no device."""
+    g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+    ns, nl = ctypes.c_uint32(), ctypes.c_uint32()
+    _check(lib().wqc_schedule_gates(n, g.ctypes.data, len(g), None, None, 0, ctypes.byref(ns), ctypes.byref(nl)))
+    site = np.zeros(ns.value, dtype=np.int32)
+    level = np.zeros(ns.value, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int32)
+    _check(lib().wqc_schedule_gates(n, g.ctypes.data, len(g), site.ctypes.data_as(ip), level.ctypes.data_as(ip),
+                                    ns.value, ctypes.byref(ns), ctypes.byref(nl)))
+    return site, level, nl.value
+
+
+def workspace_bytes(n: int, chi: int) -> int:
+    return int(lib().wqc_mps_workspace_bytes(n, chi))
+
+
+class CudaMps:
+    """MpsState on the device: try_new_with_bond (mps.rs:82-126)."""
+
+    def __init__(self, n: int, chi: int, reject_truncation: bool = False, ctx: Context | None = None,
+                 precision: int = PRECISION_FP64):
+        self.ctx = ctx or Context.shared()
+        self.n = n
+        self.chi = chi
+        h = ctypes.c_void_p()
+        _check(lib().wqc_mps_create(self.ctx._h, n, chi, precision, int(reject_truncation), ctypes.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().wqc_mps_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def reset(self) -> None:
+        """Back to |0...0> with the split records cleared (keeps device memory)."""
+        _check(lib().wqc_mps_reset(self._h))
+
+    # --- gate application (mps.rs:278-375, 520-565, 621-677) -----------------
+    def apply_gates(self, gates: np.ndarray) -> None:
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        _check(lib().wqc_mps_apply_gates(self._h, g.ctypes.data, len(g)))
+
+    def apply_gate(self, gate) -> None:
+        self.apply_gates(gates_array([gate]) if isinstance(gate, tuple) else np.atleast_1d(gate))
+
+    def apply_gates_adjoint(self, gates: np.ndarray) -> None:
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        _check(lib().wqc_mps_apply_gates_adjoint(self._h, g.ctypes.data, len(g)))
+
+    def apply_one_qubit(self, site: int, u) -> None:
+        _check(lib().wqc_mps_apply_1q(self._h, site, _dp(_c128(u).reshape(-1).view(np.float64))))
+
+    def apply_two_qubit_at_positions(self, p: int, q: int, u, ctrl_is_first: bool, want_info: bool = False):
+        if q != p + 1:
+            raise WqcCudaError(ERR_INVALID, "two-site apply needs adjacent positions")
+        info = np.zeros(1, dtype=SPLIT_INFO_DTYPE)
+        _check(lib().wqc_mps_apply_2q(self._h, p, _dp(_c128(u).reshape(-1).view(np.float64)), int(ctrl_is_first),
+                                      info.ctypes.data if want_info else None))
+        return info[0] if want_info else None
+
+    def apply_two_qubit_gate(self, ctrl: int, tgt: int, u) -> None:
+        _check(lib().wqc_mps_apply_2q_routed(self._h, ctrl, tgt, _dp(_c128(u).reshape(-1).view(np.float64))))
+
+    def apply_adjacent_disjoint_gates(self, gates: np.ndarray) -> None:
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        _check(lib().wqc_mps_apply_layer(self._h, g.ctypes.data, len(g)))
+
+    # sweep-tree hooks (mps.rs:621-655)
+    def apply_unary_at(self, site: int, gate) -> None:
+        self.apply_gate((gate[0], site, 0, 0, gate[-1] if len(gate) > 2 else 0.0))
+
+    def apply_tdg_at(self, site: int) -> None:
+        r = 0.70710678118654752440
+        self.apply_one_qubit(site, np.array([[1, 0], [0, complex(r, -r)]]))
+
+    def apply_swap_at(self, site: int) -> None:
+        self.apply_two_qubit_at_positions(site, site + 1, SWAP4, True)
+
+    def apply_pair_at(self, site: int, kind: int, ctrl_on_left: bool) -> None:
+        from .circuits import CNOT
+        self.apply_two_qubit_at_positions(site, site + 1, CNOT4 if kind == CNOT else CZ4, ctrl_on_left)
+
+    def apply_cnot_at(self, site: int, ctrl_on_left: bool) -> None:
+        self.apply_two_qubit_at_positions(site, site + 1, CNOT4, ctrl_on_left)
+
+    # --- reads ---------------------------------------------------------------
+    def set_split_rule(self, rule: int) -> None:
+        _check(lib().wqc_mps_set_split_rule(self._h, rule))
+
+    def synchronize(self) -> None:
+        _check(lib().wqc_mps_synchronize(self._h))
+
+    def cancel(self) -> None:
+        lib().wqc_mps_cancel(self._h)
+
+    def amplitude_at_compact_zero(self) -> complex:
+        out = np.zeros(2)
+        _check(lib().wqc_mps_amplitude_zero(self._h, _dp(out)))
+        return complex(out[0], out[1])
+
+    amplitude_zero = amplitude_at_compact_zero
+
+    def site_amplitudes(self, target: int):
+        out = np.zeros(4)
+        _check(lib().wqc_mps_site_amplitudes(self._h, target, _dp(out)))
+        return complex(out[0], out[1]), complex(out[2], out[3])
+
+    def control_probability(self, control: int) -> float:
+        _, a1 = self.site_amplitudes(control)
+        return a1.real * a1.real + a1.imag * a1.imag
+
+    def bond_dims(self) -> np.ndarray:
+        out = np.zeros(self.n, dtype=np.uint32)
+        _check(lib().wqc_mps_bond_dims(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))))
+        return out.astype(np.int32)
+
+    def site(self, i: int) -> np.ndarray:
+        l, r = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().wqc_mps_download_site(self._h, i, ctypes.byref(l), ctypes.byref(r), None))
+        out = np.zeros((l.value, 2, r.value), dtype=np.complex128)
+        _check(lib().wqc_mps_download_site(self._h, i, ctypes.byref(l), ctypes.byref(r), _dp(out.view(np.float64))))
+        return out
+
+    def set_site(self, i: int, t: np.ndarray) -> None:
+        t = _c128(t)
+        _check(lib().wqc_mps_upload_site(self._h, i, t.shape[0], t.shape[2], _dp(t.view(np.float64))))
+
+    def to_dense_state(self) -> np.ndarray:
+        """Dense 2^N vector from the downloaded sites (mps.rs:742-780 layout:
+        qubit q is bit q); for tests and small registers."""
+        state = np.ones((1, 1), dtype=np.complex128)  # [basis, bond]
+        for q in range(self.n):
+            s = self.site(q)
+            nxt = np.einsum("xa,asb->sxb", state, s)  # basis bit q is the new slowest index
+            state = nxt.reshape(-1, s.shape[2])
+        return state[:, 0]
+
+    def expectation(self, labels, coeffs) -> complex:
+        joined = "".join(labels).encode()
+        c = _c128(coeffs)
+        out = np.zeros(2)
+        _check(lib().wqc_mps_expectation_pauli(self._h, joined, _dp(c.view(np.float64)), len(labels), _dp(out)))
+        return complex(out[0], out[1])
+
+    def split_records(self) -> np.ndarray:
+        k = lib().wqc_mps_split_count(self._h)
+        out = np.zeros(k, dtype=SPLIT_INFO_DTYPE)
+        w = ctypes.c_uint32()
+        _check(lib().wqc_mps_split_records(self._h, out.ctypes.data if k else None, k, ctypes.byref(w)))
+        return out[: w.value]
+
+    def peak_vram_bytes(self) -> int:
+        return int(lib().wqc_mps_peak_vram_bytes(self._h))
+
+    def backend_label(self) -> str:
+        return lib().wqc_mps_backend_label(self._h).decode()
+
+    def set_profiling(self, on: bool) -> None:
+        _check(lib().wqc_mps_set_profiling(self._h, int(on)))
+
+    def kernel_stats(self) -> dict:
+        st = KernelStats()
+        _check(lib().wqc_mps_kernel_stats(self._h, ctypes.byref(st)))
+        return {
+            "launches": {k: int(st.launches[i]) for i, k in enumerate(KERNEL_KINDS)},
+            "milliseconds": {k: float(st.milliseconds[i]) for i, k in enumerate(KERNEL_KINDS)},
+            "total_launches": int(st.total_launches),
+            "h2d_bytes": int(st.h2d_bytes),
+            "d2h_bytes": int(st.d2h_bytes),
+            "jacobi_tasks": int(st.jacobi_tasks),
+            "jacobi_sweeps": int(st.jacobi_sweeps),
+        }
+
+    def reset_stats(self) -> None:
+        lib().wqc_mps_reset_stats(self._h)
+
+    def stream(self) -> int:
+        return int(lib().wqc_mps_stream(self._h) or 0)
+
+
+def _mat4(entries) -> np.ndarray:
+    m = np.zeros((2, 2, 2, 2), dtype=np.complex128)
+    for idx, v in entries:
+        m[idx] = v
+    return m
+
+
+# Mat4 [c_out][t_out][c_in][t_in] (src/tn/gates.rs:68-104)
+CNOT4 = _mat4([((0, 0, 0, 0), 1), ((0, 1, 0, 1), 1), ((1, 0, 1, 1), 1), ((1, 1, 1, 0), 1)])
+CZ4 = _mat4([((0, 0, 0, 0), 1), ((0, 1, 0, 1), 1), ((1, 0, 1, 0), 1), ((1, 1, 1, 1), -1)])
+SWAP4 = _mat4([((0, 0, 0, 0), 1), ((0, 1, 1, 0), 1), ((1, 0, 0, 1), 1), ((1, 1, 1, 1), 1)])
+
+
+def run(n: int, chi: int, gates: np.ndarray, ctx: Context | None = None, rule: int = SPLIT_RULE_REFERENCE) -> CudaMps:
+    m = CudaMps(n, chi, ctx=ctx)
+    m.set_split_rule(rule)
+    m.apply_gates(gates)
+    return m
+
+
+def svd_flops(rows: int, cols: int) -> float:
+    """Algorithmic complex SVD flops (Golub-Van Loan count for S, thin U, V, x4 for complex)."""
+    p, q = min(rows, cols), max(rows, cols)
+    return 4.0 * (14.0 * q * p * p + 8.0 * p ** 3)
+
+
+def split_flops(rec) -> float:
+    """Algorithmic flops of one split's SVD stage from its record (the exact
+    SVD, or the range finder's products, QR and projected SVD)."""
+    rows, cols, ell, path = int(rec["rows"]), int(rec["cols"]), int(rec["ell"]), int(rec["path"])
+    if path == 1:
+        return 8.0 * (3 * rows * cols * ell + ell * rows * cols) + 4.0 * (4 * rows * ell * ell) + svd_flops(ell, cols)
+    f = svd_flops(rows, cols)
+    if path == 2:
+        f += 8.0 * (3 * rows * cols * ell + ell * rows * cols) + 4.0 * (4 * rows * ell * ell) + svd_flops(ell, cols)
+    return f
+
+
+__all__ = ["CudaMps", "Context", "WqcCudaError", "lib", "build", "run", "workspace_bytes", "split_flops",
+           "svd_flops", "CNOT4", "CZ4", "SWAP4", "EXPORTS", "KERNEL_KINDS", "math"]
