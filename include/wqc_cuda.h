@@ -164,6 +164,14 @@ WQC_API wqc_status wqc_mps_upload_site(wqc_mps* mps, uint32_t site, uint32_t l, 
 WQC_API wqc_status wqc_mps_expectation_pauli(wqc_mps* mps, const char* labels, const double* coeffs, uint32_t nterms,
                                      double out[2]);
 
+/* Diagnostics: copy one split-workspace buffer of `slot` (the last wave's
+ * job in that slot) to host memory, at most `bytes`.  which: 0 theta
+ * (rows x cols, row-major), 1 Omega, 2 A*Omega, 3 A^H*(A*Omega), 4 Y then
+ * Householder vectors (column-major), 5 thin Q (column-major), 6 Q^H A,
+ * 7 Jacobi W, 8 Jacobi Z (column-major), 9 column norms, 10 sort
+ * permutation, 11 Householder scalars, 12 the split's device state. */
+WQC_API wqc_status wqc_mps_debug_workspace(wqc_mps* mps, uint32_t slot, int32_t which, void* out, uint64_t bytes);
+
 /* Split records in program order (one per merge + gate + split). */
 WQC_API uint32_t wqc_mps_split_count(wqc_mps* mps);
 WQC_API wqc_status wqc_mps_split_records(wqc_mps* mps, wqc_split_info* out, uint32_t max, uint32_t* written);

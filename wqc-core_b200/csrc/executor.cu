@@ -242,6 +242,10 @@ void set_kernel_attributes() {
     if (g_attr_err == cudaSuccess)
         g_attr_err = cudaFuncSetAttribute(jacobi_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (g_attr_err == cudaSuccess)
+        g_attr_err = cudaFuncSetAttribute(qr_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLimit));
+    if (g_attr_err == cudaSuccess)
+        g_attr_err = cudaFuncSetAttribute(qr_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (g_attr_err == cudaSuccess)
         g_attr_err = cudaFuncSetAttribute(amplitude_zero_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     if (g_attr_err == cudaSuccess)
         g_attr_err = cudaFuncSetAttribute(site_amplitudes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
@@ -672,7 +676,30 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                 rsvd_gemm_kernel<<<dim3(te, tr, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageY0);
                 rsvd_gemm_kernel<<<dim3(te, tc, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageZ);
                 rsvd_gemm_kernel<<<dim3(te, tr, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageY);
-                householder_qr_kernel<<<nj, 512, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots);
+                int cq = 0;
+                for (int c = 8; c <= m->ctx->max_cluster; c *= 2)
+                    if (qr_cluster_smem_bytes(w.max_rows, w.max_ell, c) <= kSmemLimit) {
+                        cq = c;
+                        break;
+                    }
+                if (cq) {
+                    cudaLaunchConfig_t cfg = {};
+                    cfg.gridDim = dim3(nj * cq);
+                    cfg.blockDim = dim3(kQrClusterThreads);
+                    cfg.dynamicSmemBytes = qr_cluster_smem_bytes(w.max_rows, w.max_ell, cq);
+                    cfg.stream = m->stream;
+                    cudaLaunchAttribute attr[1];
+                    attr[0].id = cudaLaunchAttributeClusterDimension;
+                    attr[0].val.clusterDim.x = cq;
+                    attr[0].val.clusterDim.y = 1;
+                    attr[0].val.clusterDim.z = 1;
+                    cfg.attrs = attr;
+                    cfg.numAttrs = 1;
+                    CUDA_TRY(cudaLaunchKernelEx(&cfg, qr_cluster_kernel, d_jobs, (const SplitState*)m->d_state,
+                                                (const SlotBuffers*)m->d_slots));
+                } else {
+                    householder_qr_kernel<<<nj, 512, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots);
+                }
                 rsvd_gemm_kernel<<<dim3(tc, te, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageB);
                 for (int k = 0; k < 6; ++k) count_launch(m, 2);
             }
@@ -690,7 +717,7 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
             finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiExact, m->chi,
                                                         m->d_records, m->d_status);
             const int per = std::max(w.max_rows, w.max_cols) * std::min(m->chi, std::max(w.max_rows, w.max_cols));
-            const int gx = std::max(1, std::min(32, per / 2048));
+            const int gx = std::max(1, std::min(128, per / 256));
             absorb_kernel<<<dim3(gx, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);
             count_launch(m, 4);
             count_launch(m, 4);
@@ -1161,6 +1188,35 @@ wqc_status wqc_mps_expectation_pauli(wqc_mps* m, const char* labels, const doubl
     }
     out[0] = re;
     out[1] = im;
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_debug_workspace(wqc_mps* m, uint32_t slot, int32_t which, void* out, uint64_t bytes) {
+    if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
+    if (int(slot) >= m->nslots) return fail(WQC_ERR_INVALID, "slot out of range");
+    if (wqc_status s = sync_status(m)) return s;
+    SlotBuffers b;
+    CUDA_TRY(cudaMemcpy(&b, m->d_slots + slot, sizeof(b), cudaMemcpyDeviceToHost));
+    const void* src = nullptr;
+    const int R = 2 * m->chi, E = std::min(m->chi + kRsvdOversample, R);
+    size_t cap = 0;
+    switch (which) {
+        case 0: src = b.theta; cap = size_t(R) * R * sizeof(double2); break;
+        case 1: src = b.omega; cap = size_t(R) * E * sizeof(double2); break;
+        case 2: src = b.y0; cap = size_t(R) * E * sizeof(double2); break;
+        case 3: src = b.zr; cap = size_t(R) * E * sizeof(double2); break;
+        case 4: src = b.y; cap = size_t(R) * E * sizeof(double2); break;
+        case 5: src = b.q; cap = size_t(R) * E * sizeof(double2); break;
+        case 6: src = b.b; cap = size_t(R) * E * sizeof(double2); break;
+        case 7: src = b.w; cap = size_t(R) * R * sizeof(double2); break;
+        case 8: src = b.z; cap = size_t(R) * R * sizeof(double2); break;
+        case 9: src = b.sigma; cap = size_t(R) * sizeof(double); break;
+        case 10: src = b.perm; cap = size_t(R) * sizeof(int); break;
+        case 11: src = b.tau; cap = size_t(E) * sizeof(double2); break;
+        case 12: src = m->d_state + slot; cap = sizeof(SplitState); break;
+        default: return fail(WQC_ERR_INVALID, "unknown workspace buffer");
+    }
+    CUDA_TRY(cudaMemcpy(out, src, std::min<size_t>(cap, bytes), cudaMemcpyDeviceToHost));
     return WQC_OK;
 }
 

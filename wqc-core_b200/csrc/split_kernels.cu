@@ -344,6 +344,128 @@ __global__ void __launch_bounds__(kQrThreads) householder_qr_kernel(const SplitJ
 }
 
 // ---------------------------------------------------------------------------
+// The same Householder QR and thin Q on a thread-block cluster: CTA r holds
+// columns [r*cpc, (r+1)*cpc) of Y and of Q in shared memory.  At step c the
+// owner of column c forms the reflector, publishes v_c and tau_c in a
+// double-buffered slot of its shared memory and updates its own trailing
+// columns; after one cluster barrier the CTAs to its right copy v_c through
+// distributed shared memory and update theirs.  Q is then accumulated
+// backward with every reflector read from its owner.  Same arithmetic as the
+// single-CTA kernel above.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void reflect_columns(double2* cols, int ldc, int count, const double2* v, double2 t,
+                                                int c, int m, int lane, int wid, int nw) {
+    for (int kk = wid; kk < count; kk += nw) {
+        double2* ck = cols + size_t(kk) * ldc;
+        double2 w = cmake(0, 0);
+        for (int i = c + lane; i < m; i += 32) cfma_conj(w, v[i], ck[i]);
+        for (int o = 16; o > 0; o >>= 1) {
+            w.x += __shfl_xor_sync(0xffffffffu, w.x, o);
+            w.y += __shfl_xor_sync(0xffffffffu, w.y, o);
+        }
+        w = cmul(t, w);
+        for (int i = c + lane; i < m; i += 32) ck[i] = csub(ck[i], cmul(v[i], w));
+    }
+}
+
+__global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const SplitJob* jobs, const SplitState* st,
+                                                                           const SlotBuffers* slots) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = int(cluster.num_blocks());
+    const int rank = int(cluster.block_rank());
+    const int j = blockIdx.x / C;
+    const SplitState S = st[j];
+    if (!S.use_rsvd) return;  // uniform over the cluster
+    const SlotBuffers B = slots[jobs[j].slot];
+    const int m = S.rows, n = S.ell;
+    const int cpc = (n + C - 1) / C;
+    const int c0 = min(n, rank * cpc), c1 = min(n, c0 + cpc), nloc = c1 - c0;
+    extern __shared__ __align__(16) double2 qsm[];
+    double2* Ys = qsm;                              // cpc columns of m
+    double2* Qs = Ys + size_t(cpc) * m;             // cpc columns of m
+    double2* bcast = Qs + size_t(cpc) * m;          // 2 slots of m
+    double2* vloc = bcast + size_t(2) * m;          // m
+    double2* taus = vloc + m;                       // cpc local tau values
+    __shared__ double red[kQrClusterThreads / 32];
+    __shared__ double2 s_tau[2];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = kQrClusterThreads / 32;
+    for (int e = tid; e < nloc * m; e += kQrClusterThreads) Ys[e] = B.y[size_t(c0) * m + e];
+    __syncthreads();
+    for (int c = 0; c < n; ++c) {
+        const int owner = c / cpc;
+        const int slot = c & 1;
+        if (rank == owner) {
+            double2* col = Ys + size_t(c - c0) * m;
+            double part = 0;
+            for (int i = c + 1 + tid; i < m; i += kQrClusterThreads) part += cnorm2(col[i]);
+            const double xnorm2 = block_sum(part, red);
+            const double2 alpha = col[c];
+            double2 t = cmake(0, 0), sc = cmake(0, 0);
+            double beta = alpha.x;
+            const bool trivial = (xnorm2 == 0.0 && alpha.y == 0.0);
+            if (!trivial) {
+                beta = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
+                if (alpha.x >= 0) beta = -beta;
+                t = cmake((beta - alpha.x) / beta, -alpha.y / beta);
+                const double2 d = cmake(alpha.x - beta, alpha.y);
+                const double dn = d.x * d.x + d.y * d.y;
+                sc = cmake(d.x / dn, -d.y / dn);
+            }
+            __syncthreads();
+            double2* bv = bcast + size_t(slot) * m;
+            for (int i = c + 1 + tid; i < m; i += kQrClusterThreads) {
+                const double2 x = trivial ? col[i] : cmul(col[i], sc);
+                col[i] = x;
+                bv[i] = x;
+            }
+            if (tid == 0) {
+                col[c] = cmake(beta, 0.0);
+                bv[c] = cmake(1.0, 0.0);
+                taus[c - c0] = t;
+                s_tau[slot] = t;
+            }
+            __syncthreads();
+            if (!trivial)
+                reflect_columns(Ys + size_t(c - c0 + 1) * m, m, c1 - c - 1, bv, cconj(t), c, m, lane, wid, nw);
+        }
+        cluster.sync();
+        if (rank > owner && nloc > 0) {
+            const double2* rv = cluster.map_shared_rank(bcast, owner) + size_t(slot) * m;
+            for (int i = c + tid; i < m; i += kQrClusterThreads) vloc[i] = rv[i];
+            const double2 t = *cluster.map_shared_rank(&s_tau[slot], owner);
+            __syncthreads();
+            if (t.x != 0.0 || t.y != 0.0) reflect_columns(Ys, m, nloc, vloc, cconj(t), c, m, lane, wid, nw);
+            __syncthreads();
+        }
+    }
+    cluster.sync();  // every reflector is final
+    for (int e = tid; e < nloc * m; e += kQrClusterThreads) {
+        const int r = e % m, cc = c0 + e / m;
+        Qs[e] = cmake(r == cc ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    for (int c = nloc > 0 ? c1 - 1 : -1; c >= 0; --c) {
+        const int owner = c / cpc;
+        const double2* rcol = cluster.map_shared_rank(Ys, owner) + size_t(c - owner * cpc) * m;
+        for (int i = c + 1 + tid; i < m; i += kQrClusterThreads) vloc[i] = rcol[i];
+        if (tid == 0) {
+            vloc[c] = cmake(1.0, 0.0);
+            s_tau[0] = *(cluster.map_shared_rank(taus, owner) + (c - owner * cpc));
+        }
+        __syncthreads();
+        const double2 t = s_tau[0];
+        const int first = max(c, c0);
+        if ((t.x != 0.0 || t.y != 0.0) && first < c1)
+            reflect_columns(Qs + size_t(first - c0) * m, m, c1 - first, vloc, t, c, m, lane, wid, nw);
+        __syncthreads();
+    }
+    for (int e = tid; e < nloc * m; e += kQrClusterThreads) B.q[size_t(c0) * m + e] = Qs[e];
+    for (int e = tid; e < nloc * m; e += kQrClusterThreads) B.y[size_t(c0) * m + e] = Ys[e];
+    if (tid < nloc) B.tau[c0 + tid] = taus[tid];
+    cluster.sync();  // no CTA leaves while another may still read its shared memory
+}
+
+// ---------------------------------------------------------------------------
 // One-sided Hestenes Jacobi SVD on a thread-block cluster.
 //
 // The tall working matrix W (M x N, padded to N' = 2*C*b columns) and the
@@ -360,6 +482,7 @@ struct JacobiCtl {
     int top_buf, bot_buf, spare_buf;
     int top_id, bot_id;
     int rot;
+    unsigned long long relmax_bits;  // largest |gamma|/sqrt(alpha beta) seen this sweep (non-negative double bits)
     double fro_part;
 };
 
@@ -384,7 +507,7 @@ __device__ __forceinline__ int circle_at(int pos, int step, int b) {
 // theta) would otherwise be re-rotated every sweep until their products
 // reach the subnormal range.
 __device__ __forceinline__ int jacobi_rotate(double2* xp, double2* xq, int M, int len, double tol, double noise_floor,
-                                             int lane) {
+                                             int lane, double& relmax) {
     double a = 0, bb = 0, gr = 0, gi = 0;
     for (int r = lane; r < M; r += 32) {
         const double2 u = xp[r], v = xq[r];
@@ -402,7 +525,9 @@ __device__ __forceinline__ int jacobi_rotate(double2* xp, double2* xq, int M, in
     }
     const double g = hypot(gr, gi);
     const double scale = sqrt(a) * sqrt(bb);
-    if (g == 0.0 || g <= tol * scale || scale <= noise_floor) return 0;
+    if (scale <= noise_floor) return 0;
+    relmax = fmax(relmax, g / scale);
+    if (g == 0.0 || g <= tol * scale) return 0;
     const double pr = gr / g, pi = gi / g;
     const double zeta = (bb - a) / (2.0 * g);
     const double t = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
@@ -533,9 +658,13 @@ __global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const
     int sweep = 0;
     bool converged = false;
     for (; sweep < max_sweeps; ++sweep) {
-        if (tid == 0) ctl.rot = 0;
+        if (tid == 0) {
+            ctl.rot = 0;
+            ctl.relmax_bits = 0ull;
+        }
         __syncthreads();
         int my_rot = 0;
+        double my_rel = 0.0;
         // Pairs inside each block (circle method on b columns).
         for (int step = 0; step < b - 1; ++step) {
             for (int pq = wid; pq < b; pq += nwarps) {
@@ -543,7 +672,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const
                 const int i = top ? pq : pq - b / 2;
                 double2* base = buf(top ? ctl.top_buf : ctl.bot_buf);
                 const int e1 = circle_at(i, step, b), e2 = circle_at(b - 1 - i, step, b);
-                my_rot += jacobi_rotate(base + size_t(e1) * len, base + size_t(e2) * len, M, len, tol, noise_floor, lane);
+                my_rot += jacobi_rotate(base + size_t(e1) * len, base + size_t(e2) * len, M, len, tol, noise_floor, lane, my_rel);
             }
             __syncthreads();
         }
@@ -554,7 +683,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const
                 double2* bb = buf(ctl.bot_buf);
                 for (int i = wid; i < b; i += nwarps) {
                     const int e2 = (i + k) % b;
-                    my_rot += jacobi_rotate(tb + size_t(i) * len, bb + size_t(e2) * len, M, len, tol, noise_floor, lane);
+                    my_rot += jacobi_rotate(tb + size_t(i) * len, bb + size_t(e2) * len, M, len, tol, noise_floor, lane, my_rel);
                 }
                 __syncthreads();
             }
@@ -605,17 +734,28 @@ __global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const
         }
         // Cluster-wide rotation count decides convergence.
         if (lane == 0 && my_rot) atomicAdd(&ctl.rot, my_rot);
+        if (lane == 0 && my_rel > 0.0) atomicMax(&ctl.relmax_bits, (unsigned long long)__double_as_longlong(my_rel));
         __syncthreads();
         int total = 0;
+        double relmax = 0.0;
         if (C == 1) {
             total = ctl.rot;
+            relmax = __longlong_as_double((long long)ctl.relmax_bits);
             __syncthreads();
         } else {
             cluster.sync();
-            for (int r = 0; r < C; ++r) total += cluster.map_shared_rank(&ctl, r)->rot;
+            for (int r = 0; r < C; ++r) {
+                const JacobiCtl* rc = cluster.map_shared_rank(&ctl, r);
+                total += rc->rot;
+                relmax = fmax(relmax, __longlong_as_double((long long)rc->relmax_bits));
+            }
             cluster.sync();
         }
-        if (total == 0) {
+        // Converged when nothing rotated, or when every pair entered this
+        // sweep orthogonal to 1e-8: one-sided Jacobi converges quadratically,
+        // so this sweep left them orthogonal to about 1e-16, below the
+        // rotation tolerance, and a verification sweep would rotate nothing.
+        if (total == 0 || relmax < 1e-8) {
             converged = true;
             break;
         }

@@ -7,7 +7,7 @@ namespace wqc {
 
 enum { kStageY0 = 0, kStageZ = 1, kStageY = 2, kStageB = 3 };
 enum { kJacobiRsvd = 0, kJacobiExact = 1 };
-constexpr int kJacobiThreads = 256;
+constexpr int kJacobiThreads = 512;  // 16 warps: one column pair per warp per step (blocks of <= 16 pairs)
 
 __global__ void prepare_kernel(const SplitJob* jobs, SplitState* st, int njobs, DeviceMps mps);
 __global__ void merge_gate_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
@@ -15,6 +15,13 @@ __global__ void merge_gate_kernel(const SplitJob* jobs, const SplitState* st, co
 __global__ void omega_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
 __global__ void rsvd_gemm_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots, int stage);
 __global__ void householder_qr_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
+constexpr int kQrClusterThreads = 256;
+__global__ void qr_cluster_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
+// Shared memory of qr_cluster_kernel for an m x n Y on a cluster of C CTAs.
+inline size_t qr_cluster_smem_bytes(int m, int n, int C) {
+    const int cpc = (n + C - 1) / C;
+    return (size_t(2) * cpc * m + size_t(3) * m + cpc) * sizeof(double2);
+}
 __global__ void jacobi_cluster_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
                                       const int* idx, int mode, int max_sweeps, int* status,
                                       unsigned long long* counters);

@@ -44,7 +44,7 @@ EXPORTS = (
     "wqc_mps_amplitude_zero", "wqc_mps_site_amplitudes", "wqc_mps_bond_dims", "wqc_mps_download_site",
     "wqc_mps_upload_site", "wqc_mps_expectation_pauli", "wqc_mps_set_split_rule", "wqc_mps_split_count", "wqc_mps_split_records",
     "wqc_mps_peak_vram_bytes", "wqc_mps_backend_label", "wqc_mps_set_profiling", "wqc_mps_kernel_stats",
-    "wqc_mps_reset_stats", "wqc_mps_stream", "wqc_schedule_gates", "wqc_mps_reset",
+    "wqc_mps_reset_stats", "wqc_mps_stream", "wqc_schedule_gates", "wqc_mps_reset", "wqc_mps_debug_workspace",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
@@ -123,6 +123,7 @@ def lib():
         L.wqc_mps_reset_stats.restype = None
         L.wqc_schedule_gates.argtypes = [U32, P, U32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                          U32, ctypes.POINTER(U32), ctypes.POINTER(U32)]
+        L.wqc_mps_debug_workspace.argtypes = [P, U32, ctypes.c_int32, P, ctypes.c_uint64]
         L.wqc_mps_stream.argtypes = [P]
         L.wqc_mps_stream.restype = P
         _LIB = L
@@ -344,6 +345,12 @@ class CudaMps:
 
     def reset_stats(self) -> None:
         lib().wqc_mps_reset_stats(self._h)
+
+    def debug_workspace(self, slot: int, which: int, count: int, dtype=np.complex128) -> np.ndarray:
+        """Copy of one split-workspace buffer (see wqc_mps_debug_workspace)."""
+        out = np.zeros(count, dtype=dtype)
+        _check(lib().wqc_mps_debug_workspace(self._h, slot, which, out.ctypes.data, out.nbytes))
+        return out
 
     def stream(self) -> int:
         return int(lib().wqc_mps_stream(self._h) or 0)
