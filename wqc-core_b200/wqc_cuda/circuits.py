@@ -77,6 +77,13 @@ class Workload:
         k = self.gates["kind"]
         return int(np.count_nonzero((k == CNOT) | (k == CZ)) + np.count_nonzero(k == CCNOT))
 
+    def layer_starts(self) -> list:
+        """Gate index where each layer begins: every generator opens a layer
+        with a one-qubit gate on qubit 0."""
+        k, q0 = self.gates["kind"], self.gates["q0"]
+        first = np.isin(k, ONE_QUBIT) & (q0 == 0)
+        return [i for i in range(len(k)) if first[i] and (i == 0 or not first[i - 1])]
+
 
 def ry_rz_brickwork(n: int, depth: int, seed: int) -> list:
     """RY(theta) and RZ(phi) on every qubit (angles U[0, 2pi)), then CNOT on
