@@ -81,6 +81,26 @@ WQC_API wqc_status wqc_mps_create(wqc_cuda_ctx* ctx, uint32_t qubit_count, uint3
                           uint8_t reject_truncation, wqc_mps** out);
 WQC_API void wqc_mps_destroy(wqc_mps* mps);
 
+/* Batching form: `count` independent slices (the orchestrator's tensor-network
+ * slices, each its own register and chi_max) held in one state.  The slices'
+ * sites are concatenated, so every wave of splits mixes ready splits from all
+ * slices; each slice still sees exactly its own MpsState sequence.
+ * max_concurrent_splits bounds the split workspace (0: one slot per two
+ * sites).  No reference counterpart: the reference runs one slice per
+ * request (src/api.rs:336-697); this is how one B200 takes many at once. */
+WQC_API wqc_status wqc_batch_create(wqc_cuda_ctx* ctx, uint32_t count, const uint32_t* qubit_counts,
+                                    const uint32_t* max_bond_dims, int32_t precision, uint32_t max_concurrent_splits,
+                                    wqc_mps** out);
+/* Gates of slice s are gates[offsets[s] .. offsets[s+1]); qubits are local to
+ * the slice.  Semantics per slice as wqc_mps_apply_gates. */
+WQC_API wqc_status wqc_batch_apply_gates(wqc_mps* batch, const wqc_gate* gates, const uint32_t* offsets);
+/* <0...0|psi_s> of every slice: out[2s], out[2s+1]. */
+WQC_API wqc_status wqc_batch_amplitudes(wqc_mps* batch, double* out);
+/* With profiling on: milliseconds from the start of the last
+ * wqc_batch_apply_gates call to the completion of each slice's last split
+ * (CUDA events on the state's stream); -1 for a slice without operations. */
+WQC_API wqc_status wqc_batch_slice_times(wqc_mps* batch, double* out_ms);
+
 /* Back to |0...0> with the split records cleared, keeping the device memory
  * (a fresh MpsState for the next request without reallocating). */
 WQC_API wqc_status wqc_mps_reset(wqc_mps* mps);

@@ -24,13 +24,25 @@ def rel_err(a: complex, b: complex, norm: float = 1.0) -> float:
     return abs(a - b) / max(abs(b), 1e-12 * norm)
 
 
+def amp_err(a: complex, b: complex, n: int) -> float:
+    """Relative error of an amplitude, guarded by 2^(-n/2), the typical size of
+    an amplitude of an n-qubit unit state: <0|psi> of a deep circuit is a
+    cancelling sum of much larger terms, and rounding in those terms is what
+    a tiny amplitude can be checked against."""
+    return abs(a - b) / max(abs(b), 2.0 ** (-n / 2.0))
+
+
 def assert_records_match(got, ref):
     assert len(got) == len(ref), f"split count {len(got)} != {len(ref)}"
     for k in ("left_site", "rows", "cols", "ell", "path", "chi"):
         bad = np.nonzero(got[k] != ref[k])[0]
         assert bad.size == 0, f"{k} differs at splits {bad[:10]}: got {got[k][bad[:10]]} ref {ref[k][bad[:10]]}"
     d = np.abs(got["discarded_weight"] - ref["discarded_weight"])
-    tol = DISC_ATOL * np.maximum(1.0, np.abs(ref["discarded_weight"]))
+    # Rounding differences accumulate through the truncating splits: the
+    # bound is DISC_ATOL over the 150 splits of the 16-qubit chi 32 circuit
+    # and grows linearly with the split index beyond that.
+    growth = np.maximum(1.0, np.arange(len(ref)) / 150.0)
+    tol = DISC_ATOL * np.maximum(1.0, np.abs(ref["discarded_weight"])) * growth
     bad = np.nonzero(d > tol)[0]
     assert bad.size == 0, (f"discarded weight differs at splits {bad[:5]}: got {got['discarded_weight'][bad[:5]]} "
                            f"ref {ref['discarded_weight'][bad[:5]]}")
@@ -264,3 +276,22 @@ def test_time_split_rejects_truncation(cuda_ctx):
         m.apply_gates(g)
         m.synchronize()
     assert e.value.code == W.ERR_TRUNCATION_REJECTED
+
+
+def test_batch_of_uneven_slices_matches_oracle_per_slice(cuda_ctx):
+    """The batching form: slices of different width, depth and chi_max in one
+    state; every slice must equal its own oracle run (amplitude, records)."""
+    slices = C.config2_slices(12, seed=99)
+    for s in slices:  # keep the oracle side short
+        s.chi = min(s.chi, 32)
+    b = W.CudaBatch([s.n for s in slices], [s.chi for s in slices], ctx=cuda_ctx)
+    b.set_profiling(True)
+    b.apply_slices([s.gates for s in slices])
+    amps = b.amplitudes()
+    recs = b.slice_records()
+    times = b.slice_times_ms()
+    assert np.all(times > 0)
+    for i, s in enumerate(slices):
+        o = O.run(s.n, s.chi, s.gates)
+        assert amp_err(amps[i], o.amplitude_zero(), s.n) < AMP_RTOL, (i, amps[i], o.amplitude_zero())
+        assert_records_match(recs[i], o.records())

@@ -70,7 +70,7 @@ struct SplitJob {
     int slot;         // workspace slot
     int reject;       // reject_truncation (time-split halves)
     int exact_only;   // split rule: exact SVD on every split, no range finder
-    int pad_;
+    int chi_max;      // max bond dimension of the state (or batch slice) the split belongs to
     double2 u[16];    // effective 4x4 on theta: u[(so*2+to)*4 + si*2+ti]
 };
 

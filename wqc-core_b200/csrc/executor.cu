@@ -137,7 +137,8 @@ void effective(const Mat4& u, bool ctrl_is_first, double2* out) {
 
 struct Op {
     bool two;
-    int site;        // 1q: site; 2q: left site
+    int site;        // 1q: site; 2q: left site (global site index)
+    int slice = 0;   // batch slice the operation belongs to
     Mat2 m2;
     double2 ueff[16];
 };
@@ -145,6 +146,7 @@ struct Op {
 struct Group {
     int mode, C, idx_off, count;
     size_t smem;
+    int threads;  // one warp per column pair of a block, at most kJacobiThreads
 };
 
 struct Wave {
@@ -177,7 +179,7 @@ struct wqc_mps {
     cudaStream_t stream = nullptr;
     // device state
     double2* site_pool = nullptr;
-    size_t site_cap = 0;  // complex entries per site
+    std::vector<double2*> site_ptr;  // device address of every site (capacity chi_slice * 2 * chi_slice)
     DeviceMps dev{};
     double2** d_site_ptr = nullptr;
     int* d_dl = nullptr;
@@ -202,6 +204,15 @@ struct wqc_mps {
     unsigned long long* d_counters = nullptr;  // Jacobi tasks, Jacobi sweeps
     // host bounds: ub[i] = upper bound of the bond between sites i and i+1
     std::vector<int> ub;
+    // slices: a single state is one slice; a batch concatenates its slices'
+    // sites, and no split ever crosses a slice boundary
+    std::vector<int> seg_first, seg_n, seg_chi;
+    std::vector<int> site_chi, site_slice;
+    int* d_seg = nullptr;  // (first, count) per slice for the amplitude kernel
+    // per-slice completion times of the last call (batch, profiling on)
+    std::vector<int> slice_last_wave;
+    std::vector<cudaEvent_t> wave_done;
+    cudaEvent_t call_start = nullptr;
     // accounting
     uint64_t bytes_now = 0, bytes_peak = 0;
     bool profiling = false;
@@ -253,17 +264,37 @@ void set_kernel_attributes() {
 
 int round_up(int x, int q) { return ((x + q - 1) / q) * q; }
 
-// Smallest cluster that holds the working matrix, preferring blocks of at
-// most 16 columns so each CTA step has at most two pairs per warp.
-int choose_cluster(int M, int N, int max_c) {
-    int fallback = -1;
-    for (int Cc = 1; Cc <= max_c; Cc *= 2) {
+// Cluster size for a Jacobi SVD of an M x N working matrix.  Every sweep has
+// N'-1 steps (N' = N padded to a multiple of 4C) whatever C is; a larger C
+// gives each CTA fewer column pairs per step (b = N'/2C) but adds 2C-1 block
+// exchanges per sweep.  The model below (FP64 work per step and CTA, a floor
+// for one pair's latency, a fixed cost per exchange plus its DSMEM traffic)
+// picks the fastest sweep when the wave's splits cannot fill the GPU, and the
+// least SM-time per split when they can.
+int choose_cluster(int M, int N, int max_c, int njobs, int sm_count) {
+    struct Cand { int C; double sweep_us; };
+    std::vector<Cand> cands;
+    for (int Cc = 1; Cc <= max_c; ++Cc) {
         if (jacobi_smem_bytes(M, N, Cc) > kSmemLimit) continue;
-        const int b = round_up(N, 4 * Cc) / (2 * Cc);
-        if (b <= 16) return Cc;
-        if (fallback < 0) fallback = Cc;
+        const int Np = round_up(N, 4 * Cc), b = Np / (2 * Cc);
+        if (b > 16 && Cc < max_c) continue;  // more pairs than warps
+        const double len = M + Np;
+        const double step = std::max(0.3, b * (8.0 * M + 12.0 * len) / 64.0 / 1900.0);
+        const double exch = Cc > 1 ? 2.0 + 2.0 * b * len * 16.0 / 1.0e5 : 0.0;
+        cands.push_back({Cc, (Np - 1) * step + (2 * Cc - 1) * exch});
     }
-    return fallback;
+    if (cands.empty()) return -1;
+    int best = cands[0].C;
+    double best_cost = 1e300;
+    for (const Cand& c : cands) {
+        const bool fills = double(njobs) * c.C >= 1.5 * sm_count;
+        const double cost = fills ? c.sweep_us * c.C : c.sweep_us;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c.C;
+        }
+    }
+    return best;
 }
 
 cudaEvent_t get_event(wqc_mps* m) {
@@ -351,11 +382,11 @@ struct Expander {
     }
 };
 
-wqc_status check_gate(const wqc_mps* m, const wqc_gate& g) {
+wqc_status check_gate(int n, const wqc_gate& g) {
     auto chk = [&](int q) -> wqc_status {
-        if (q < 0 || q >= m->n)
+        if (q < 0 || q >= n)
             return fail(WQC_ERR_QUBIT_OUT_OF_RANGE,
-                        "Qubit index " + std::to_string(q) + " out of bounds (limit: " + std::to_string(m->n) + ")");
+                        "Qubit index " + std::to_string(q) + " out of bounds (limit: " + std::to_string(n) + ")");
         return WQC_OK;
     };
     wqc_status s = WQC_OK;
@@ -378,10 +409,10 @@ wqc_status check_gate(const wqc_mps* m, const wqc_gate& g) {
     }
 }
 
-wqc_status expand(const wqc_mps* m, const wqc_gate* gates, uint32_t count, bool adjoint, Expander& ex) {
+wqc_status expand(int n, const wqc_gate* gates, uint32_t count, bool adjoint, Expander& ex) {
     for (uint32_t i = 0; i < count; ++i) {
         const wqc_gate& g = gates[adjoint ? count - 1 - i : i];
-        if (wqc_status s = check_gate(m, g)) return s;
+        if (wqc_status s = check_gate(n, g)) return s;
         switch (g.kind) {
             case WQC_GATE_CNOT:
                 ex.two_routed(g.q0, g.q1, adjoint ? adjoint4(cnot_matrix()) : cnot_matrix());
@@ -414,6 +445,7 @@ struct Plan {
     std::vector<double2> mats;
     std::vector<SplitJob> jobs;
     std::vector<int> idx;
+    std::vector<int> slice_last_wave;  // last wave holding an operation of each slice
     uint32_t first_seq = 0, nsplits = 0;
 };
 
@@ -443,6 +475,8 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
         std::vector<int> oq_index;                          // site -> entry in oq (built lazily)
         std::vector<SplitJob> jobs;
         std::vector<std::pair<int, int>> bounds;  // (ub left of p, ub right of p+1) at the job
+        std::vector<int> job_slice;
+        std::vector<int> oq_slices;
     };
     std::vector<LevelBuild> levels;
     std::vector<int> level_of;
@@ -462,6 +496,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
             if (e < 0) {
                 e = int(lb.oq.size());
                 lb.oq.push_back({o.site, {}});
+                lb.oq_slices.push_back(o.slice);
             }
             lb.oq[e].second.push_back(o.m2);
         } else {
@@ -472,20 +507,24 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
             J.seq = int(seq++);
             J.reject = m->reject ? 1 : 0;
             J.exact_only = m->exact_only ? 1 : 0;
+            J.chi_max = m->site_chi[p];
             std::memcpy(J.u, o.ueff, sizeof(J.u));
             const int bl = m->left_bond(p), br = m->right_bond(p + 1);
             lb.jobs.push_back(J);
             lb.bounds.push_back({bl, br});
-            m->ub[p] = std::min(std::min(2 * bl, 2 * br), m->chi);
+            lb.job_slice.push_back(o.slice);
+            m->ub[p] = std::min(std::min(2 * bl, 2 * br), J.chi_max);
         }
     }
     plan.nsplits = seq - plan.first_seq;
+    plan.slice_last_wave.assign(m->seg_first.size(), -1);
     for (LevelBuild& lb : levels) {
         // one-qubit ops run first, in one wave with no splits when needed
         size_t j0 = 0;
         bool first = true;
         do {
             Wave w;
+            const int wave_index = int(plan.waves.size());
             if (first) {
                 w.oq_off = int(plan.oq.size());
                 for (auto& e : lb.oq) {
@@ -497,6 +536,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                         for (int k = 0; k < 4; ++k) plan.mats.push_back(u.u[k]);
                     plan.oq.push_back(op);
                 }
+                for (int sl : lb.oq_slices) plan.slice_last_wave[sl] = std::max(plan.slice_last_wave[sl], wave_index);
                 w.oq_count = int(lb.oq.size());
                 first = false;
             }
@@ -505,36 +545,43 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
             w.njobs = int(j1 - j0);
             // cluster groups: key (mode, C)
             std::vector<std::pair<std::pair<int, int>, std::vector<int>>> groups;
-            auto add = [&](int mode, int Cc, int local, size_t smem) {
+            auto add = [&](int mode, int Cc, int local) {
                 for (auto& g : groups)
                     if (g.first.first == mode && g.first.second == Cc) {
                         g.second.push_back(local);
                         return;
                     }
                 groups.push_back({{mode, Cc}, {local}});
-                (void)smem;
             };
-            std::vector<size_t> gsmem;
+            auto shape = [&](size_t k, int& rows, int& cols, int& ell) {
+                rows = 2 * lb.bounds[k].first;
+                cols = 2 * lb.bounds[k].second;
+                ell = std::min(std::min(lb.jobs[k].chi_max + kRsvdOversample, rows), cols);
+            };
             for (size_t k = j0; k < j1; ++k) {
                 SplitJob J = lb.jobs[k];
                 const int local = int(k - j0);
                 J.slot = local;
                 plan.jobs.push_back(J);
-                const int bl = lb.bounds[k].first, br = lb.bounds[k].second;
-                const int rows = 2 * bl, cols = 2 * br;
-                const int ell = std::min(std::min(m->chi + kRsvdOversample, rows), cols);
+                plan.slice_last_wave[lb.job_slice[k]] = std::max(plan.slice_last_wave[lb.job_slice[k]], wave_index);
+                int rows, cols, ell;
+                shape(k, rows, cols, ell);
                 const unsigned long long f = (unsigned long long)rows * cols * ell;
                 const bool rs = !m->reject && !m->exact_only && ell < std::min(rows, cols) &&
                                 f >= (unsigned long long)kRsvdMinSide * kRsvdMinSide * kRsvdMinSide;
-                w.max_dl = std::max(w.max_dl, bl);
-                w.max_dr = std::max(w.max_dr, br);
+                w.max_dl = std::max(w.max_dl, lb.bounds[k].first);
+                w.max_dr = std::max(w.max_dr, lb.bounds[k].second);
                 w.max_rows = std::max(w.max_rows, rows);
                 w.max_cols = std::max(w.max_cols, cols);
                 w.max_ell = std::max(w.max_ell, ell);
-                add(kJacobiExact, choose_cluster(std::max(rows, cols), std::min(rows, cols), m->ctx->max_cluster), local, 0);
+                const int nj_wave = int(j1 - j0);
+                add(kJacobiExact,
+                    choose_cluster(std::max(rows, cols), std::min(rows, cols), m->ctx->max_cluster, nj_wave,
+                                   m->ctx->sm_count),
+                    local);
                 if (rs) {
                     w.any_rsvd = true;
-                    add(kJacobiRsvd, choose_cluster(cols, ell, m->ctx->max_cluster), local, 0);
+                    add(kJacobiRsvd, choose_cluster(cols, ell, m->ctx->max_cluster, nj_wave, m->ctx->sm_count), local);
                 }
             }
             for (auto& g : groups) {
@@ -546,15 +593,23 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 // shared memory for the largest job of the group
                 size_t sm = 0;
                 for (int local : g.second) {
-                    const int bl = lb.bounds[j0 + local].first, br = lb.bounds[j0 + local].second;
-                    const int rows = 2 * bl, cols = 2 * br;
-                    const int ell = std::min(std::min(m->chi + kRsvdOversample, rows), cols);
-                    const size_t s = gr.mode == kJacobiExact
-                                         ? jacobi_smem_bytes(std::max(rows, cols), std::min(rows, cols), std::max(gr.C, 1))
-                                         : jacobi_smem_bytes(cols, ell, std::max(gr.C, 1));
-                    sm = std::max(sm, s);
+                    int rows, cols, ell;
+                    shape(j0 + local, rows, cols, ell);
+                    const size_t sz = gr.mode == kJacobiExact
+                                          ? jacobi_smem_bytes(std::max(rows, cols), std::min(rows, cols), std::max(gr.C, 1))
+                                          : jacobi_smem_bytes(cols, ell, std::max(gr.C, 1));
+                    sm = std::max(sm, sz);
                 }
                 gr.smem = sm;
+                int bmax = 1;
+                for (int local : g.second) {
+                    int rows, cols, ell;
+                    shape(j0 + local, rows, cols, ell);
+                    const int N = gr.mode == kJacobiExact ? std::min(rows, cols) : ell;
+                    const int Cc = std::max(gr.C, 1);
+                    bmax = std::max(bmax, round_up(N, 4 * Cc) / (2 * Cc));
+                }
+                gr.threads = 32 * std::min(kJacobiThreads / 32, std::max(2, bmax));
                 for (int local : g.second) plan.idx.push_back(local);
                 w.groups.push_back(gr);
             }
@@ -625,14 +680,29 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
     const SplitJob* d_jobs_all = reinterpret_cast<const SplitJob*>(dbase + o_jobs);
     const int* d_idx = reinterpret_cast<const int*>(dbase + o_idx);
 
-    for (const Wave& w : plan.waves) {
+    const bool track = m->profiling && !plan.slice_last_wave.empty();
+    if (track) {
+        while (m->wave_done.size() < plan.waves.size()) {
+            cudaEvent_t e = nullptr;
+            CUDA_TRY(cudaEventCreate(&e));
+            m->wave_done.push_back(e);
+        }
+        if (!m->call_start) CUDA_TRY(cudaEventCreate(&m->call_start));
+        CUDA_TRY(cudaEventRecord(m->call_start, m->stream));
+        m->slice_last_wave = plan.slice_last_wave;
+    }
+    for (size_t wi = 0; wi < plan.waves.size(); ++wi) {
+        const Wave& w = plan.waves[wi];
         if (w.oq_count > 0) {
             Timed t(m, 3);
             const int gx = std::min(64, std::max(1, (m->chi * m->chi + 1023) / 1024));
             apply_1q_kernel<<<dim3(gx, w.oq_count), 256, 0, m->stream>>>(d_oq + w.oq_off, d_mats, m->dev);
             count_launch(m, 3);
         }
-        if (w.njobs == 0) continue;
+        if (w.njobs == 0) {
+            if (track) CUDA_TRY(cudaEventRecord(m->wave_done[wi], m->stream));
+            continue;
+        }
         const SplitJob* d_jobs = d_jobs_all + w.jobs_off;
         const int nj = w.njobs;
         {
@@ -651,7 +721,7 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                 Timed t(m, 0);
                 cudaLaunchConfig_t cfg = {};
                 cfg.gridDim = dim3(gr.count * gr.C);
-                cfg.blockDim = dim3(kJacobiThreads);
+                cfg.blockDim = dim3(gr.threads);
                 cfg.dynamicSmemBytes = gr.smem;
                 cfg.stream = m->stream;
                 cudaLaunchAttribute attr[1];
@@ -722,6 +792,7 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
             count_launch(m, 4);
             count_launch(m, 4);
         }
+        if (track) CUDA_TRY(cudaEventRecord(m->wave_done[wi], m->stream));
     }
     CUDA_TRY(cudaGetLastError());
     m->rec_count = plan.first_seq + plan.nsplits;
@@ -733,6 +804,14 @@ wqc_status run_ops(wqc_mps* m, const std::vector<Op>& ops) {
     Plan plan;
     build_plan(m, ops, plan);
     return launch_plan(m, plan);
+}
+
+// |0> on every site, all bonds 1, status cleared (mps.rs:101-109).
+wqc_status reset_sites(wqc_mps* m) {
+    reset_sites_kernel<<<(m->n + 255) / 256, 256, 0, m->stream>>>(m->dev);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(m->stream));
+    return WQC_OK;
 }
 
 wqc_status sync_status(wqc_mps* m) {
@@ -817,34 +896,56 @@ uint64_t wqc_mps_workspace_bytes(uint32_t n, uint32_t chi) {
     return v > ~uint64_t(0) ? ~uint64_t(0) : uint64_t(v);
 }
 
-wqc_status wqc_mps_create(wqc_cuda_ctx* ctx, uint32_t n, uint32_t chi, int32_t precision, uint8_t reject,
-                          wqc_mps** out) {
+static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, const std::vector<int>& chis,
+                               int32_t precision, bool reject, int nslots_req, wqc_mps** out) {
     if (!ctx || !out) return fail(WQC_ERR_INVALID, "null argument");
-    if (n == 0) return fail(WQC_ERR_INVALID_QUBIT_COUNT, "Invalid qubit count: 0. Max limit is 40.");
-    if (chi == 0) return fail(WQC_ERR_INVALID, "MPS max bond dimension must be > 0");
+    if (ns.empty()) return fail(WQC_ERR_INVALID, "no slices");
+    long total_n = 0;
+    int chi_cap = 0;
+    for (size_t i = 0; i < ns.size(); ++i) {
+        if (ns[i] <= 0)
+            return fail(WQC_ERR_INVALID_QUBIT_COUNT, "Invalid qubit count: " + std::to_string(ns[i]) + ". Max limit is 40.");
+        if (chis[i] <= 0) return fail(WQC_ERR_INVALID, "MPS max bond dimension must be > 0");
+        if (chis[i] > 256) return fail(WQC_ERR_INVALID, "the cuda backend supports max_bond_dim <= 256");
+        total_n += ns[i];
+        chi_cap = std::max(chi_cap, chis[i]);
+    }
     if (precision != WQC_PRECISION_FP64) return fail(WQC_ERR_INVALID, "unsupported precision form");
-    if (chi > 256) return fail(WQC_ERR_INVALID, "the cuda backend supports max_bond_dim <= 256");
+    if (total_n > (1L << 24)) return fail(WQC_ERR_INVALID, "too many sites");
     CUDA_TRY(cudaSetDevice(ctx->device));
     auto* m = new wqc_mps();
+    const int n = int(total_n);
     m->ctx = ctx;
-    m->n = int(n);
-    m->chi = int(chi);
-    m->reject = reject != 0;
+    m->n = n;
+    m->chi = chi_cap;
+    m->reject = reject;
     m->ub.assign(n > 0 ? n - 1 : 0, 1);
-    auto bail = [&](wqc_status s) {
+    m->site_chi.resize(n);
+    m->site_slice.resize(n);
+    std::vector<size_t> site_off(n + 1, 0);
+    for (size_t sl = 0, g = 0; sl < ns.size(); ++sl) {
+        m->seg_first.push_back(int(g));
+        m->seg_n.push_back(ns[sl]);
+        m->seg_chi.push_back(chis[sl]);
+        for (int q = 0; q < ns[sl]; ++q, ++g) {
+            m->site_chi[g] = chis[sl];
+            m->site_slice[g] = int(sl);
+            site_off[g + 1] = site_off[g] + size_t(chis[sl]) * 2 * chis[sl];
+        }
+    }
+    auto bail = [&](wqc_status st) {
         wqc_mps_destroy(m);
-        return s;
+        return st;
     };
     if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "stream"));
     if (cudaEventCreateWithFlags(&m->stage_done, cudaEventDisableTiming) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "event"));
     cudaEventRecord(m->stage_done, m->stream);
     // Budget check before any large allocation (mps.rs:36-48 analogue).
-    const int R = 2 * int(chi), E = std::min(int(chi) + kRsvdOversample, R);
+    const int R = 2 * chi_cap, E = std::min(chi_cap + kRsvdOversample, R);
     const size_t slot_c = size_t(R) * R * 3 + size_t(R) * E * 6 + E;  // theta, w, z + range finder + tau
     const size_t slot_bytes = ((slot_c * sizeof(double2) + size_t(R) * (sizeof(double) + sizeof(int)) + 4095) / 4096) * 4096;
-    m->nslots = std::max(1, int(n) / 2);
-    m->site_cap = size_t(chi) * 2 * chi;
-    const size_t site_bytes = size_t(n) * m->site_cap * sizeof(double2);
+    m->nslots = nslots_req > 0 ? nslots_req : std::max(1, n / 2);
+    const size_t site_bytes = site_off[n] * sizeof(double2);
     const uint64_t need = site_bytes + uint64_t(m->nslots) * slot_bytes;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "cudaMemGetInfo"));
@@ -852,24 +953,27 @@ wqc_status wqc_mps_create(wqc_cuda_ctx* ctx, uint32_t n, uint32_t chi, int32_t p
         return bail(fail(WQC_ERR_OOM, "Insufficient memory: need " + std::to_string(need) + " bytes, only " +
                                           std::to_string(fr) + " bytes free on the device"));
     void* p = nullptr;
-    if (wqc_status s = dmalloc(m, &p, site_bytes)) return bail(s);
+    if (wqc_status st = dmalloc(m, &p, site_bytes)) return bail(st);
     m->site_pool = static_cast<double2*>(p);
-    if (wqc_status s = dmalloc(m, &p, n * sizeof(double2*))) return bail(s);
+    if (wqc_status st = dmalloc(m, &p, size_t(n) * sizeof(double2*))) return bail(st);
     m->d_site_ptr = static_cast<double2**>(p);
-    if (wqc_status s = dmalloc(m, &p, 2 * n * sizeof(int) + 64)) return bail(s);
+    if (wqc_status st = dmalloc(m, &p, 2 * size_t(n) * sizeof(int) + 64)) return bail(st);
     m->d_dl = static_cast<int*>(p);
     m->d_dr = m->d_dl + n;
     m->d_status = m->d_dr + n;
-    if (wqc_status s = dmalloc(m, &p, size_t(m->nslots) * slot_bytes)) return bail(s);
+    if (wqc_status st = dmalloc(m, &p, 2 * ns.size() * sizeof(int))) return bail(st);
+    m->d_seg = static_cast<int*>(p);
+    if (wqc_status st = dmalloc(m, &p, size_t(m->nslots) * slot_bytes)) return bail(st);
     m->slot_pool = static_cast<char*>(p);
-    if (wqc_status s = dmalloc(m, &p, m->nslots * sizeof(SlotBuffers))) return bail(s);
+    if (wqc_status st = dmalloc(m, &p, m->nslots * sizeof(SlotBuffers))) return bail(st);
     m->d_slots = static_cast<SlotBuffers*>(p);
-    if (wqc_status s = dmalloc(m, &p, m->nslots * sizeof(SplitState))) return bail(s);
+    if (wqc_status st = dmalloc(m, &p, m->nslots * sizeof(SplitState))) return bail(st);
     m->d_state = static_cast<SplitState*>(p);
-    if (wqc_status s = dmalloc(m, &p, 64 * sizeof(double2))) return bail(s);
+    const size_t small = std::max<size_t>(64, 2 * ns.size() + 8);
+    if (wqc_status st = dmalloc(m, &p, small * sizeof(double2))) return bail(st);
     m->d_small = static_cast<double2*>(p);
-    m->d_counters = reinterpret_cast<unsigned long long*>(m->d_small + 60);
-    if (cudaMemset(m->d_small, 0, 64 * sizeof(double2)) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "memset"));
+    m->d_counters = reinterpret_cast<unsigned long long*>(m->d_small + small - 4);
+    if (cudaMemset(m->d_small, 0, small * sizeof(double2)) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "memset"));
     int* hc = nullptr;
     if (cudaHostAlloc(reinterpret_cast<void**>(&hc), sizeof(int), cudaHostAllocMapped) != cudaSuccess)
         return bail(fail(WQC_ERR_CUDA, "cudaHostAlloc"));
@@ -877,60 +981,70 @@ wqc_status wqc_mps_create(wqc_cuda_ctx* ctx, uint32_t n, uint32_t chi, int32_t p
     m->h_cancel = hc;
     if (cudaHostGetDevicePointer(reinterpret_cast<void**>(&m->d_cancel), hc, 0) != cudaSuccess)
         return bail(fail(WQC_ERR_CUDA, "cudaHostGetDevicePointer"));
-    // site pointers, |0> sites, dims
-    std::vector<double2*> ptrs(n);
-    for (uint32_t i = 0; i < n; ++i) ptrs[i] = m->site_pool + i * m->site_cap;
-    std::vector<int> ones(2 * n + 16, 1);
-    for (int i = 0; i < 16; ++i) ones[2 * n + i] = 0;
-    std::vector<double2> zero_site(2, make_double2(0, 0));
-    zero_site[0] = make_double2(1.0, 0.0);
-    if (cudaMemcpy(m->d_site_ptr, ptrs.data(), n * sizeof(double2*), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(m->d_dl, ones.data(), (2 * n + 16) * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    m->site_ptr.resize(n);
+    for (int i = 0; i < n; ++i) m->site_ptr[i] = m->site_pool + site_off[i];
+    std::vector<int> seg(2 * ns.size());
+    for (size_t sl = 0; sl < ns.size(); ++sl) {
+        seg[2 * sl] = m->seg_first[sl];
+        seg[2 * sl + 1] = m->seg_n[sl];
+    }
+    if (cudaMemcpy(m->d_site_ptr, m->site_ptr.data(), size_t(n) * sizeof(double2*), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m->d_seg, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(WQC_ERR_CUDA, "initial upload"));
-    for (uint32_t i = 0; i < n; ++i)
-        if (cudaMemcpy(ptrs[i], zero_site.data(), 2 * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
-            return bail(fail(WQC_ERR_CUDA, "initial upload"));
     std::vector<SlotBuffers> slots(m->nslots);
-    for (int s = 0; s < m->nslots; ++s) {
-        char* base = m->slot_pool + size_t(s) * slot_bytes;
+    for (int sl = 0; sl < m->nslots; ++sl) {
+        char* base = m->slot_pool + size_t(sl) * slot_bytes;
         double2* c = reinterpret_cast<double2*>(base);
-        SlotBuffers& b = slots[s];
-        b.theta = c; c += size_t(R) * R;
-        b.w = c; c += size_t(R) * R;
-        b.z = c; c += size_t(R) * R;
-        b.omega = c; c += size_t(R) * E;
-        b.y0 = c; c += size_t(R) * E;
-        b.zr = c; c += size_t(R) * E;
-        b.y = c; c += size_t(R) * E;
-        b.q = c; c += size_t(R) * E;
-        b.b = c; c += size_t(R) * E;
-        b.tau = c; c += E;
-        b.sigma = reinterpret_cast<double*>(c);
-        b.perm = reinterpret_cast<int*>(b.sigma + R);
+        SlotBuffers& bf = slots[sl];
+        bf.theta = c; c += size_t(R) * R;
+        bf.w = c; c += size_t(R) * R;
+        bf.z = c; c += size_t(R) * R;
+        bf.omega = c; c += size_t(R) * E;
+        bf.y0 = c; c += size_t(R) * E;
+        bf.zr = c; c += size_t(R) * E;
+        bf.y = c; c += size_t(R) * E;
+        bf.q = c; c += size_t(R) * E;
+        bf.b = c; c += size_t(R) * E;
+        bf.tau = c; c += E;
+        bf.sigma = reinterpret_cast<double*>(c);
+        bf.perm = reinterpret_cast<int*>(bf.sigma + R);
     }
     if (cudaMemcpy(m->d_slots, slots.data(), slots.size() * sizeof(SlotBuffers), cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(WQC_ERR_CUDA, "slot table upload"));
     m->dev.site = m->d_site_ptr;
     m->dev.dl = m->d_dl;
     m->dev.dr = m->d_dr;
-    m->dev.n = int(n);
-    m->dev.chi_max = int(chi);
+    m->dev.n = n;
+    m->dev.chi_max = chi_cap;
     m->dev.status = m->d_status;
     m->dev.cancel = m->d_cancel;
-    if (wqc_status s = ensure_records(m, 1024)) return bail(s);
+    if (wqc_status st = ensure_records(m, 1024)) return bail(st);
+    if (wqc_status st = reset_sites(m)) return bail(st);
     *out = m;
     return WQC_OK;
 }
 
+wqc_status wqc_mps_create(wqc_cuda_ctx* ctx, uint32_t n, uint32_t chi, int32_t precision, uint8_t reject,
+                          wqc_mps** out) {
+    return create_state(ctx, {int(n)}, {int(chi)}, precision, reject != 0, 0, out);
+}
+
+wqc_status wqc_batch_create(wqc_cuda_ctx* ctx, uint32_t count, const uint32_t* qubit_counts,
+                            const uint32_t* max_bond_dims, int32_t precision, uint32_t max_concurrent_splits,
+                            wqc_mps** out) {
+    if (!qubit_counts || !max_bond_dims || count == 0) return fail(WQC_ERR_INVALID, "null argument");
+    std::vector<int> ns(count), chis(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        ns[i] = int(qubit_counts[i]);
+        chis[i] = int(max_bond_dims[i]);
+    }
+    return create_state(ctx, ns, chis, precision, false, int(max_concurrent_splits), out);
+}
+
 wqc_status wqc_mps_reset(wqc_mps* m) {
     if (!m) return fail(WQC_ERR_INVALID, "null argument");
-    if (wqc_status s = sync_status(m)) return s;
-    std::vector<int> ones(2 * m->n + 16, 1);
-    for (int i = 0; i < 16; ++i) ones[2 * m->n + i] = 0;
-    CUDA_TRY(cudaMemcpy(m->d_dl, ones.data(), ones.size() * sizeof(int), cudaMemcpyHostToDevice));
-    const double2 zero[2] = {make_double2(1.0, 0.0), make_double2(0.0, 0.0)};
-    for (int i = 0; i < m->n; ++i)
-        CUDA_TRY(cudaMemcpy(m->site_pool + size_t(i) * m->site_cap, zero, sizeof(zero), cudaMemcpyHostToDevice));
+    if (wqc_status st = sync_status(m)) return st;
+    if (wqc_status st = reset_sites(m)) return st;
     std::fill(m->ub.begin(), m->ub.end(), 1);
     m->rec_count = 0;
     *m->h_cancel = 0;
@@ -948,6 +1062,9 @@ void wqc_mps_destroy(wqc_mps* m) {
     dfree(m, m->d_state, 0);
     dfree(m, m->d_small, 0);
     dfree(m, m->d_records, 0);
+    dfree(m, m->d_seg, 0);
+    for (auto e : m->wave_done) cudaEventDestroy(e);
+    if (m->call_start) cudaEventDestroy(m->call_start);
     dfree(m, m->d_stage.d, 0);
     if (m->h_stage) cudaFreeHost(m->h_stage);
     if (m->h_cancel) cudaFreeHost(const_cast<int*>(m->h_cancel));
@@ -964,10 +1081,8 @@ void wqc_mps_destroy(wqc_mps* m) {
 wqc_status wqc_schedule_gates(uint32_t n, const wqc_gate* gates, uint32_t count, int32_t* split_site,
                               int32_t* split_level, uint32_t max, uint32_t* nsplits, uint32_t* nlevels) {
     if (n == 0 || (!gates && count) || !nsplits || !nlevels) return fail(WQC_ERR_INVALID, "null argument");
-    wqc_mps probe;
-    probe.n = int(n);
     Expander ex;
-    if (wqc_status s = expand(&probe, gates, count, false, ex)) return s;
+    if (wqc_status s = expand(int(n), gates, count, false, ex)) return s;
     std::vector<int> level_of;
     assign_levels(int(n), ex.ops, level_of);
     uint32_t k = 0;
@@ -989,15 +1104,59 @@ wqc_status wqc_schedule_gates(uint32_t n, const wqc_gate* gates, uint32_t count,
 wqc_status wqc_mps_apply_gates(wqc_mps* m, const wqc_gate* gates, uint32_t count) {
     if (!m || (!gates && count)) return fail(WQC_ERR_INVALID, "null argument");
     Expander ex;
-    if (wqc_status s = expand(m, gates, count, false, ex)) return s;
+    if (wqc_status s = expand(m->n, gates, count, false, ex)) return s;
     return run_ops(m, ex.ops);
 }
 
 wqc_status wqc_mps_apply_gates_adjoint(wqc_mps* m, const wqc_gate* gates, uint32_t count) {
     if (!m || (!gates && count)) return fail(WQC_ERR_INVALID, "null argument");
     Expander ex;
-    if (wqc_status s = expand(m, gates, count, true, ex)) return s;
+    if (wqc_status s = expand(m->n, gates, count, true, ex)) return s;
     return run_ops(m, ex.ops);
+}
+
+wqc_status wqc_batch_apply_gates(wqc_mps* m, const wqc_gate* gates, const uint32_t* offsets) {
+    if (!m || !offsets) return fail(WQC_ERR_INVALID, "null argument");
+    Expander all;
+    for (size_t sl = 0; sl < m->seg_first.size(); ++sl) {
+        const uint32_t g0 = offsets[sl], g1 = offsets[sl + 1];
+        if (g1 < g0) return fail(WQC_ERR_INVALID, "gate offsets must not decrease");
+        if (g1 == g0) continue;
+        if (!gates) return fail(WQC_ERR_INVALID, "null gates");
+        Expander ex;
+        if (wqc_status s = expand(m->seg_n[sl], gates + g0, g1 - g0, false, ex)) return s;
+        for (Op& o : ex.ops) {
+            o.site += m->seg_first[sl];
+            o.slice = int(sl);
+            all.ops.push_back(o);
+        }
+    }
+    return run_ops(m, all.ops);
+}
+
+wqc_status wqc_batch_amplitudes(wqc_mps* m, double* out) {
+    if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
+    const int nseg = int(m->seg_first.size());
+    amplitude_zero_kernel<<<nseg, 512, 2 * m->chi * sizeof(double2), m->stream>>>(m->dev, m->d_seg, m->d_small);
+    count_launch(m, -1);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, m->d_small, nseg * sizeof(double2), cudaMemcpyDeviceToHost, m->stream));
+    m->stats.d2h_bytes += nseg * sizeof(double2);
+    return sync_status(m);
+}
+
+wqc_status wqc_batch_slice_times(wqc_mps* m, double* out_ms) {
+    if (!m || !out_ms) return fail(WQC_ERR_INVALID, "null argument");
+    if (wqc_status s = sync_status(m)) return s;
+    const size_t nseg = m->seg_first.size();
+    for (size_t sl = 0; sl < nseg; ++sl) {
+        const int w = sl < m->slice_last_wave.size() ? m->slice_last_wave[sl] : -1;
+        float ms = -1.0f;
+        if (w >= 0 && m->call_start && size_t(w) < m->wave_done.size())
+            CUDA_TRY(cudaEventElapsedTime(&ms, m->call_start, m->wave_done[w]));
+        out_ms[sl] = double(ms);
+    }
+    return WQC_OK;
 }
 
 wqc_status wqc_mps_apply_1q(wqc_mps* m, uint32_t site, const double u[8]) {
@@ -1069,7 +1228,7 @@ void wqc_mps_cancel(wqc_mps* m) {
 
 wqc_status wqc_mps_amplitude_zero(wqc_mps* m, double out[2]) {
     if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
-    amplitude_zero_kernel<<<1, 512, 2 * m->chi * sizeof(double2), m->stream>>>(m->dev, m->d_small);
+    amplitude_zero_kernel<<<1, 512, 2 * m->chi * sizeof(double2), m->stream>>>(m->dev, m->d_seg, m->d_small);
     count_launch(m, -1);
     CUDA_TRY(cudaGetLastError());
     double2 h;
@@ -1116,7 +1275,7 @@ wqc_status wqc_mps_download_site(wqc_mps* m, uint32_t site, uint32_t* l, uint32_
     *l = uint32_t(dl);
     *r = uint32_t(dr);
     if (buf)
-        CUDA_TRY(cudaMemcpy(buf, m->site_pool + site * m->site_cap, size_t(dl) * 2 * dr * sizeof(double2),
+        CUDA_TRY(cudaMemcpy(buf, m->site_ptr[site], size_t(dl) * 2 * dr * sizeof(double2),
                             cudaMemcpyDeviceToHost));
     return WQC_OK;
 }
@@ -1126,7 +1285,7 @@ wqc_status wqc_mps_upload_site(wqc_mps* m, uint32_t site, uint32_t l, uint32_t r
     if (int(site) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
     if (l == 0 || r == 0 || int(l) > m->chi || int(r) > m->chi) return fail(WQC_ERR_INVALID, "site shape exceeds max_bond_dim");
     if (wqc_status s = sync_status(m)) return s;
-    CUDA_TRY(cudaMemcpy(m->site_pool + site * m->site_cap, buf, size_t(l) * 2 * r * sizeof(double2), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(m->site_ptr[site], buf, size_t(l) * 2 * r * sizeof(double2), cudaMemcpyHostToDevice));
     const int il = int(l), ir = int(r);
     CUDA_TRY(cudaMemcpy(m->d_dl + site, &il, sizeof(int), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(m->d_dr + site, &ir, sizeof(int), cudaMemcpyHostToDevice));

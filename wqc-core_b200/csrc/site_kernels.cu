@@ -30,15 +30,29 @@ __global__ void __launch_bounds__(256) apply_1q_kernel(const OneQubitOp* ops, co
     }
 }
 
-// <0...0|psi> (mps.rs:262-276): v <- v . site[:, 0, :] along the chain.
-__global__ void __launch_bounds__(512) amplitude_zero_kernel(DeviceMps mps, double2* out) {
+// Every site back to |0> (mps.rs:101-109): [1, 0] with bonds 1.
+__global__ void reset_sites_kernel(DeviceMps mps) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *mps.status = 0;
+    if (i >= mps.n) return;
+    mps.site[i][0] = cmake(1.0, 0.0);
+    mps.site[i][1] = cmake(0.0, 0.0);
+    mps.dl[i] = 1;
+    mps.dr[i] = 1;
+}
+
+// <0...0|psi> (mps.rs:262-276): v <- v . site[:, 0, :] along the chain.  One
+// CTA per state: block b runs sites seg[2b] .. seg[2b] + seg[2b+1] - 1 (the
+// slices of a batch, or the single state).
+__global__ void __launch_bounds__(512) amplitude_zero_kernel(DeviceMps mps, const int* seg, double2* out) {
     extern __shared__ double2 vbuf[];  // 2 * chi_max
     double2* v = vbuf;
     double2* nx = vbuf + mps.chi_max;
+    const int first = seg[2 * blockIdx.x], count = seg[2 * blockIdx.x + 1];
     int len = 1;
     if (threadIdx.x == 0) v[0] = cmake(1.0, 0.0);
     __syncthreads();
-    for (int i = 0; i < mps.n; ++i) {
+    for (int i = first; i < first + count; ++i) {
         const int l = mps.dl[i], r = mps.dr[i];
         const double2* s = mps.site[i];
         const int la = min(l, len);
@@ -53,7 +67,7 @@ __global__ void __launch_bounds__(512) amplitude_zero_kernel(DeviceMps mps, doub
         nx = t;
         len = r;
     }
-    if (threadIdx.x == 0) *out = len > 0 ? v[0] : cmake(0, 0);
+    if (threadIdx.x == 0) out[blockIdx.x] = len > 0 ? v[0] : cmake(0, 0);
 }
 
 // Trace feeders (mps.rs:679-740): environments with the all-ones physical

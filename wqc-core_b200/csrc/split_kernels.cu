@@ -37,7 +37,7 @@ __global__ void prepare_kernel(const SplitJob* jobs, SplitState* st, int njobs, 
     s.k = min(mps.dr[J.p], mps.dl[J.p + 1]);
     s.rows = 2 * s.dl;
     s.cols = 2 * s.dr;
-    s.ell = min(min(mps.chi_max + kRsvdOversample, s.rows), s.cols);
+    s.ell = min(min(J.chi_max + kRsvdOversample, s.rows), s.cols);
     const unsigned long long f = (unsigned long long)s.rows * s.cols * s.ell;
     const unsigned long long side = kRsvdMinSide;
     const bool worth = f >= side * side * side;
@@ -533,13 +533,13 @@ __device__ __forceinline__ int jacobi_rotate(double2* xp, double2* xq, int M, in
     const double t = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
     const double c = 1.0 / sqrt(1.0 + t * t);
     const double s = c * t;
+    // With w = s * phase the rephased rotation (svd_guard.rs:189-197) is
+    // xp' = c xp - conj(w) xq,  xq' = w xp + c xq   (|phase| = 1).
+    const double wr = s * pr, wi = s * pi;
     for (int r = lane; r < len; r += 32) {
         const double2 u = xp[r], v = xq[r];
-        const double vqx = v.x * pr + v.y * pi, vqy = v.y * pr - v.x * pi;  // v * conj(phase)
-        const double npx = u.x * c - vqx * s, npy = u.y * c - vqy * s;
-        const double tx = u.x * s + vqx * c, ty = u.y * s + vqy * c;
-        xp[r] = cmake(npx, npy);
-        xq[r] = cmake(tx * pr - ty * pi, tx * pi + ty * pr);  // * phase
+        xp[r] = cmake(fma(c, u.x, -fma(wr, v.x, wi * v.y)), fma(c, u.y, -fma(wr, v.y, -wi * v.x)));
+        xq[r] = cmake(fma(wr, u.x, fma(-wi, u.y, c * v.x)), fma(wr, u.y, fma(wi, u.x, c * v.y)));
     }
     return 1;
 }
@@ -565,7 +565,7 @@ __device__ __forceinline__ bool jacobi_active(const SplitState& S, int mode) {
     return mode == kJacobiRsvd ? S.use_rsvd != 0 : S.need_exact != 0;
 }
 
-__global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const SplitJob* jobs, const SplitState* st,
+__global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const SplitJob* jobs, const SplitState* st,
                                                                           const SlotBuffers* slots, const int* idx,
                                                                           int mode, int max_sweeps, int* status,
                                                                           unsigned long long* counters) {
@@ -591,7 +591,8 @@ __global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const
     extern __shared__ __align__(16) double2 smem[];
     __shared__ JacobiCtl ctl;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int nwarps = kJacobiThreads / 32;
+    const int nthreads = blockDim.x;  // a multiple of 32, at most kJacobiThreads
+    const int nwarps = nthreads / 32;
     auto buf = [&](int k) { return smem + size_t(k) * b * len; };
     __shared__ double red[kJacobiThreads / 32];
 
@@ -610,7 +611,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const
     double part = 0;
     for (int half = 0; half < 2; ++half) {
         const int id = half == 0 ? rank : 2 * C - 1 - rank;
-        for (int e = tid; e < b * M; e += kJacobiThreads) {
+        for (int e = tid; e < b * M; e += nthreads) {
             int c, i;
             if (rows_of_src) { c = e / M; i = e % M; } else { i = e / b; c = e % b; }
             const int col = id * b + c;
@@ -636,7 +637,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const
     for (int half = 0; half < 2; ++half) {
         const int id = half == 0 ? rank : 2 * C - 1 - rank;
         double2* base = buf(half);
-        for (int e = tid; e < b * M; e += kJacobiThreads) {
+        for (int e = tid; e < b * M; e += nthreads) {
             int c, i;
             if (rows_of_src) { c = e / M; i = e % M; } else { i = e / b; c = e % b; }
             const int col = id * b + c;
@@ -644,7 +645,7 @@ __global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const
             if (cnorm2(x) < dust2) x = cmake(0, 0);
             base[size_t(c) * len + i] = x;
         }
-        for (int e = tid; e < b * Np; e += kJacobiThreads) {
+        for (int e = tid; e < b * Np; e += nthreads) {
             const int c = e / Np, i = e % Np;
             base[size_t(c) * len + M + i] = cmake(i == id * b + c ? 1.0 : 0.0, 0.0);
         }
@@ -697,14 +698,14 @@ __global__ void __launch_bounds__(kJacobiThreads, 1) jacobi_cluster_kernel(const
                 const int sbuf = rank == 1 ? rc->bot_buf : rc->top_buf;
                 const double2* rsrc = cluster.map_shared_rank(smem, srank) + size_t(sbuf) * blk;
                 double2* dst = buf(ctl.spare_buf);
-                for (size_t e = tid; e < blk; e += kJacobiThreads) dst[e] = rsrc[e];
+                for (size_t e = tid; e < blk; e += nthreads) dst[e] = rsrc[e];
             }
             cluster.sync();
             if (rank <= C - 2) {
                 const JacobiCtl* rc = cluster.map_shared_rank(&ctl, rank + 1);
                 const double2* rsrc = cluster.map_shared_rank(smem, rank + 1) + size_t(rc->bot_buf) * blk;
                 double2* dst = buf(rank == 0 ? ctl.bot_buf : ctl.top_buf);
-                for (size_t e = tid; e < blk; e += kJacobiThreads) dst[e] = rsrc[e];
+                for (size_t e = tid; e < blk; e += nthreads) dst[e] = rsrc[e];
             }
             // Block ids travel with the data.
             int new_top_id = ctl.top_id, new_bot_id = ctl.bot_id;
@@ -825,7 +826,7 @@ __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const Slot
         if (vals[i] > kSingularCutoff) ++rank;
         if (!isfinite(vals[i]) || vals[i] < 0.0) bad = true;
     }
-    int chi = N == 0 ? 0 : min(min(max(rank, 1), chi_max), min(S.rows, S.cols));
+    int chi = N == 0 ? 0 : min(min(max(rank, 1), J.chi_max > 0 ? J.chi_max : chi_max), min(S.rows, S.cols));
     if (mode == kJacobiRsvd) {
         // needs_f64_fallback (svd_guard.rs:58-76)
         bool fb = bad || chi == 0;

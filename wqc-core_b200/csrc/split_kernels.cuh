@@ -37,7 +37,8 @@ struct OneQubitOp {
     int count;  // gates applied in order
 };
 __global__ void apply_1q_kernel(const OneQubitOp* ops, const double2* mats, DeviceMps mps);
-__global__ void amplitude_zero_kernel(DeviceMps mps, double2* out);
+__global__ void amplitude_zero_kernel(DeviceMps mps, const int* seg, double2* out);
+__global__ void reset_sites_kernel(DeviceMps mps);
 __global__ void site_amplitudes_kernel(DeviceMps mps, int target, double2* out);
 __global__ void pauli_expectation_kernel(DeviceMps mps, const char* labels, int nterms, double2* scratch,
                                          int env_cap, double2* out);

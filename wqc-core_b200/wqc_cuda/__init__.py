@@ -45,6 +45,7 @@ EXPORTS = (
     "wqc_mps_upload_site", "wqc_mps_expectation_pauli", "wqc_mps_set_split_rule", "wqc_mps_split_count", "wqc_mps_split_records",
     "wqc_mps_peak_vram_bytes", "wqc_mps_backend_label", "wqc_mps_set_profiling", "wqc_mps_kernel_stats",
     "wqc_mps_reset_stats", "wqc_mps_stream", "wqc_schedule_gates", "wqc_mps_reset", "wqc_mps_debug_workspace",
+    "wqc_batch_create", "wqc_batch_apply_gates", "wqc_batch_amplitudes", "wqc_batch_slice_times",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
@@ -124,6 +125,11 @@ def lib():
         L.wqc_schedule_gates.argtypes = [U32, P, U32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                          U32, ctypes.POINTER(U32), ctypes.POINTER(U32)]
         L.wqc_mps_debug_workspace.argtypes = [P, U32, ctypes.c_int32, P, ctypes.c_uint64]
+        L.wqc_batch_create.argtypes = [P, U32, ctypes.POINTER(U32), ctypes.POINTER(U32), ctypes.c_int32, U32,
+                                       ctypes.POINTER(P)]
+        L.wqc_batch_apply_gates.argtypes = [P, P, ctypes.POINTER(U32)]
+        L.wqc_batch_amplitudes.argtypes = [P, D]
+        L.wqc_batch_slice_times.argtypes = [P, D]
         L.wqc_mps_stream.argtypes = [P]
         L.wqc_mps_stream.restype = P
         _LIB = L
@@ -356,6 +362,58 @@ class CudaMps:
         return int(lib().wqc_mps_stream(self._h) or 0)
 
 
+class CudaBatch(CudaMps):
+    """Many independent slices in one device state (wqc_batch_create): their
+    splits share waves; each slice keeps its own MpsState semantics."""
+
+    def __init__(self, qubits, chis, ctx: Context | None = None, max_concurrent_splits: int = 0,
+                 precision: int = PRECISION_FP64):
+        self.ctx = ctx or Context.shared()
+        self.qubits = np.ascontiguousarray(qubits, dtype=np.uint32)
+        self.chis = np.ascontiguousarray(chis, dtype=np.uint32)
+        self.n = int(self.qubits.sum())
+        self.chi = int(self.chis.max())
+        self.first_site = np.concatenate([[0], np.cumsum(self.qubits)[:-1]]).astype(np.int64)
+        u32 = ctypes.POINTER(ctypes.c_uint32)
+        h = ctypes.c_void_p()
+        _check(lib().wqc_batch_create(self.ctx._h, len(self.qubits), self.qubits.ctypes.data_as(u32),
+                                      self.chis.ctypes.data_as(u32), precision, max_concurrent_splits,
+                                      ctypes.byref(h)))
+        self._h = h
+
+    def apply_slices(self, gate_lists) -> None:
+        """gate_lists[s] are slice s's gates (qubits local to the slice)."""
+        lens = [len(g) for g in gate_lists]
+        offsets = np.zeros(len(lens) + 1, dtype=np.uint32)
+        offsets[1:] = np.cumsum(lens)
+        allg = np.ascontiguousarray(np.concatenate(gate_lists) if sum(lens) else np.zeros(0, GATE_DTYPE),
+                                    dtype=GATE_DTYPE)
+        _check(lib().wqc_batch_apply_gates(self._h, allg.ctypes.data if len(allg) else None,
+                                           offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))))
+
+    def amplitudes(self) -> np.ndarray:
+        out = np.zeros(len(self.qubits), dtype=np.complex128)
+        _check(lib().wqc_batch_amplitudes(self._h, _dp(out.view(np.float64))))
+        return out
+
+    def slice_times_ms(self) -> np.ndarray:
+        out = np.zeros(len(self.qubits))
+        _check(lib().wqc_batch_slice_times(self._h, _dp(out)))
+        return out
+
+    def slice_records(self):
+        """Split records of each slice (left_site local to the slice), in order."""
+        rec = self.split_records()
+        site = rec["left_site"].astype(np.int64)
+        sl = np.searchsorted(self.first_site, site, side="right") - 1
+        out = []
+        for s in range(len(self.qubits)):
+            r = rec[sl == s].copy()
+            r["left_site"] -= self.first_site[s]
+            out.append(r)
+        return out
+
+
 def _mat4(entries) -> np.ndarray:
     m = np.zeros((2, 2, 2, 2), dtype=np.complex128)
     for idx, v in entries:
@@ -394,5 +452,5 @@ def split_flops(rec) -> float:
     return f
 
 
-__all__ = ["CudaMps", "Context", "WqcCudaError", "lib", "build", "run", "workspace_bytes", "split_flops",
+__all__ = ["CudaMps", "CudaBatch", "Context", "WqcCudaError", "lib", "build", "run", "workspace_bytes", "split_flops",
            "svd_flops", "CNOT4", "CZ4", "SWAP4", "EXPORTS", "KERNEL_KINDS", "math"]
