@@ -184,6 +184,35 @@ WQC_API wqc_status wqc_mps_upload_site(wqc_mps* mps, uint32_t site, uint32_t l, 
 WQC_API wqc_status wqc_mps_expectation_pauli(wqc_mps* mps, const char* labels, const double* coeffs, uint32_t nterms,
                                      double out[2]);
 
+/* The same sum for an MPS held in the caller's own device memory, computed
+ * without allocating any device memory.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot let a
+ * library call cudaMalloc: hosts whose allocator already owns the GPU's
+ * memory (a PyTorch caching allocator, a fixed per-tenant budget), where
+ * cudaMalloc may fail although their pool has room and cudaFree would
+ * synchronise the whole device.
+ *
+ * sites: device memory of the current device, 16-byte aligned, holding
+ * qubit_count * site_stride complex128 values (re,im pairs); site q starts at
+ * complex element q * site_stride and is [l][2][r] row-major, r =
+ * bond_dims[q] and l = bond_dims[q - 1] (1 for q = 0), the layout that
+ * wqc_mps_download_site returns.  bond_dims, labels, coeffs and out are host
+ * memory.  stream: a cudaStream_t of the current device (NULL = the legacy
+ * default stream); the call returns once its work on it has finished.
+ *
+ * Working memory is one array of 16 MiB + 128 KiB that the library holds in
+ * every GPU where this code is loaded, until the process exits.  Limits:
+ * bond dimensions 1..256 and at most 1024 qubits; larger sizes are rejected
+ * with WQC_ERR_INVALID or WQC_ERR_INVALID_QUBIT_COUNT and a message naming
+ * the limit.  The first call on a device looks up that device's address of
+ * the array (and may load this code onto the GPU); make that first call
+ * before any stream capture.  All calls on a device share the array, which
+ * keeps the last call's contents; calls that overlap on the GPU (from two
+ * host threads at once) race on it, so serialise them. */
+WQC_API wqc_status wqc_expectation_pauli_noalloc(const double* sites, uint64_t site_stride, const uint32_t* bond_dims,
+                                                 uint32_t qubit_count, const char* labels, const double* coeffs,
+                                                 uint32_t nterms, void* stream, double out[2]);
+
 /* Diagnostics: copy one split-workspace buffer of `slot` (the last wave's
  * job in that slot) to host memory, at most `bytes`.  which: 0 theta
  * (rows x cols, row-major), 1 Omega, 2 A*Omega, 3 A^H*(A*Omega), 4 Y then

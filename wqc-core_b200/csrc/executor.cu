@@ -827,6 +827,12 @@ wqc_status sync_status(wqc_mps* m) {
 
 }  // namespace
 
+// Lets entry points defined in other files of the library set the message
+// that wqc_cuda_last_error returns.
+namespace wqc {
+wqc_status record_error(wqc_status code, const std::string& msg) { return fail(code, msg); }
+}  // namespace wqc
+
 // ===========================================================================
 // C ABI
 // ===========================================================================

@@ -46,6 +46,7 @@ EXPORTS = (
     "wqc_mps_peak_vram_bytes", "wqc_mps_backend_label", "wqc_mps_set_profiling", "wqc_mps_kernel_stats",
     "wqc_mps_reset_stats", "wqc_mps_stream", "wqc_schedule_gates", "wqc_mps_reset", "wqc_mps_debug_workspace",
     "wqc_batch_create", "wqc_batch_apply_gates", "wqc_batch_amplitudes", "wqc_batch_slice_times",
+    "wqc_expectation_pauli_noalloc",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
@@ -132,6 +133,8 @@ def lib():
         L.wqc_batch_slice_times.argtypes = [P, D]
         L.wqc_mps_stream.argtypes = [P]
         L.wqc_mps_stream.restype = P
+        L.wqc_expectation_pauli_noalloc.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(U32), U32, ctypes.c_char_p, D,
+                                                    U32, P, D]
         _LIB = L
     return _LIB
 
@@ -360,6 +363,23 @@ class CudaMps:
 
     def stream(self) -> int:
         return int(lib().wqc_mps_stream(self._h) or 0)
+
+
+def expectation_pauli_noalloc(sites_ptr: int, site_stride: int, bond_dims, labels, coeffs, stream: int = 0) -> complex:
+    """Sum_t coeff_t <psi|P_t|psi> for an MPS in the caller's own device memory
+    (wqc_expectation_pauli_noalloc): the call allocates no device memory.
+    sites_ptr is a device address on the current device holding
+    len(bond_dims) sites of site_stride complex128 values each, site q laid
+    out [l][2][r]; stream is a cudaStream_t handle (0 = legacy default)."""
+    dims = np.ascontiguousarray(bond_dims, dtype=np.uint32)
+    joined = "".join(labels).encode()
+    c = _c128(coeffs)
+    out = np.zeros(2)
+    _check(lib().wqc_expectation_pauli_noalloc(sites_ptr or None, site_stride,
+                                               dims.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(dims),
+                                               joined, _dp(c.view(np.float64)), len(labels), stream or None,
+                                               _dp(out)))
+    return complex(out[0], out[1])
 
 
 class CudaBatch(CudaMps):
