@@ -108,6 +108,93 @@ def oracle_sample(w, budget_s: float, threads: int = 1, skip_layers: int = 0):
 SATURATED_LAYERS = {"config1": 10, "config0": 4}
 
 
+def oracle_batch_sample(slices, budget_s: float, threads: int):
+    """CPU leg of the batching form: thread t runs slice t from |0...0> on the
+    oracle, gate chunk by gate chunk, until `budget_s` seconds; returns (splits
+    done by all threads, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.lib()
+    done = [0] * threads
+    secs = [0.0] * threads
+    barrier = threading.Barrier(threads)
+
+    def worker(t):
+        s = slices[t % len(slices)]
+        m = O.OracleMps(s.n, s.chi)
+        barrier.wait()
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(s.gates) and time.perf_counter() - t0 < budget_s:
+            m.apply_gates(s.gates[i:i + 16])
+            i += 16
+        secs[t] = time.perf_counter() - t0
+        done[t] = len(m.records())
+
+    ths = [threading.Thread(target=worker, args=(t,)) for t in range(threads)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    return sum(done), max(secs)
+
+
+def batch_leg(W, torch, ctx, count: int, flush, cpu_budget: float) -> dict:
+    """The batching form: `count` independent slices (width U[20,60], depth
+    U[10,50], chi_max from {16,32,64,128}) in one device state, one pass from
+    |0...0> to every slice's <0...0|psi>.  Latency of a slice = device time
+    from the start of the pass to the end of the wave holding its last split."""
+    slices = C.config2_slices(count)
+    b = W.CudaBatch([s.n for s in slices], [s.chi for s in slices], ctx=ctx)
+    stream = torch.cuda.ExternalStream(b.stream())
+    gate_lists = [s.gates for s in slices]
+    b.set_profiling(True)
+    flush.fill_(float(np.random.random()))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    b.apply_slices(gate_lists)
+    amps = b.amplitudes()
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    dev_s = e0.elapsed_time(e1) * 1e-3
+    lat = np.sort(b.slice_times_ms())
+    splits = int(b.split_count())
+    stats = b.kernel_stats()
+    out = {
+        "workload": f"{count} slices: width U[20,60], depth U[10,50], chi_max U{{16,32,64,128}}, RY/RZ + CNOT "
+                    f"brickwork, own seed each; plain FP64 (complex128), split rule reference",
+        "slices": count,
+        "slices_per_s": count / dev_s,
+        "e2e_slices_per_s": count / wall,
+        "p50_ms": float(np.percentile(lat, 50)),
+        "p99_ms": float(np.percentile(lat, 99)),
+        "applies": splits,
+        "applies_per_s": splits / dev_s,
+        "gpu_launches": stats["total_launches"],
+        "peak_vram_bytes": b.peak_vram_bytes(),
+        "finite_amplitudes": bool(np.all(np.isfinite(amps))),
+    }
+    b.close()
+    if cpu_budget > 0:
+        threads = os.cpu_count() or 1
+        done, secs = oracle_batch_sample(slices, cpu_budget, threads)
+        per_slice = splits / count
+        out["cpu_baseline"] = {
+            "value": done / secs / per_slice,
+            "unit": "slices/s",
+            "cores": threads,
+            "kind": "port",
+            "sample": f"FP64 restatement, one slice per thread on {threads} threads (slices 0..{threads - 1} "
+                      f"from their start, {cpu_budget:.0f} s): {done} splits in {secs:.1f} s, converted at the "
+                      f"batch's mean of {per_slice:.0f} splits per slice",
+        }
+    return out
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -332,7 +419,9 @@ def run_cuda(args) -> None:
                 "peak": peak,
                 "unit": "TFLOP/s",
                 "frac": (achieved / peak) if (achieved and peak) else None,
-                "traffic": None,
+                "traffic": 334848,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one saturated launch "
+                                  "(profiles/jacobi_svd_random50_d40_chi128.md); W and Z stay in shared memory",
                 "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "flops_per_step": flops / args.steps,
                 "kernel_ms_per_step": jac_ms / args.steps,
@@ -358,6 +447,9 @@ def run_cuda(args) -> None:
                           f"layers untimed (bonds reach chi_max), then gates {win[0]}..{win[1]} of {len(w.gates)} "
                           f"({s} splits) timed in {secs:.1f} s",
             }
+        if world == 1 and args.batch_slices > 0:
+            line["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush,
+                                      0.0 if args.no_cpu_baseline else args.cpu_budget)
         print(json.dumps(line), flush=True)
     m.close()
     if dist is not None:
@@ -376,6 +468,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--reference-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-slices", type=int, default=512,
+                    help="slices of the batching-form leg run once after the timed steps (0 = skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

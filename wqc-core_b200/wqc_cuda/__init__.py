@@ -323,6 +323,9 @@ class CudaMps:
         _check(lib().wqc_mps_expectation_pauli(self._h, joined, _dp(c.view(np.float64)), len(labels), _dp(out)))
         return complex(out[0], out[1])
 
+    def split_count(self) -> int:
+        return int(lib().wqc_mps_split_count(self._h))
+
     def split_records(self) -> np.ndarray:
         k = lib().wqc_mps_split_count(self._h)
         out = np.zeros(k, dtype=SPLIT_INFO_DTYPE)
