@@ -479,8 +479,6 @@ __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const 
 // 174-199), with column dot products reduced by warp shuffles.
 // ---------------------------------------------------------------------------
 struct JacobiCtl {
-    int top_buf, bot_buf, spare_buf;
-    int top_id, bot_id;
     int rot;
     unsigned long long relmax_bits;  // largest |gamma|/sqrt(alpha beta) seen this sweep (non-negative double bits)
     double fro_part;
@@ -523,15 +521,27 @@ __device__ __forceinline__ int jacobi_rotate(double2* xp, double2* xq, int M, in
         gr += __shfl_xor_sync(0xffffffffu, gr, o);
         gi += __shfl_xor_sync(0xffffffffu, gi, o);
     }
-    const double g = hypot(gr, gi);
-    const double scale = sqrt(a) * sqrt(bb);
-    if (scale <= noise_floor) return 0;
-    relmax = fmax(relmax, g / scale);
-    if (g == 0.0 || g <= tol * scale) return 0;
-    const double pr = gr / g, pi = gi / g;
-    const double zeta = (bb - a) / (2.0 * g);
-    const double t = copysign(1.0, zeta) / (fabs(zeta) + hypot(1.0, zeta));
-    const double c = 1.0 / sqrt(1.0 + t * t);
+    // Squared forms keep the dependent chain short: |gamma|^2 against
+    // tol^2 alpha beta, one reciprocal square root for the phase.
+    const double g2 = fma(gr, gr, gi * gi);
+    const double ab = a * bb;
+    if (ab <= noise_floor * noise_floor) return 0;
+    relmax = fmax(relmax, g2 / ab);  // squared ratio; the caller compares with squared bounds
+    if (g2 == 0.0 || g2 <= tol * tol * ab) return 0;
+    double pr, pi, zeta;
+    if (g2 > 1e-290) {
+        const double inv_g = rsqrt(g2);
+        pr = gr * inv_g;
+        pi = gi * inv_g;
+        zeta = 0.5 * (bb - a) * inv_g;
+    } else {  // |gamma|^2 near the subnormal range: hypot keeps the phase of unit modulus
+        const double g = hypot(gr, gi);
+        pr = gr / g;
+        pi = gi / g;
+        zeta = (bb - a) / (2.0 * g);
+    }
+    const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
+    const double c = rsqrt(fma(t, t, 1.0));
     const double s = c * t;
     // With w = s * phase the rephased rotation (svd_guard.rs:189-197) is
     // xp' = c xp - conj(w) xq,  xq' = w xp + c xq   (|phase| = 1).
@@ -542,6 +552,22 @@ __device__ __forceinline__ int jacobi_rotate(double2* xp, double2* xq, int M, in
         xq[r] = cmake(fma(wr, u.x, fma(-wi, u.y, c * v.x)), fma(wr, u.y, fma(wi, u.x, c * v.y)));
     }
     return 1;
+}
+
+// Block copy from another CTA's shared memory: eight 16-byte loads in flight
+// per thread before the stores.
+__device__ __forceinline__ void dsmem_copy(double2* __restrict__ dst, const double2* __restrict__ src, size_t n,
+                                           int tid, int nthreads) {
+    size_t e = tid;
+    const size_t st = nthreads;
+    for (; e + 7 * st < n; e += 8 * st) {
+        double2 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = src[e + u * st];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) dst[e + u * st] = v[u];
+    }
+    for (; e < n; e += st) dst[e] = src[e];
 }
 
 __device__ __forceinline__ void jacobi_task(const SplitJob& J, const SplitState& S, const SlotBuffers& B, int mode,
@@ -586,7 +612,6 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
     const int Np = ((N + quantum - 1) / quantum) * quantum;
     const int b = Np / (2 * C);
     const int len = M + Np;
-    const int nbuf = C == 1 ? 2 : 3;
 
     extern __shared__ __align__(16) double2 smem[];
     __shared__ JacobiCtl ctl;
@@ -596,14 +621,17 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
     auto buf = [&](int k) { return smem + size_t(k) * b * len; };
     __shared__ double red[kJacobiThreads / 32];
 
-    if (tid == 0) {
-        ctl.top_buf = 0;
-        ctl.bot_buf = 1;
-        ctl.spare_buf = nbuf - 1;
-        ctl.top_id = rank;
-        ctl.bot_id = 2 * C - 1 - rank;
-        ctl.rot = 0;
-    }
+    if (tid == 0) ctl.rot = 0;
+    // Buffer roles and block ids after xk block exchanges, the same on every
+    // CTA without reading a neighbour's state: CTA 0 keeps its top block
+    // (position 0) in buffer 0 and receives into buffer 1; every other CTA
+    // turns its (top, bottom, spare) buffers one place per exchange; the
+    // blocks at positions 1 .. 2C-1 move one position on per exchange, so
+    // position p holds block circle_at(p, xk, 2C).
+    int xk = 0;
+    auto top_buf_of = [&](int r, int k) { return r == 0 ? 0 : (3 - k % 3) % 3; };
+    auto bot_buf_of = [&](int r, int k) { return r == 0 ? 1 : (4 - k % 3) % 3; };
+    auto spare_buf_of = [&](int k) { return (5 - k % 3) % 3; };
     // Frobenius norm over the columns this CTA loads, then over the cluster.
     auto src_at = [&](int i, int col) -> double2 {
         return rows_of_src ? cconj(src[size_t(col) * ld + i]) : src[size_t(i) * ld + col];
@@ -671,7 +699,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
             for (int pq = wid; pq < b; pq += nwarps) {
                 const bool top = pq < b / 2;
                 const int i = top ? pq : pq - b / 2;
-                double2* base = buf(top ? ctl.top_buf : ctl.bot_buf);
+                double2* base = buf(top ? top_buf_of(rank, xk) : bot_buf_of(rank, xk));
                 const int e1 = circle_at(i, step, b), e2 = circle_at(b - 1 - i, step, b);
                 my_rot += jacobi_rotate(base + size_t(e1) * len, base + size_t(e2) * len, M, len, tol, noise_floor, lane, my_rel);
             }
@@ -680,8 +708,8 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
         // Cross pairs between the two blocks, 2C-1 block steps.
         for (int bs = 0; bs < 2 * C - 1; ++bs) {
             for (int k = 0; k < b; ++k) {
-                double2* tb = buf(ctl.top_buf);
-                double2* bb = buf(ctl.bot_buf);
+                double2* tb = buf(top_buf_of(rank, xk));
+                double2* bb = buf(bot_buf_of(rank, xk));
                 for (int i = wid; i < b; i += nwarps) {
                     const int e2 = (i + k) % b;
                     my_rot += jacobi_rotate(tb + size_t(i) * len, bb + size_t(e2) * len, M, len, tol, noise_floor, lane, my_rel);
@@ -689,48 +717,30 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
                 __syncthreads();
             }
             if (C == 1) continue;
-            // Circle rotation of blocks between CTAs (pull protocol, one spare buffer).
-            cluster.sync();  // all block-step rotations are finished and roles are current
+            // Circle rotation of blocks between CTAs (pull protocol, one spare
+            // buffer, two cluster barriers): CTA r >= 1 first pulls the block
+            // that moves into its top position into its spare buffer; after
+            // the second barrier, when every such pull is done, CTA r <= C-2
+            // pulls the block that moves into its bottom position over its
+            // old top (CTA 0: over its old bottom).  No barrier is needed
+            // after the second pull: a neighbour still reading this CTA's old
+            // bottom reads what is now its spare buffer, which nothing writes
+            // before the next exchange's first barrier, and the roles are
+            // computed locally instead of read across the cluster.
+            cluster.sync();  // all block-step rotations are finished
             const size_t blk = size_t(b) * len;
             if (rank >= 1) {
                 const int srank = rank == 1 ? 0 : rank - 1;
-                const JacobiCtl* rc = cluster.map_shared_rank(&ctl, srank);
-                const int sbuf = rank == 1 ? rc->bot_buf : rc->top_buf;
-                const double2* rsrc = cluster.map_shared_rank(smem, srank) + size_t(sbuf) * blk;
-                double2* dst = buf(ctl.spare_buf);
-                for (size_t e = tid; e < blk; e += nthreads) dst[e] = rsrc[e];
+                const int sbuf = rank == 1 ? bot_buf_of(0, xk) : top_buf_of(srank, xk);
+                dsmem_copy(buf(spare_buf_of(xk)), cluster.map_shared_rank(smem, srank) + size_t(sbuf) * blk, blk,
+                           tid, nthreads);
             }
             cluster.sync();
             if (rank <= C - 2) {
-                const JacobiCtl* rc = cluster.map_shared_rank(&ctl, rank + 1);
-                const double2* rsrc = cluster.map_shared_rank(smem, rank + 1) + size_t(rc->bot_buf) * blk;
-                double2* dst = buf(rank == 0 ? ctl.bot_buf : ctl.top_buf);
-                for (size_t e = tid; e < blk; e += nthreads) dst[e] = rsrc[e];
+                const double2* rsrc = cluster.map_shared_rank(smem, rank + 1) + size_t(bot_buf_of(rank + 1, xk)) * blk;
+                dsmem_copy(buf(rank == 0 ? bot_buf_of(0, xk) : top_buf_of(rank, xk)), rsrc, blk, tid, nthreads);
             }
-            // Block ids travel with the data.
-            int new_top_id = ctl.top_id, new_bot_id = ctl.bot_id;
-            if (rank >= 1) {
-                const JacobiCtl* rc = cluster.map_shared_rank(&ctl, rank == 1 ? 0 : rank - 1);
-                new_top_id = rank == 1 ? rc->bot_id : rc->top_id;
-            }
-            if (rank <= C - 2) {
-                new_bot_id = cluster.map_shared_rank(&ctl, rank + 1)->bot_id;
-            } else {
-                new_bot_id = ctl.top_id;
-            }
-            cluster.sync();
-            if (tid == 0) {
-                if (rank == 0) {
-                    ctl.bot_id = new_bot_id;
-                } else {
-                    const int ot = ctl.top_buf, ob = ctl.bot_buf, os = ctl.spare_buf;
-                    ctl.top_buf = os;
-                    ctl.bot_buf = ot;
-                    ctl.spare_buf = ob;
-                    ctl.top_id = new_top_id;
-                    ctl.bot_id = new_bot_id;
-                }
-            }
+            ++xk;
             __syncthreads();
         }
         // Cluster-wide rotation count decides convergence.
@@ -756,7 +766,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
         // sweep orthogonal to 1e-8: one-sided Jacobi converges quadratically,
         // so this sweep left them orthogonal to about 1e-16, below the
         // rotation tolerance, and a verification sweep would rotate nothing.
-        if (total == 0 || relmax < 1e-8) {
+        if (total == 0 || relmax < 1e-16) {  // relmax holds squared ratios
             converged = true;
             break;
         }
@@ -768,8 +778,8 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
     }
     // Write back: W columns, Z columns (first N rows) and column norms.
     for (int half = 0; half < 2; ++half) {
-        const int id = half == 0 ? ctl.top_id : ctl.bot_id;
-        const double2* base = buf(half == 0 ? ctl.top_buf : ctl.bot_buf);
+        const int id = circle_at(half == 0 ? rank : 2 * C - 1 - rank, xk, 2 * C);
+        const double2* base = buf(half == 0 ? top_buf_of(rank, xk) : bot_buf_of(rank, xk));
         for (int c = wid; c < b; c += nwarps) {
             const int col = id * b + c;
             if (col >= N) continue;
