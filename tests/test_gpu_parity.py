@@ -187,6 +187,65 @@ def test_range_finder_split_matches_oracle_on_rank_24_theta(cuda_ctx):
     assert abs(float(info["discarded_weight"]) - float(ref["discarded_weight"])) <= DISC_ATOL
 
 
+def test_range_finder_fallback_matches_oracle(cuda_ctx):
+    """needs_f64_fallback (svd_guard.rs:58-76, mps.rs:1027-1032): a 192x192
+    theta of rank 48 with singular values graded from 3 to 0.3.  The range
+    finder's B keeps 64 rows of rounding noise, which the oracle puts inside
+    the (1e-14, 1e-10] band for every scale of theta from 0.1 to 100 (3 is
+    in the middle), so the ambiguity test sends the split to the exact SVD,
+    whose own noise (~1e-15) stays far below the 1e-12 cut: path
+    RSVD_FALLBACK and chi 48 on both sides, and the kept product is unique."""
+    rng = np.random.default_rng(7)
+    rank, bond = 48, 96
+    ul, _ = np.linalg.qr(rng.normal(size=(2 * bond, rank)) + 1j * rng.normal(size=(2 * bond, rank)))
+    vr, _ = np.linalg.qr(rng.normal(size=(2 * bond, rank)) + 1j * rng.normal(size=(2 * bond, rank)))
+    sig = 3.0 * np.geomspace(1.0, 0.1, rank)
+    outer = _random_sites(rng, [(1, bond), (bond, 1)])
+    sites = [outer[0], (ul * sig).reshape(bond, 2, rank), vr.conj().T.reshape(rank, 2, bond), outer[1]]
+    m = W.CudaMps(4, bond, ctx=cuda_ctx)
+    o = O.OracleMps(4, bond)
+    for i, s in enumerate(sites):
+        m.set_site(i, s)
+        o.set_site(i, s)
+    eye = np.eye(4, dtype=np.complex128)
+    info = m.apply_two_qubit_at_positions(1, 2, eye, True, want_info=True)
+    o.apply_2q_at(1, eye, True)
+    ref = o.records()[0]
+    assert int(ref["path"]) == 2 and int(info["path"]) == 2, (ref, info)
+    assert int(info["chi"]) == int(ref["chi"]) == rank, (ref, info)
+    got, want = _theta(m.site(1), m.site(2)), _theta(o.site(1), o.site(2))
+    err = np.abs(got - want).max() / np.abs(want).max()
+    assert err <= 1e-12, err
+    assert abs(float(info["discarded_weight"]) - float(ref["discarded_weight"])) <= DISC_ATOL
+
+
+def test_exact_and_range_finder_splits_in_one_wave(cuda_ctx):
+    """One level holding a range-finder split (sites 1-2, the rank-24 theta)
+    and an exact split (sites 4-5): the exact SVD runs on the state's second
+    stream while the range finder runs on the first.  Both splits, the bonds
+    and the amplitude must equal the oracle's."""
+    rng = np.random.default_rng(41)
+    sites = _random_sites(rng, [(1, 96), (96, 12), (12, 96), (96, 8), (8, 16), (16, 8), (8, 1)])
+    gates = C.gates_array([C.g2(C.CNOT, 1, 2), C.g2(C.CZ, 4, 5)])
+    _, level, nlev = W.schedule(7, gates)
+    assert nlev == 1 and list(level) == [0, 0]
+    m = W.CudaMps(7, 96, ctx=cuda_ctx)
+    o = O.OracleMps(7, 96)
+    for i, s in enumerate(sites):
+        m.set_site(i, s)
+        o.set_site(i, s)
+    m.apply_gates(gates)
+    o.apply_gates(gates)
+    got, ref = m.split_records(), o.records()
+    assert list(ref["path"]) == [1, 0]
+    assert_records_match(got, ref)
+    assert list(m.bond_dims()) == list(o.bond_dims())
+    for p in (1, 4):
+        a, b = _theta(m.site(p), m.site(p + 1)), _theta(o.site(p), o.site(p + 1))
+        assert np.abs(a - b).max() / np.abs(b).max() <= 1e-12, p
+    assert rel_err(m.amplitude_zero(), o.amplitude_zero()) < AMP_RTOL
+
+
 @pytest.mark.parametrize("bond", [64, 128])
 def test_exact_split_of_full_rank_theta_matches_oracle(cuda_ctx, bond):
     """2*bond x 2*bond full-rank theta through the exact rule (cluster-resident

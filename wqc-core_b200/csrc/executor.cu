@@ -177,6 +177,10 @@ struct wqc_mps {
     bool reject = false;
     bool exact_only = false;  // WQC_SPLIT_RULE_EXACT
     cudaStream_t stream = nullptr;
+    // Second stream of a wave: the exact-path SVDs run there while the range
+    // finder runs on `stream`; fork after the merge, join before the absorb.
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     // device state
     double2* site_pool = nullptr;
     std::vector<double2*> site_ptr;  // device address of every site (capacity chi_slice * 2 * chi_slice)
@@ -312,16 +316,17 @@ struct Timed {
     wqc_mps* m;
     int kind;
     cudaEvent_t a = nullptr, b = nullptr;
-    Timed(wqc_mps* mm, int k) : m(mm), kind(k) {
+    cudaStream_t s;
+    Timed(wqc_mps* mm, int k, cudaStream_t on = nullptr) : m(mm), kind(k), s(on ? on : mm->stream) {
         if (m->profiling) {
             a = get_event(m);
             b = get_event(m);
-            cudaEventRecord(a, m->stream);
+            cudaEventRecord(a, s);
         }
     }
     ~Timed() {
         if (m->profiling) {
-            cudaEventRecord(b, m->stream);
+            cudaEventRecord(b, s);
             m->events.push_back({kind, {a, b}});
         }
     }
@@ -575,12 +580,12 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 w.max_cols = std::max(w.max_cols, cols);
                 w.max_ell = std::max(w.max_ell, ell);
                 const int nj_wave = int(j1 - j0);
-                add(kJacobiExact,
-                    choose_cluster(std::max(rows, cols), std::min(rows, cols), m->ctx->max_cluster, nj_wave,
-                                   m->ctx->sm_count),
-                    local);
+                const int c_exact = choose_cluster(std::max(rows, cols), std::min(rows, cols), m->ctx->max_cluster,
+                                                   nj_wave, m->ctx->sm_count);
+                add(kJacobiExact, c_exact, local);
                 if (rs) {
                     w.any_rsvd = true;
+                    add(kJacobiFallback, c_exact, local);
                     add(kJacobiRsvd, choose_cluster(cols, ell, m->ctx->max_cluster, nj_wave, m->ctx->sm_count), local);
                 }
             }
@@ -595,7 +600,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 for (int local : g.second) {
                     int rows, cols, ell;
                     shape(j0 + local, rows, cols, ell);
-                    const size_t sz = gr.mode == kJacobiExact
+                    const size_t sz = gr.mode != kJacobiRsvd
                                           ? jacobi_smem_bytes(std::max(rows, cols), std::min(rows, cols), std::max(gr.C, 1))
                                           : jacobi_smem_bytes(cols, ell, std::max(gr.C, 1));
                     sm = std::max(sm, sz);
@@ -605,7 +610,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 for (int local : g.second) {
                     int rows, cols, ell;
                     shape(j0 + local, rows, cols, ell);
-                    const int N = gr.mode == kJacobiExact ? std::min(rows, cols) : ell;
+                    const int N = gr.mode != kJacobiRsvd ? std::min(rows, cols) : ell;
                     const int Cc = std::max(gr.C, 1);
                     bmax = std::max(bmax, round_up(N, 4 * Cc) / (2 * Cc));
                 }
@@ -713,17 +718,17 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
             merge_gate_kernel<<<g, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);
             count_launch(m, 1);
         }
-        auto jacobi = [&](int mode) -> wqc_status {
+        auto jacobi = [&](int mode, cudaStream_t on) -> wqc_status {
             for (const Group& gr : w.groups) {
                 if (gr.mode != mode) continue;
                 if (gr.C < 1)
                     return fail(WQC_ERR_INVALID, "two-site matrix too large for the cluster-resident Jacobi SVD");
-                Timed t(m, 0);
+                Timed t(m, 0, on);
                 cudaLaunchConfig_t cfg = {};
                 cfg.gridDim = dim3(gr.count * gr.C);
                 cfg.blockDim = dim3(gr.threads);
                 cfg.dynamicSmemBytes = gr.smem;
-                cfg.stream = m->stream;
+                cfg.stream = on;
                 cudaLaunchAttribute attr[1];
                 attr[0].id = cudaLaunchAttributeClusterDimension;
                 attr[0].val.clusterDim.x = gr.C;
@@ -738,6 +743,22 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
             }
             return WQC_OK;
         };
+        // Exact-path SVDs on the side stream, concurrently with the range
+        // finder below (different jobs, different slots and records).
+        const bool fork = w.any_rsvd;
+        cudaStream_t xs = fork ? m->side : m->stream;
+        if (fork) {
+            CUDA_TRY(cudaEventRecord(m->fork_ev, m->stream));
+            CUDA_TRY(cudaStreamWaitEvent(m->side, m->fork_ev, 0));
+        }
+        if (wqc_status s = jacobi(kJacobiExact, xs)) return s;
+        {
+            Timed t(m, 4, xs);
+            finalize_kernel<<<nj, 256, 0, xs>>>(d_jobs, m->d_state, m->d_slots, kJacobiExact, m->chi, m->d_records,
+                                                m->d_status);
+            count_launch(m, 4);
+        }
+        if (fork) CUDA_TRY(cudaEventRecord(m->join_ev, m->side));
         if (w.any_rsvd) {
             {
                 Timed t(m, 2);
@@ -773,23 +794,27 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                 rsvd_gemm_kernel<<<dim3(tc, te, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageB);
                 for (int k = 0; k < 6; ++k) count_launch(m, 2);
             }
-            if (wqc_status s = jacobi(kJacobiRsvd)) return s;
+            if (wqc_status s = jacobi(kJacobiRsvd, m->stream)) return s;
             {
                 Timed t(m, 4);
                 finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiRsvd, m->chi,
                                                             m->d_records, m->d_status);
                 count_launch(m, 4);
             }
+            if (wqc_status s = jacobi(kJacobiFallback, m->stream)) return s;
+            {
+                Timed t(m, 4);
+                finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiFallback, m->chi,
+                                                            m->d_records, m->d_status);
+                count_launch(m, 4);
+            }
         }
-        if (wqc_status s = jacobi(kJacobiExact)) return s;
+        if (fork) CUDA_TRY(cudaStreamWaitEvent(m->stream, m->join_ev, 0));
         {
             Timed t(m, 4);
-            finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiExact, m->chi,
-                                                        m->d_records, m->d_status);
             const int per = std::max(w.max_rows, w.max_cols) * std::min(m->chi, std::max(w.max_rows, w.max_cols));
             const int gx = std::max(1, std::min(128, per / 256));
             absorb_kernel<<<dim3(gx, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);
-            count_launch(m, 4);
             count_launch(m, 4);
         }
         if (track) CUDA_TRY(cudaEventRecord(m->wave_done[wi], m->stream));
@@ -944,6 +969,10 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
         return st;
     };
     if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "stream"));
+    if (cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "stream"));
+    if (cudaEventCreateWithFlags(&m->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&m->join_ev, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(WQC_ERR_CUDA, "event"));
     if (cudaEventCreateWithFlags(&m->stage_done, cudaEventDisableTiming) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "event"));
     cudaEventRecord(m->stage_done, m->stream);
     // Budget check before any large allocation (mps.rs:36-48 analogue).
@@ -1080,6 +1109,9 @@ void wqc_mps_destroy(wqc_mps* m) {
     }
     for (auto e : m->event_pool) cudaEventDestroy(e);
     if (m->stage_done) cudaEventDestroy(m->stage_done);
+    if (m->fork_ev) cudaEventDestroy(m->fork_ev);
+    if (m->join_ev) cudaEventDestroy(m->join_ev);
+    if (m->side) cudaStreamDestroy(m->side);
     if (m->stream) cudaStreamDestroy(m->stream);
     delete m;
 }

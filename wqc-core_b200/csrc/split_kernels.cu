@@ -588,7 +588,11 @@ __device__ __forceinline__ void jacobi_task(const SplitJob& J, const SplitState&
 }
 
 __device__ __forceinline__ bool jacobi_active(const SplitState& S, int mode) {
-    return mode == kJacobiRsvd ? S.use_rsvd != 0 : S.need_exact != 0;
+    if (mode == kJacobiRsvd) return S.use_rsvd != 0;
+    // The exact path's two modes never overlap: prepare sets path EXACT, and a
+    // fallback changes a range-finder split's path to RSVD_FALLBACK only.
+    if (mode == kJacobiExact) return S.need_exact != 0 && S.path == WQC_SPLIT_EXACT;
+    return S.need_exact != 0 && S.path == WQC_SPLIT_RSVD_FALLBACK;
 }
 
 __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const SplitJob* jobs, const SplitState* st,

@@ -6,7 +6,9 @@
 namespace wqc {
 
 enum { kStageY0 = 0, kStageZ = 1, kStageY = 2, kStageB = 3 };
-enum { kJacobiRsvd = 0, kJacobiExact = 1 };
+// Jacobi / finalize modes: the range finder's B^H; theta of a split that takes
+// the exact path from the start; theta of a range-finder split that fell back.
+enum { kJacobiRsvd = 0, kJacobiExact = 1, kJacobiFallback = 2 };
 constexpr int kJacobiThreads = 512;  // 16 warps: one column pair per warp per step (blocks of <= 16 pairs)
 
 __global__ void prepare_kernel(const SplitJob* jobs, SplitState* st, int njobs, DeviceMps mps);
