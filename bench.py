@@ -140,13 +140,57 @@ def oracle_batch_sample(slices, budget_s: float, threads: int):
     return sum(done), max(secs)
 
 
-def batch_leg(W, torch, ctx, count: int, flush, cpu_budget: float) -> dict:
+def precision_leg(W, torch, ctx, w, rule, steps: int, flush, fp64_value: float) -> dict:
+    """The precision form (WQC_PRECISION_FP32: complex64 Jacobi columns, FP64
+    rotation parameters, tests and norms) on the same circuit and steps, and
+    its amplitude error on the 16-qubit chi 32 brickwork against the plain
+    FP64 form (itself within 1e-12 of the FP64 oracle there)."""
+    m = W.CudaMps(w.n, w.chi, ctx=ctx, precision=W.PRECISION_FP32)
+    m.set_split_rule(rule)
+    stream = torch.cuda.ExternalStream(m.stream())
+    total_ms, splits = 0.0, 0
+    for k in range(steps + 1):
+        m.reset()
+        flush.fill_(float(np.random.random()))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.apply_gates(w.gates)
+        m.amplitude_at_compact_zero()
+        e1.record(stream)
+        e1.synchronize()
+        if k > 0:  # the first pass is a warm-up
+            total_ms += e0.elapsed_time(e1)
+            splits += m.split_count()
+    m.close()
+    value = splits / (total_ms * 1e-3)
+    w0 = C.config0()
+    amps = []
+    for prec in (W.PRECISION_FP64, W.PRECISION_FP32):
+        m0 = W.CudaMps(w0.n, w0.chi, ctx=ctx, precision=prec)
+        m0.apply_gates(w0.gates)
+        amps.append(m0.amplitude_at_compact_zero())
+        m0.close()
+    return {
+        "form": "complex64 Jacobi columns (FP32 dot products and rotation updates), FP64 rotation parameters, "
+                "tolerance and convergence tests, column norms, sort and cut; sites, merge and range finder FP64",
+        "value": value,
+        "unit": UNIT,
+        "steps": steps,
+        "speedup_vs_fp64": value / fp64_value,
+        "amp_rel_err_vs_fp64": abs(amps[1] - amps[0]) / abs(amps[0]),
+        "error_workload": f"{w0.name}: {w0.n} qubits, chi_max {w0.chi} (the 50-qubit circuit's amplitude, ~1e-25, "
+                          f"is not stable under any change of rounding and is not used)",
+    }
+
+
+def batch_leg(W, torch, ctx, count: int, flush, cpu_budget: float, precision: int = 0) -> dict:
     """The batching form: `count` independent slices (width U[20,60], depth
     U[10,50], chi_max from {16,32,64,128}) in one device state, one pass from
     |0...0> to every slice's <0...0|psi>.  Latency of a slice = device time
     from the start of the pass to the end of the wave holding its last split."""
     slices = C.config2_slices(count)
-    b = W.CudaBatch([s.n for s in slices], [s.chi for s in slices], ctx=ctx)
+    b = W.CudaBatch([s.n for s in slices], [s.chi for s in slices], ctx=ctx, precision=precision)
     stream = torch.cuda.ExternalStream(b.stream())
     gate_lists = [s.gates for s in slices]
     b.set_profiling(True)
@@ -166,7 +210,8 @@ def batch_leg(W, torch, ctx, count: int, flush, cpu_budget: float) -> dict:
     stats = b.kernel_stats()
     out = {
         "workload": f"{count} slices: width U[20,60], depth U[10,50], chi_max U{{16,32,64,128}}, RY/RZ + CNOT "
-                    f"brickwork, own seed each; plain FP64 (complex128), split rule reference",
+                    f"brickwork, own seed each; {'precision form (complex64 Jacobi)' if precision else 'plain FP64'}"
+                    f", split rule reference",
         "slices": count,
         "slices_per_s": count / dev_s,
         "e2e_slices_per_s": count / wall,
@@ -450,6 +495,11 @@ def run_cuda(args) -> None:
         if world == 1 and args.batch_slices > 0:
             line["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush,
                                       0.0 if args.no_cpu_baseline else args.cpu_budget)
+        if world == 1 and args.precision_leg:
+            line["precision_form"] = precision_leg(W, torch, ctx, w, rule, args.steps, flush, value)
+            if args.batch_slices > 0:
+                line["precision_form"]["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush, 0.0,
+                                                            W.PRECISION_FP32)
         print(json.dumps(line), flush=True)
     m.close()
     if dist is not None:
@@ -468,6 +518,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--reference-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision-leg", dest="precision_leg", action="store_false",
+                    help="skip the precision-form (complex64 Jacobi) leg run after the timed steps")
     ap.add_argument("--batch-slices", type=int, default=512,
                     help="slices of the batching-form leg run once after the timed steps (0 = skip)")
     args = ap.parse_args()

@@ -49,7 +49,14 @@ enum wqc_status_code {
 
 /* Arithmetic of the split path. */
 enum wqc_precision {
-    WQC_PRECISION_FP64 = 0 /* plain form: complex128 throughout */
+    WQC_PRECISION_FP64 = 0, /* plain form: complex128 throughout */
+    WQC_PRECISION_FP32 = 1  /* precision form: the Jacobi SVD works on complex64 columns
+                               (FP32 dot products and rotation updates; FP64 rotation
+                               parameters, tolerance tests, convergence test and column
+                               norms); sites, merges, range finder, sort and cut stay
+                               FP64.  Results carry FP32-level error against the plain
+                               form; split decisions made on near-tied singular values
+                               may differ from it. */
 };
 
 typedef struct wqc_cuda_ctx wqc_cuda_ctx;

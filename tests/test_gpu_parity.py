@@ -246,6 +246,29 @@ def test_exact_and_range_finder_splits_in_one_wave(cuda_ctx):
     assert rel_err(m.amplitude_zero(), o.amplitude_zero()) < AMP_RTOL
 
 
+PRECISION_FORM_AMP_RTOL = 1e-3  # measured 1e-4 on the 16-qubit chi 32 circuit (150 truncating splits)
+
+
+def test_precision_form_tracks_the_fp64_oracle(cuda_ctx):
+    """WQC_PRECISION_FP32: the Jacobi SVD on complex64 columns (FP64 rotation
+    parameters, tests and norms).  On the 16-qubit chi 32 brickwork the
+    amplitude stays within PRECISION_FORM_AMP_RTOL of the FP64 oracle, the
+    split sequence and paths are the reference's, and kept chi differs only
+    where singular values tie to FP32 precision at the cut."""
+    w = C.config0()
+    m = W.CudaMps(w.n, w.chi, ctx=cuda_ctx, precision=W.PRECISION_FP32)
+    m.apply_gates(w.gates)
+    o = O.run(w.n, w.chi, w.gates)
+    a, b = m.amplitude_zero(), o.amplitude_zero()
+    assert rel_err(a, b) < PRECISION_FORM_AMP_RTOL, (a, b)
+    got, ref = m.split_records(), o.records()
+    assert np.array_equal(got["left_site"], ref["left_site"])
+    assert np.array_equal(got["path"], ref["path"])
+    for k in ("rows", "cols", "chi"):
+        assert np.mean(got[k] != ref[k]) <= 0.05, (k, np.nonzero(got[k] != ref[k])[0][:10])
+    assert np.abs(got["discarded_weight"] - ref["discarded_weight"]).max() <= 1e-4
+
+
 @pytest.mark.parametrize("bond", [64, 128])
 def test_exact_split_of_full_rank_theta_matches_oracle(cuda_ctx, bond):
     """2*bond x 2*bond full-rank theta through the exact rule (cluster-resident

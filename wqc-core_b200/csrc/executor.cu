@@ -176,6 +176,7 @@ struct wqc_mps {
     int n = 0, chi = 0;
     bool reject = false;
     bool exact_only = false;  // WQC_SPLIT_RULE_EXACT
+    bool fp32 = false;        // WQC_PRECISION_FP32: complex64 Jacobi columns
     cudaStream_t stream = nullptr;
     // Second stream of a wave: the exact-path SVDs run there while the range
     // finder runs on `stream`; fork after the merge, join before the absorb.
@@ -253,9 +254,12 @@ std::once_flag g_attr_once;
 cudaError_t g_attr_err = cudaSuccess;
 
 void set_kernel_attributes() {
-    g_attr_err = cudaFuncSetAttribute(jacobi_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLimit));
-    if (g_attr_err == cudaSuccess)
-        g_attr_err = cudaFuncSetAttribute(jacobi_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (const void* f : {jacobi_kernel(false), jacobi_kernel(true)}) {
+        if (g_attr_err == cudaSuccess)
+            g_attr_err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLimit));
+        if (g_attr_err == cudaSuccess)
+            g_attr_err = cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
     if (g_attr_err == cudaSuccess)
         g_attr_err = cudaFuncSetAttribute(qr_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLimit));
     if (g_attr_err == cudaSuccess)
@@ -275,11 +279,11 @@ int round_up(int x, int q) { return ((x + q - 1) / q) * q; }
 // for one pair's latency, a fixed cost per exchange plus its DSMEM traffic)
 // picks the fastest sweep when the wave's splits cannot fill the GPU, and the
 // least SM-time per split when they can.
-int choose_cluster(int M, int N, int max_c, int njobs, int sm_count) {
+int choose_cluster(int M, int N, int max_c, int njobs, int sm_count, size_t elem) {
     struct Cand { int C; double sweep_us; };
     std::vector<Cand> cands;
     for (int Cc = 1; Cc <= max_c; ++Cc) {
-        if (jacobi_smem_bytes(M, N, Cc) > kSmemLimit) continue;
+        if (jacobi_smem_bytes(M, N, Cc, elem) > kSmemLimit) continue;
         const int Np = round_up(N, 4 * Cc), b = Np / (2 * Cc);
         if (b > 16 && Cc < max_c) continue;  // more pairs than warps
         const double len = M + Np;
@@ -580,13 +584,15 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 w.max_cols = std::max(w.max_cols, cols);
                 w.max_ell = std::max(w.max_ell, ell);
                 const int nj_wave = int(j1 - j0);
+                const size_t elem = m->fp32 ? sizeof(float2) : sizeof(double2);
                 const int c_exact = choose_cluster(std::max(rows, cols), std::min(rows, cols), m->ctx->max_cluster,
-                                                   nj_wave, m->ctx->sm_count);
+                                                   nj_wave, m->ctx->sm_count, elem);
                 add(kJacobiExact, c_exact, local);
                 if (rs) {
                     w.any_rsvd = true;
                     add(kJacobiFallback, c_exact, local);
-                    add(kJacobiRsvd, choose_cluster(cols, ell, m->ctx->max_cluster, nj_wave, m->ctx->sm_count), local);
+                    add(kJacobiRsvd, choose_cluster(cols, ell, m->ctx->max_cluster, nj_wave, m->ctx->sm_count, elem),
+                        local);
                 }
             }
             for (auto& g : groups) {
@@ -601,8 +607,10 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                     int rows, cols, ell;
                     shape(j0 + local, rows, cols, ell);
                     const size_t sz = gr.mode != kJacobiRsvd
-                                          ? jacobi_smem_bytes(std::max(rows, cols), std::min(rows, cols), std::max(gr.C, 1))
-                                          : jacobi_smem_bytes(cols, ell, std::max(gr.C, 1));
+                                          ? jacobi_smem_bytes(std::max(rows, cols), std::min(rows, cols), std::max(gr.C, 1),
+                                                              m->fp32 ? sizeof(float2) : sizeof(double2))
+                                          : jacobi_smem_bytes(cols, ell, std::max(gr.C, 1),
+                                                              m->fp32 ? sizeof(float2) : sizeof(double2));
                     sm = std::max(sm, sz);
                 }
                 gr.smem = sm;
@@ -710,6 +718,10 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
         }
         const SplitJob* d_jobs = d_jobs_all + w.jobs_off;
         const int nj = w.njobs;
+        // Precision form: singular values under 1e-5 of the largest are the
+        // complex64 Jacobi's rounding noise (zero columns come out at ~1e-6
+        // of the norm), far above the 1e-12 cut, so they count as zero.
+        const double noise_rel = m->fp32 ? 1e-5 : 0.0;
         {
             Timed t(m, 1);
             prepare_kernel<<<(nj + 127) / 128, 128, 0, m->stream>>>(d_jobs, m->d_state, nj, m->dev);
@@ -736,9 +748,8 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                 attr[0].val.clusterDim.z = 1;
                 cfg.attrs = attr;
                 cfg.numAttrs = 1;
-                CUDA_TRY(cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel, d_jobs, (const SplitState*)m->d_state,
-                                            (const SlotBuffers*)m->d_slots, d_idx + gr.idx_off, mode, kMaxSweeps,
-                                            m->d_status, m->d_counters));
+                CUDA_TRY(launch_jacobi(m->fp32, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off, mode,
+                                       kMaxSweeps, m->d_status, m->d_counters));
                 count_launch(m, 0);
             }
             return WQC_OK;
@@ -754,8 +765,8 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
         if (wqc_status s = jacobi(kJacobiExact, xs)) return s;
         {
             Timed t(m, 4, xs);
-            finalize_kernel<<<nj, 256, 0, xs>>>(d_jobs, m->d_state, m->d_slots, kJacobiExact, m->chi, m->d_records,
-                                                m->d_status);
+            finalize_kernel<<<nj, 256, 0, xs>>>(d_jobs, m->d_state, m->d_slots, kJacobiExact, m->chi, noise_rel,
+                                                m->d_records, m->d_status);
             count_launch(m, 4);
         }
         if (fork) CUDA_TRY(cudaEventRecord(m->join_ev, m->side));
@@ -797,14 +808,14 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
             if (wqc_status s = jacobi(kJacobiRsvd, m->stream)) return s;
             {
                 Timed t(m, 4);
-                finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiRsvd, m->chi,
+                finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiRsvd, m->chi, noise_rel,
                                                             m->d_records, m->d_status);
                 count_launch(m, 4);
             }
             if (wqc_status s = jacobi(kJacobiFallback, m->stream)) return s;
             {
                 Timed t(m, 4);
-                finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiFallback, m->chi,
+                finalize_kernel<<<nj, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kJacobiFallback, m->chi, noise_rel,
                                                             m->d_records, m->d_status);
                 count_launch(m, 4);
             }
@@ -901,7 +912,7 @@ wqc_status wqc_cuda_open(int device, wqc_cuda_ctx** out) {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, jacobi_cluster_kernel, &cfg) == cudaSuccess && clusters > 0)
+        if (cudaOccupancyMaxActiveClusters(&clusters, jacobi_kernel(false), &cfg) == cudaSuccess && clusters > 0)
             ctx->max_cluster = 16;
         cudaGetLastError();
     }
@@ -941,7 +952,8 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
         total_n += ns[i];
         chi_cap = std::max(chi_cap, chis[i]);
     }
-    if (precision != WQC_PRECISION_FP64) return fail(WQC_ERR_INVALID, "unsupported precision form");
+    if (precision != WQC_PRECISION_FP64 && precision != WQC_PRECISION_FP32)
+        return fail(WQC_ERR_INVALID, "unsupported precision form");
     if (total_n > (1L << 24)) return fail(WQC_ERR_INVALID, "too many sites");
     CUDA_TRY(cudaSetDevice(ctx->device));
     auto* m = new wqc_mps();
@@ -950,6 +962,7 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     m->n = n;
     m->chi = chi_cap;
     m->reject = reject;
+    m->fp32 = precision == WQC_PRECISION_FP32;
     m->ub.assign(n > 0 ? n - 1 : 0, 1);
     m->site_chi.resize(n);
     m->site_slice.resize(n);

@@ -504,23 +504,43 @@ __device__ __forceinline__ int circle_at(int pos, int step, int b) {
 // above 1e-32 ||W||_F^2, while exactly parallel columns (a rank-deficient
 // theta) would otherwise be re-rotated every sweep until their products
 // reach the subnormal range.
-__device__ __forceinline__ int jacobi_rotate(double2* xp, double2* xq, int M, int len, double tol, double noise_floor,
+//
+// The columns are complex128 (double2) in the plain form and complex64
+// (float2) in the precision form.  The precision form accumulates the dot
+// products and applies the rotation in FP32; the rotation parameters, the
+// tests against tol and the noise floor, and the convergence measure are
+// FP64 in both.
+template <typename T>
+struct JacobiReal;
+template <>
+struct JacobiReal<double2> {
+    using R = double;
+};
+template <>
+struct JacobiReal<float2> {
+    using R = float;
+};
+
+template <typename T>
+__device__ __forceinline__ int jacobi_rotate(T* xp, T* xq, int M, int len, double tol, double noise_floor,
                                              int lane, double& relmax) {
-    double a = 0, bb = 0, gr = 0, gi = 0;
+    using R = typename JacobiReal<T>::R;
+    R a_ = 0, b_ = 0, gr_ = 0, gi_ = 0;
     for (int r = lane; r < M; r += 32) {
-        const double2 u = xp[r], v = xq[r];
-        a = fma(u.x, u.x, fma(u.y, u.y, a));
-        bb = fma(v.x, v.x, fma(v.y, v.y, bb));
-        gr = fma(u.x, v.x, fma(u.y, v.y, gr));
-        gi = fma(u.x, v.y, fma(-u.y, v.x, gi));
+        const T u = xp[r], v = xq[r];
+        a_ = fma(u.x, u.x, fma(u.y, u.y, a_));
+        b_ = fma(v.x, v.x, fma(v.y, v.y, b_));
+        gr_ = fma(u.x, v.x, fma(u.y, v.y, gr_));
+        gi_ = fma(u.x, v.y, fma(-u.y, v.x, gi_));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, o);
-        bb += __shfl_xor_sync(0xffffffffu, bb, o);
-        gr += __shfl_xor_sync(0xffffffffu, gr, o);
-        gi += __shfl_xor_sync(0xffffffffu, gi, o);
+        a_ += __shfl_xor_sync(0xffffffffu, a_, o);
+        b_ += __shfl_xor_sync(0xffffffffu, b_, o);
+        gr_ += __shfl_xor_sync(0xffffffffu, gr_, o);
+        gi_ += __shfl_xor_sync(0xffffffffu, gi_, o);
     }
+    const double a = a_, bb = b_, gr = gr_, gi = gi_;
     // Squared forms keep the dependent chain short: |gamma|^2 against
     // tol^2 alpha beta, one reciprocal square root for the phase.
     const double g2 = fma(gr, gr, gi * gi);
@@ -545,23 +565,29 @@ __device__ __forceinline__ int jacobi_rotate(double2* xp, double2* xq, int M, in
     const double s = c * t;
     // With w = s * phase the rephased rotation (svd_guard.rs:189-197) is
     // xp' = c xp - conj(w) xq,  xq' = w xp + c xq   (|phase| = 1).
-    const double wr = s * pr, wi = s * pi;
+    const R wr = R(s * pr), wi = R(s * pi), cr = R(c);
     for (int r = lane; r < len; r += 32) {
-        const double2 u = xp[r], v = xq[r];
-        xp[r] = cmake(fma(c, u.x, -fma(wr, v.x, wi * v.y)), fma(c, u.y, -fma(wr, v.y, -wi * v.x)));
-        xq[r] = cmake(fma(wr, u.x, fma(-wi, u.y, c * v.x)), fma(wr, u.y, fma(wi, u.x, c * v.y)));
+        const T u = xp[r], v = xq[r];
+        T p, q;
+        p.x = fma(cr, u.x, -fma(wr, v.x, wi * v.y));
+        p.y = fma(cr, u.y, -fma(wr, v.y, -wi * v.x));
+        q.x = fma(wr, u.x, fma(-wi, u.y, cr * v.x));
+        q.y = fma(wr, u.y, fma(wi, u.x, cr * v.y));
+        xp[r] = p;
+        xq[r] = q;
     }
     return 1;
 }
 
-// Block copy from another CTA's shared memory: eight 16-byte loads in flight
-// per thread before the stores.
-__device__ __forceinline__ void dsmem_copy(double2* __restrict__ dst, const double2* __restrict__ src, size_t n,
-                                           int tid, int nthreads) {
+// Block copy from another CTA's shared memory: eight loads in flight per
+// thread before the stores.
+template <typename T>
+__device__ __forceinline__ void dsmem_copy(T* __restrict__ dst, const T* __restrict__ src, size_t n, int tid,
+                                           int nthreads) {
     size_t e = tid;
     const size_t st = nthreads;
     for (; e + 7 * st < n; e += 8 * st) {
-        double2 v[8];
+        T v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) v[u] = src[e + u * st];
 #pragma unroll
@@ -595,10 +621,25 @@ __device__ __forceinline__ bool jacobi_active(const SplitState& S, int mode) {
     return S.need_exact != 0 && S.path == WQC_SPLIT_RSVD_FALLBACK;
 }
 
+template <typename T>
+__device__ __forceinline__ T to_store(double2 x);
+template <>
+__device__ __forceinline__ double2 to_store<double2>(double2 x) {
+    return x;
+}
+template <>
+__device__ __forceinline__ float2 to_store<float2>(double2 x) {
+    return make_float2(float(x.x), float(x.y));
+}
+__device__ __forceinline__ double2 to_f64(double2 x) { return x; }
+__device__ __forceinline__ double2 to_f64(float2 x) { return make_double2(x.x, x.y); }
+
+template <typename T>
 __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const SplitJob* jobs, const SplitState* st,
                                                                           const SlotBuffers* slots, const int* idx,
                                                                           int mode, int max_sweeps, int* status,
                                                                           unsigned long long* counters) {
+    constexpr bool kF64 = sizeof(T) == sizeof(double2);
     cg::cluster_group cluster = cg::this_cluster();
     const int C = int(cluster.num_blocks());
     const int rank = int(cluster.block_rank());
@@ -617,7 +658,8 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
     const int b = Np / (2 * C);
     const int len = M + Np;
 
-    extern __shared__ __align__(16) double2 smem[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
     __shared__ JacobiCtl ctl;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int nthreads = blockDim.x;  // a multiple of 32, at most kJacobiThreads
@@ -668,26 +710,31 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
     // Load W (dust-zeroed) and Z = identity.
     for (int half = 0; half < 2; ++half) {
         const int id = half == 0 ? rank : 2 * C - 1 - rank;
-        double2* base = buf(half);
+        T* base = buf(half);
         for (int e = tid; e < b * M; e += nthreads) {
             int c, i;
             if (rows_of_src) { c = e / M; i = e % M; } else { i = e / b; c = e % b; }
             const int col = id * b + c;
             double2 x = col < N ? src_at(i, col) : cmake(0, 0);
             if (cnorm2(x) < dust2) x = cmake(0, 0);
-            base[size_t(c) * len + i] = x;
+            base[size_t(c) * len + i] = to_store<T>(x);
         }
         for (int e = tid; e < b * Np; e += nthreads) {
             const int c = e / Np, i = e % Np;
-            base[size_t(c) * len + M + i] = cmake(i == id * b + c ? 1.0 : 0.0, 0.0);
+            base[size_t(c) * len + M + i] = to_store<T>(cmake(i == id * b + c ? 1.0 : 0.0, 0.0));
         }
     }
     __syncthreads();
-    // Pairs count as orthogonal at |gamma| <= 1e-14 sqrt(alpha beta): above
-    // the rounding of an M <= 512 dot product (sqrt(M) eps <= 5e-15), so the
-    // sweeps stop, and the singular values are then exact to second order.
-    const double tol = 1e-14;
-    const double noise_floor = 1e-32 * fro2;
+    // Pairs count as orthogonal at |gamma| <= tol sqrt(alpha beta), just
+    // above the rounding of an M <= 512 dot product (sqrt(M) eps: 5e-15 in
+    // FP64, 3e-6 in FP32), so the sweeps stop and the singular values are
+    // exact to second order.  A sweep that every pair entered orthogonal to
+    // stop_rel ends the iteration: one-sided Jacobi converges quadratically,
+    // so that sweep leaves them at about stop_rel^2 <= tol.  Columns at the
+    // storage's rounding level against ||W||_F are left alone (noise floor).
+    const double tol = kF64 ? 1e-14 : 4e-6;
+    const double stop_rel2 = kF64 ? 1e-16 : 4e-6;  // squared: 1e-8 and 2e-3
+    const double noise_floor = (kF64 ? 1e-32 : 1e-14) * fro2;
     int sweep = 0;
     bool converged = false;
     for (; sweep < max_sweeps; ++sweep) {
@@ -703,7 +750,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
             for (int pq = wid; pq < b; pq += nwarps) {
                 const bool top = pq < b / 2;
                 const int i = top ? pq : pq - b / 2;
-                double2* base = buf(top ? top_buf_of(rank, xk) : bot_buf_of(rank, xk));
+                T* base = buf(top ? top_buf_of(rank, xk) : bot_buf_of(rank, xk));
                 const int e1 = circle_at(i, step, b), e2 = circle_at(b - 1 - i, step, b);
                 my_rot += jacobi_rotate(base + size_t(e1) * len, base + size_t(e2) * len, M, len, tol, noise_floor, lane, my_rel);
             }
@@ -712,8 +759,8 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
         // Cross pairs between the two blocks, 2C-1 block steps.
         for (int bs = 0; bs < 2 * C - 1; ++bs) {
             for (int k = 0; k < b; ++k) {
-                double2* tb = buf(top_buf_of(rank, xk));
-                double2* bb = buf(bot_buf_of(rank, xk));
+                T* tb = buf(top_buf_of(rank, xk));
+                T* bb = buf(bot_buf_of(rank, xk));
                 for (int i = wid; i < b; i += nwarps) {
                     const int e2 = (i + k) % b;
                     my_rot += jacobi_rotate(tb + size_t(i) * len, bb + size_t(e2) * len, M, len, tol, noise_floor, lane, my_rel);
@@ -741,7 +788,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
             }
             cluster.sync();
             if (rank <= C - 2) {
-                const double2* rsrc = cluster.map_shared_rank(smem, rank + 1) + size_t(bot_buf_of(rank + 1, xk)) * blk;
+                const T* rsrc = cluster.map_shared_rank(smem, rank + 1) + size_t(bot_buf_of(rank + 1, xk)) * blk;
                 dsmem_copy(buf(rank == 0 ? bot_buf_of(0, xk) : top_buf_of(rank, xk)), rsrc, blk, tid, nthreads);
             }
             ++xk;
@@ -767,10 +814,10 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
             cluster.sync();
         }
         // Converged when nothing rotated, or when every pair entered this
-        // sweep orthogonal to 1e-8: one-sided Jacobi converges quadratically,
-        // so this sweep left them orthogonal to about 1e-16, below the
-        // rotation tolerance, and a verification sweep would rotate nothing.
-        if (total == 0 || relmax < 1e-16) {  // relmax holds squared ratios
+        // sweep orthogonal to stop_rel (FP64: 1e-8, leaving them at about
+        // 1e-16, below the rotation tolerance, so a verification sweep would
+        // rotate nothing).
+        if (total == 0 || relmax < stop_rel2) {  // relmax holds squared ratios
             converged = true;
             break;
         }
@@ -783,18 +830,18 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
     // Write back: W columns, Z columns (first N rows) and column norms.
     for (int half = 0; half < 2; ++half) {
         const int id = circle_at(half == 0 ? rank : 2 * C - 1 - rank, xk, 2 * C);
-        const double2* base = buf(half == 0 ? top_buf_of(rank, xk) : bot_buf_of(rank, xk));
+        const T* base = buf(half == 0 ? top_buf_of(rank, xk) : bot_buf_of(rank, xk));
         for (int c = wid; c < b; c += nwarps) {
             const int col = id * b + c;
             if (col >= N) continue;
-            const double2* x = base + size_t(c) * len;
-            double s2 = 0;
+            const T* x = base + size_t(c) * len;
+            double s2 = 0;  // column norms in FP64 in both forms
             for (int r = lane; r < M; r += 32) {
-                const double2 v = x[r];
+                const double2 v = to_f64(x[r]);
                 s2 = fma(v.x, v.x, fma(v.y, v.y, s2));
                 Bf.w[size_t(col) * M + r] = v;
             }
-            for (int r = lane; r < N; r += 32) Bf.z[size_t(col) * N + r] = x[M + r];
+            for (int r = lane; r < N; r += 32) Bf.z[size_t(col) * N + r] = to_f64(x[M + r]);
             for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
             if (lane == 0) Bf.sigma[col] = sqrt(s2);
         }
@@ -806,7 +853,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
 // discarded weight and the split record.
 // ---------------------------------------------------------------------------
 __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const SlotBuffers* slots, int mode,
-                                int chi_max, wqc_split_info* records, int* status) {
+                                int chi_max, double noise_rel, wqc_split_info* records, int* status) {
     const int j = blockIdx.x;
     SplitState& S = st[j];
     if (!jacobi_active(S, mode)) return;
@@ -826,9 +873,11 @@ __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const Slot
         B.perm[r] = c;
     }
     __syncthreads();
+    const double floor_abs = N > 0 ? noise_rel * B.sigma[B.perm[0]] : 0.0;
     for (int c = tid; c < N; c += blockDim.x) {
         double v = B.sigma[B.perm[c]];
         if (mode == kJacobiRsvd && v < kRsvdZero) v = 0.0;
+        if (v < floor_abs) v = 0.0;
         vals[c] = v;
     }
     __syncthreads();
@@ -958,4 +1007,21 @@ __global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const
     }
 }
 
+}  // namespace wqc
+
+namespace wqc {
+const void* jacobi_kernel(bool fp32) {
+    return fp32 ? reinterpret_cast<const void*>(jacobi_cluster_kernel<float2>)
+                : reinterpret_cast<const void*>(jacobi_cluster_kernel<double2>);
+}
+
+cudaError_t launch_jacobi(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, const SplitState* st,
+                          const SlotBuffers* slots, const int* idx, int mode, int max_sweeps, int* status,
+                          unsigned long long* counters) {
+    if (fp32)
+        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<float2>, jobs, st, slots, idx, mode, max_sweeps, status,
+                                  counters);
+    return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<double2>, jobs, st, slots, idx, mode, max_sweeps, status,
+                              counters);
+}
 }  // namespace wqc

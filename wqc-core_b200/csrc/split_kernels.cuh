@@ -24,11 +24,17 @@ inline size_t qr_cluster_smem_bytes(int m, int n, int C) {
     const int cpc = (n + C - 1) / C;
     return (size_t(2) * cpc * m + size_t(3) * m + cpc) * sizeof(double2);
 }
-__global__ void jacobi_cluster_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
-                                      const int* idx, int mode, int max_sweeps, int* status,
-                                      unsigned long long* counters);
+// The cluster Jacobi SVD kernel (a template over the column type: complex128
+// in the plain form, complex64 in the precision form), reached from other
+// files through these host functions.
+const void* jacobi_kernel(bool fp32);
+cudaError_t launch_jacobi(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, const SplitState* st,
+                          const SlotBuffers* slots, const int* idx, int mode, int max_sweeps, int* status,
+                          unsigned long long* counters);
+// noise_rel: singular values below noise_rel * (largest) count as zero (0 in
+// the plain form; the precision form's FP32 rounding level).
 __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const SlotBuffers* slots, int mode,
-                                int chi_max, wqc_split_info* records, int* status);
+                                int chi_max, double noise_rel, wqc_split_info* records, int* status);
 __global__ void absorb_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
                               DeviceMps mps);
 
@@ -46,13 +52,13 @@ __global__ void pauli_expectation_kernel(DeviceMps mps, const char* labels, int 
                                          int env_cap, double2* out);
 
 // Jacobi shared-memory footprint for a working matrix of M rows and N columns
-// on a cluster of C CTAs.
-inline size_t jacobi_smem_bytes(int M, int N, int C) {
+// on a cluster of C CTAs, `elem` bytes per complex entry.
+inline size_t jacobi_smem_bytes(int M, int N, int C, size_t elem = sizeof(double2)) {
     const int quantum = 4 * C;
     const int Np = ((N + quantum - 1) / quantum) * quantum;
     const int b = Np / (2 * C);
     const int nbuf = C == 1 ? 2 : 3;
-    return size_t(nbuf) * b * (M + Np) * sizeof(double2);
+    return size_t(nbuf) * b * (M + Np) * elem;
 }
 
 }  // namespace wqc

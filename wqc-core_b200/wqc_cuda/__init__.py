@@ -33,6 +33,7 @@ ERR_QUBIT_OUT_OF_RANGE = 9
 ERR_INVALID_QUBIT_COUNT = 10
 
 PRECISION_FP64 = 0
+PRECISION_FP32 = 1
 SPLIT_RULE_REFERENCE = 0
 SPLIT_RULE_EXACT = 1
 
