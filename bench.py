@@ -184,6 +184,90 @@ def precision_leg(W, torch, ctx, w, rule, steps: int, flush, fp64_value: float) 
     }
 
 
+def oracle_gradient_sample(n, chi, lists, labels, coeffs, budget_s: float, threads: int):
+    """CPU leg of the differentiation form: threads run whole shifted circuits
+    (and the observable) on the oracle until `budget_s`; returns (circuits
+    done, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.lib()
+    done = [0] * threads
+    secs = [0.0] * threads
+    barrier = threading.Barrier(threads)
+
+    def worker(t):
+        barrier.wait()
+        t0 = time.perf_counter()
+        k = t
+        while k < len(lists) and time.perf_counter() - t0 < budget_s:
+            o = O.run(n, chi, lists[k])
+            o.expectation(labels, coeffs)
+            done[t] += 1
+            k += threads
+        secs[t] = time.perf_counter() - t0
+
+    ths = [threading.Thread(target=worker, args=(t,)) for t in range(threads)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    return sum(done), max(secs)
+
+
+def differentiation_leg(W, torch, ctx, flush, cpu_budget: float) -> dict:
+    """Config 3's workload: the 32-qubit hardware-efficient ansatz (8 layers
+    of RY, RZ on every qubit and a CZ ladder; 512 parameters), observable
+    sum Z_i Z_i+1 + 0.5 sum X_i, chi_max 64.  One full gradient by the
+    parameter-shift rule: 1025 circuits (unshifted + two per parameter) as
+    slices of one batch, the observable evaluated on every slice."""
+    from wqc_cuda import gradients as G
+
+    n, chi = 32, 64
+    gates, pidx, _ = C.hea_ansatz(n, 8)
+    labels, coeffs = C.zz_x_observable(n)
+    lists, _ = G.shifted_circuits(gates, pidx)
+    b = W.CudaBatch([n] * len(lists), [chi] * len(lists), ctx=ctx)
+    stream = torch.cuda.ExternalStream(b.stream())
+    flush.fill_(float(np.random.random()))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    b.apply_slices(lists)
+    vals = b.expectations(labels, coeffs).real
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    dev_s = e0.elapsed_time(e1) * 1e-3
+    splits = b.split_count()
+    b.close()
+    grad = 0.5 * (vals[1::2] - vals[2::2])
+    out = {
+        "workload": "hea32_l8_chi64: 32 qubits, 8 layers RY/RZ + CZ ladder, 512 parameters, "
+                    "sum Z_i Z_i+1 + 0.5 sum X_i (63 terms), chi_max 64, FP64",
+        "method": "parameter shift on the batching form (the adjoint is not built)",
+        "circuits": len(lists),
+        "gradient_seconds": dev_s,
+        "gradient_seconds_e2e": wall,
+        "applies_per_s": splits / dev_s,
+        "value": float(vals[0]),
+        "grad_norm": float(np.linalg.norm(grad)),
+    }
+    if cpu_budget > 0:
+        threads = os.cpu_count() or 1
+        done, secs = oracle_gradient_sample(n, chi, lists, labels, coeffs, cpu_budget, threads)
+        out["cpu_baseline"] = {
+            "value": (done / secs) / len(lists) if done else None,
+            "unit": "gradients/s",
+            "cores": threads,
+            "kind": "port",
+            "sample": f"FP64 restatement, whole shifted circuits + observable, one per thread on {threads} threads: "
+                      f"{done} of {len(lists)} circuits in {secs:.1f} s",
+        }
+    return out
+
+
 def batch_leg(W, torch, ctx, count: int, flush, cpu_budget: float, precision: int = 0) -> dict:
     """The batching form: `count` independent slices (width U[20,60], depth
     U[10,50], chi_max from {16,32,64,128}) in one device state, one pass from
@@ -495,6 +579,9 @@ def run_cuda(args) -> None:
         if world == 1 and args.batch_slices > 0:
             line["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush,
                                       0.0 if args.no_cpu_baseline else args.cpu_budget)
+        if world == 1 and args.differentiation_leg:
+            line["differentiation"] = differentiation_leg(W, torch, ctx, flush,
+                                                          0.0 if args.no_cpu_baseline else args.cpu_budget)
         if world == 1 and args.precision_leg:
             line["precision_form"] = precision_leg(W, torch, ctx, w, rule, args.steps, flush, value)
             if args.batch_slices > 0:
@@ -518,6 +605,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--reference-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-differentiation-leg", dest="differentiation_leg", action="store_false",
+                    help="skip the parameter-shift gradient of the 32-qubit ansatz run after the timed steps")
     ap.add_argument("--no-precision-leg", dest="precision_leg", action="store_false",
                     help="skip the precision-form (complex64 Jacobi) leg run after the timed steps")
     ap.add_argument("--batch-slices", type=int, default=512,

@@ -107,6 +107,12 @@ WQC_API wqc_status wqc_batch_amplitudes(wqc_mps* batch, double* out);
  * wqc_batch_apply_gates call to the completion of each slice's last split
  * (CUDA events on the state's stream); -1 for a slice without operations. */
 WQC_API wqc_status wqc_batch_slice_times(wqc_mps* batch, double* out_ms);
+/* compute_expectations (src/expectation.rs:98-200) on every slice: the same
+ * Pauli sum (labels as for wqc_mps_expectation_pauli; every slice must have
+ * the labels' width), out[2s], out[2s+1] for slice s.  The batching form's
+ * route to parameter-shift gradients: each shifted circuit is one slice. */
+WQC_API wqc_status wqc_batch_expectation_pauli(wqc_mps* batch, const char* labels, const double* coeffs,
+                                               uint32_t nterms, double* out);
 
 /* Back to |0...0> with the split records cleared, keeping the device memory
  * (a fresh MpsState for the next request without reallocating). */

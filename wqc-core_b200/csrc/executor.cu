@@ -1196,6 +1196,79 @@ wqc_status wqc_batch_amplitudes(wqc_mps* m, double* out) {
     return sync_status(m);
 }
 
+wqc_status wqc_batch_expectation_pauli(wqc_mps* m, const char* labels, const double* coeffs, uint32_t nterms,
+                                       double* out) {
+    if (!m || !labels || !coeffs || !out) return fail(WQC_ERR_INVALID, "null argument");
+    const int nseg = int(m->seg_first.size());
+    const int width = nseg > 0 ? (m->n / nseg) : 0;
+    for (int s = 0; s < nseg; ++s) {
+        const int first = m->seg_first[s], last = s + 1 < nseg ? m->seg_first[s + 1] : m->n;
+        if (last - first != width) return fail(WQC_ERR_INVALID, "batch expectation needs slices of one width");
+    }
+    for (size_t i = 0; i < size_t(nterms) * width; ++i) {
+        const char ch = labels[i];
+        if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z')
+            return fail(WQC_ERR_INVALID, std::string("invalid pauli character in label"));
+    }
+    if (nterms == 0 || nseg == 0) {
+        for (int s = 0; s < 2 * nseg; ++s) out[s] = 0;
+        return WQC_OK;
+    }
+    const size_t E = size_t(m->chi) * m->chi;
+    const size_t scratch = size_t(nterms) * 4 * E * sizeof(double2);
+    const size_t lab_bytes = size_t(nterms) * width + 16;
+    const size_t out_bytes = size_t(nterms) * nseg * sizeof(double2);
+    void* d_lab = nullptr;
+    void* d_scr = nullptr;
+    void* d_out = nullptr;
+    if (wqc_status s = dmalloc(m, &d_lab, lab_bytes)) return s;
+    if (wqc_status s = dmalloc(m, &d_scr, scratch)) {
+        dfree(m, d_lab, lab_bytes);
+        return s;
+    }
+    if (wqc_status s = dmalloc(m, &d_out, out_bytes)) {
+        dfree(m, d_lab, lab_bytes);
+        dfree(m, d_scr, scratch);
+        return s;
+    }
+    wqc_status rc = WQC_OK;
+    std::vector<double2> vals(size_t(nterms) * nseg);
+    cudaError_t e = cudaMemcpyAsync(d_lab, labels, size_t(nterms) * width, cudaMemcpyHostToDevice, m->stream);
+    // One launch per slice on a view of its sites; launches share the scratch
+    // in stream order.
+    for (int s = 0; s < nseg && e == cudaSuccess; ++s) {
+        DeviceMps view = m->dev;
+        const int first = m->seg_first[s];
+        view.site += first;
+        view.dl += first;
+        view.dr += first;
+        view.n = width;
+        pauli_expectation_kernel<<<nterms, 256, 0, m->stream>>>(view, static_cast<const char*>(d_lab), int(nterms),
+                                                                  static_cast<double2*>(d_scr), m->chi,
+                                                                  static_cast<double2*>(d_out) + size_t(s) * nterms);
+        count_launch(m, -1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(vals.data(), d_out, out_bytes, cudaMemcpyDeviceToHost, m->stream);
+    if (e != cudaSuccess) rc = fail(WQC_ERR_CUDA, cudaGetErrorString(e));
+    if (rc == WQC_OK) rc = sync_status(m);
+    dfree(m, d_lab, lab_bytes);
+    dfree(m, d_scr, scratch);
+    dfree(m, d_out, out_bytes);
+    if (rc != WQC_OK) return rc;
+    for (int s = 0; s < nseg; ++s) {
+        double re = 0, im = 0;
+        for (uint32_t t = 0; t < nterms; ++t) {  // coeff * Re<P> (expectation.rs:177-185), term order
+            const double v = vals[size_t(s) * nterms + t].x;
+            re += coeffs[2 * t] * v;
+            im += coeffs[2 * t + 1] * v;
+        }
+        out[2 * s] = re;
+        out[2 * s + 1] = im;
+    }
+    return WQC_OK;
+}
+
 wqc_status wqc_batch_slice_times(wqc_mps* m, double* out_ms) {
     if (!m || !out_ms) return fail(WQC_ERR_INVALID, "null argument");
     if (wqc_status s = sync_status(m)) return s;

@@ -47,7 +47,7 @@ EXPORTS = (
     "wqc_mps_peak_vram_bytes", "wqc_mps_backend_label", "wqc_mps_set_profiling", "wqc_mps_kernel_stats",
     "wqc_mps_reset_stats", "wqc_mps_stream", "wqc_schedule_gates", "wqc_mps_reset", "wqc_mps_debug_workspace",
     "wqc_batch_create", "wqc_batch_apply_gates", "wqc_batch_amplitudes", "wqc_batch_slice_times",
-    "wqc_expectation_pauli_noalloc",
+    "wqc_expectation_pauli_noalloc", "wqc_batch_expectation_pauli",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
@@ -132,6 +132,7 @@ def lib():
         L.wqc_batch_apply_gates.argtypes = [P, P, ctypes.POINTER(U32)]
         L.wqc_batch_amplitudes.argtypes = [P, D]
         L.wqc_batch_slice_times.argtypes = [P, D]
+        L.wqc_batch_expectation_pauli.argtypes = [P, ctypes.c_char_p, D, U32, D]
         L.wqc_mps_stream.argtypes = [P]
         L.wqc_mps_stream.restype = P
         L.wqc_expectation_pauli_noalloc.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(U32), U32, ctypes.c_char_p, D,
@@ -418,6 +419,15 @@ class CudaBatch(CudaMps):
     def amplitudes(self) -> np.ndarray:
         out = np.zeros(len(self.qubits), dtype=np.complex128)
         _check(lib().wqc_batch_amplitudes(self._h, _dp(out.view(np.float64))))
+        return out
+
+    def expectations(self, labels, coeffs) -> np.ndarray:
+        """The Pauli sum on every slice (wqc_batch_expectation_pauli)."""
+        joined = "".join(labels).encode()
+        c = _c128(coeffs)
+        out = np.zeros(len(self.qubits), dtype=np.complex128)
+        _check(lib().wqc_batch_expectation_pauli(self._h, joined, _dp(c.view(np.float64)), len(labels),
+                                                 _dp(out.view(np.float64))))
         return out
 
     def slice_times_ms(self) -> np.ndarray:
