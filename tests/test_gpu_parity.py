@@ -269,10 +269,11 @@ def test_precision_form_tracks_the_fp64_oracle(cuda_ctx):
     assert np.abs(got["discarded_weight"] - ref["discarded_weight"]).max() <= 1e-4
 
 
-@pytest.mark.parametrize("bond", [64, 128])
+@pytest.mark.parametrize("bond", [64, 128, 256])
 def test_exact_split_of_full_rank_theta_matches_oracle(cuda_ctx, bond):
     """2*bond x 2*bond full-rank theta through the exact rule (cluster-resident
-    Jacobi at its largest size for chi 128): kept product, rank, discarded
+    Jacobi at its largest size for chi 128; the staged Jacobi, columns in the
+    global workspace, for 512 x 512 at chi 256): kept product, rank, discarded
     weight."""
     rng = np.random.default_rng(bond)
     sites = _random_sites(rng, [(1, bond), (bond, bond), (bond, bond), (bond, 1)])
@@ -290,6 +291,33 @@ def test_exact_split_of_full_rank_theta_matches_oracle(cuda_ctx, bond):
     got, want = _theta(m.site(1), m.site(2)), _theta(o.site(1), o.site(2))
     err = np.abs(got - want).max() / np.abs(want).max()
     assert err <= 1e-11, err
+    assert abs(float(info["discarded_weight"]) - float(ref["discarded_weight"])) <= DISC_ATOL
+
+
+def test_range_finder_split_at_chi_256_matches_oracle(cuda_ctx):
+    """A 512x512 split at chi 256 takes the range finder (ell 272); B^H
+    (512 x 272) exceeds a cluster's shared memory and runs on the staged
+    Jacobi.  At this shape the reference's Rademacher rows repeat every 64
+    rows and theta's columns (t, b) split at 256, so Omega cannot tell the
+    t = 0 and t = 1 halves apart and Y = A A^H A Omega has half of theta's
+    rank: the range finder is rounding-determined for a generic theta.  With
+    the t = 1 half empty (right site's t = 1 slice zero, diagonal CZ) theta
+    keeps rank 12 in Y and the result is unique."""
+    rng = np.random.default_rng(256)
+    sites = _random_sites(rng, [(1, 256), (256, 12), (12, 256), (256, 1)])
+    sites[2][:, 1, :] = 0
+    m = W.CudaMps(4, 256, ctx=cuda_ctx)
+    o = O.OracleMps(4, 256)
+    for i, s in enumerate(sites):
+        m.set_site(i, s)
+        o.set_site(i, s)
+    info = m.apply_two_qubit_at_positions(1, 2, W.CZ4, False, want_info=True)
+    o.apply_2q_at(1, W.CZ4, False)
+    ref = o.records()[0]
+    assert int(ref["path"]) == 1 and int(info["path"]) == 1, (ref, info)
+    assert int(info["ell"]) == 272 and int(info["chi"]) == int(ref["chi"]) == 12, (ref, info)
+    got, want = _theta(m.site(1), m.site(2)), _theta(o.site(1), o.site(2))
+    assert np.abs(got - want).max() / np.abs(want).max() <= 1e-12
     assert abs(float(info["discarded_weight"]) - float(ref["discarded_weight"])) <= DISC_ATOL
 
 

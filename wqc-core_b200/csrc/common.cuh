@@ -101,6 +101,7 @@ struct SlotBuffers {
     double* sigma;   // N
     int* perm;       // N: sorted position -> column
     double2* tau;    // ell Householder scalars
+    void* gs;        // staged Jacobi workspace (padded W and Z columns), chi_max > 128 only
 };
 
 // One Jacobi SVD task: decompose X where column j of the tall working matrix

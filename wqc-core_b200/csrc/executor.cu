@@ -146,7 +146,9 @@ struct Op {
 struct Group {
     int mode, C, idx_off, count;
     size_t smem;
-    int threads;  // one warp per column pair of a block, at most kJacobiThreads
+    int threads;          // one warp per column pair of a block, at most kJacobiThreads
+    bool staged = false;  // jacobi_staged_kernel with blocks of b columns
+    int b = 0;
 };
 
 struct Wave {
@@ -254,7 +256,7 @@ std::once_flag g_attr_once;
 cudaError_t g_attr_err = cudaSuccess;
 
 void set_kernel_attributes() {
-    for (const void* f : {jacobi_kernel(false), jacobi_kernel(true)}) {
+    for (const void* f : {jacobi_kernel(false), jacobi_kernel(true), jacobi_staged(false), jacobi_staged(true)}) {
         if (g_attr_err == cudaSuccess)
             g_attr_err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLimit));
         if (g_attr_err == cudaSuccess)
@@ -585,14 +587,18 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 w.max_ell = std::max(w.max_ell, ell);
                 const int nj_wave = int(j1 - j0);
                 const size_t elem = m->fp32 ? sizeof(float2) : sizeof(double2);
-                const int c_exact = choose_cluster(std::max(rows, cols), std::min(rows, cols), m->ctx->max_cluster,
-                                                   nj_wave, m->ctx->sm_count, elem);
+                // A shape beyond every cluster's shared memory goes to the
+                // staged kernel: group key -b (0: no kernel takes it).
+                auto cluster_or_staged = [&](int M, int N) {
+                    const int c = choose_cluster(M, N, m->ctx->max_cluster, nj_wave, m->ctx->sm_count, elem);
+                    return c >= 1 ? c : -jacobi_staged_b(M, N, elem, kSmemLimit, nullptr);
+                };
+                const int c_exact = cluster_or_staged(std::max(rows, cols), std::min(rows, cols));
                 add(kJacobiExact, c_exact, local);
                 if (rs) {
                     w.any_rsvd = true;
                     add(kJacobiFallback, c_exact, local);
-                    add(kJacobiRsvd, choose_cluster(cols, ell, m->ctx->max_cluster, nj_wave, m->ctx->sm_count, elem),
-                        local);
+                    add(kJacobiRsvd, cluster_or_staged(cols, ell), local);
                 }
             }
             for (auto& g : groups) {
@@ -601,6 +607,26 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 gr.C = g.first.second;
                 gr.idx_off = int(plan.idx.size());
                 gr.count = int(g.second.size());
+                const size_t elem = m->fp32 ? sizeof(float2) : sizeof(double2);
+                if (gr.C < 0) {
+                    gr.staged = true;
+                    gr.b = -gr.C;
+                    gr.C = m->ctx->max_cluster;
+                    size_t sm = 0;
+                    for (int local : g.second) {
+                        int rows, cols, ell;
+                        shape(j0 + local, rows, cols, ell);
+                        const int M = gr.mode != kJacobiRsvd ? std::max(rows, cols) : cols;
+                        const int N = gr.mode != kJacobiRsvd ? std::min(rows, cols) : ell;
+                        const int K = (N + 2 * gr.b - 1) / (2 * gr.b);
+                        sm = std::max(sm, size_t(2) * gr.b * (size_t(M) + size_t(2) * K * gr.b) * elem);
+                    }
+                    gr.smem = sm;
+                    gr.threads = 32 * std::min(kJacobiThreads / 32, std::max(4, gr.b));
+                    for (int local : g.second) plan.idx.push_back(local);
+                    w.groups.push_back(gr);
+                    continue;
+                }
                 // shared memory for the largest job of the group
                 size_t sm = 0;
                 for (int local : g.second) {
@@ -748,8 +774,12 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                 attr[0].val.clusterDim.z = 1;
                 cfg.attrs = attr;
                 cfg.numAttrs = 1;
-                CUDA_TRY(launch_jacobi(m->fp32, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off, mode,
-                                       kMaxSweeps, m->d_status, m->d_counters));
+                if (gr.staged)
+                    CUDA_TRY(launch_jacobi_staged(m->fp32, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off,
+                                                  mode, kMaxSweeps, gr.b, m->d_status, m->d_counters));
+                else
+                    CUDA_TRY(launch_jacobi(m->fp32, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off, mode,
+                                           kMaxSweeps, m->d_status, m->d_counters));
                 count_launch(m, 0);
             }
             return WQC_OK;
@@ -858,6 +888,9 @@ wqc_status sync_status(wqc_mps* m) {
     if (st & kStatusCancelled) return fail(WQC_ERR_CANCELLED, "computation cancelled: the client has gone");
     if (st & kStatusTruncationRejected) return fail(WQC_ERR_TRUNCATION_REJECTED, "mps bond exceeded chi");
     if (st & kStatusNonFinite) return fail(WQC_ERR_SVD_FAILED, "SVD of a two-site matrix produced non-finite values");
+    if (st & kStatusJacobiNoConvergence)
+        return fail(WQC_ERR_SVD_FAILED, "Jacobi SVD of a two-site matrix did not converge in 60 sweeps");
+    if (st & kStatusBadShape) return fail(WQC_ERR_INVALID, "two-site matrix without a Jacobi workspace");
     return WQC_OK;
 }
 
@@ -990,7 +1023,13 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     cudaEventRecord(m->stage_done, m->stream);
     // Budget check before any large allocation (mps.rs:36-48 analogue).
     const int R = 2 * chi_cap, E = std::min(chi_cap + kRsvdOversample, R);
-    const size_t slot_c = size_t(R) * R * 3 + size_t(R) * E * 6 + E;  // theta, w, z + range finder + tau
+    // theta, w, z + range finder + tau (+ the staged Jacobi's workspace when a
+    // two-site matrix can exceed a cluster's shared memory)
+    const size_t el = precision == WQC_PRECISION_FP32 ? sizeof(float2) : sizeof(double2);
+    const bool staged = choose_cluster(R, R, ctx->max_cluster, 1, ctx->sm_count, el) < 1 ||
+                        choose_cluster(R, E, ctx->max_cluster, 1, ctx->sm_count, el) < 1;
+    const size_t gs_c = staged ? jacobi_staged_elems(R) : 0;
+    const size_t slot_c = size_t(R) * R * 3 + size_t(R) * E * 6 + E + gs_c;
     const size_t slot_bytes = ((slot_c * sizeof(double2) + size_t(R) * (sizeof(double) + sizeof(int)) + 4095) / 4096) * 4096;
     m->nslots = nslots_req > 0 ? nslots_req : std::max(1, n / 2);
     const size_t site_bytes = site_off[n] * sizeof(double2);
@@ -1054,6 +1093,8 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
         bf.q = c; c += size_t(R) * E;
         bf.b = c; c += size_t(R) * E;
         bf.tau = c; c += E;
+        bf.gs = gs_c ? static_cast<void*>(c) : nullptr;
+        c += gs_c;
         bf.sigma = reinterpret_cast<double*>(c);
         bf.perm = reinterpret_cast<int*>(bf.sigma + R);
     }

@@ -849,6 +849,189 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
 }
 
 // ---------------------------------------------------------------------------
+// The same Jacobi SVD for working matrices too large for a cluster's shared
+// memory (theta up to 512 x 512 at chi 256: W and Z take 8 MB in FP64, a
+// 16-CTA cluster holds 3.6 MB).  The padded columns (W then Z, `len`
+// entries each) live in the slot's global workspace `gs`, which stays in L2.
+// The N' = 2Kb columns form 2K blocks of b; a sweep runs 2K-1 steps of the
+// circle method over the blocks (position 0 fixed, block at position p at
+// step s: circle_at(p, s, 2K)), and at each step CTA r takes the block pairs
+// r, r+C, ... < K: it loads both blocks into shared memory, rotates the b*b
+// cross pairs (and, at a sweep's first step, the pairs inside each block),
+// and stores them back.  One cluster barrier separates the steps: every
+// block is held by one pair per step, so a block's store and its next load
+// are ordered by that barrier.  Rotation rule, tolerances, stop test and
+// outputs are those of jacobi_cluster_kernel.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const SplitJob* jobs, const SplitState* st,
+                                                                         const SlotBuffers* slots, const int* idx,
+                                                                         int mode, int max_sweeps, int b, int* status,
+                                                                         unsigned long long* counters) {
+    constexpr bool kF64 = sizeof(T) == sizeof(double2);
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = int(cluster.num_blocks());
+    const int rank = int(cluster.block_rank());
+    const int j = idx[blockIdx.x / C];
+    const SplitState S = st[j];
+    if (!jacobi_active(S, mode)) return;  // uniform over the cluster
+    const SplitJob& J = jobs[j];
+    const SlotBuffers Bf = slots[J.slot];
+    const double2* src;
+    int sr, sc, ld, rows_of_src;
+    jacobi_task(J, S, Bf, mode, src, sr, sc, ld, rows_of_src);
+    const int M = rows_of_src ? sc : sr;
+    const int N = rows_of_src ? sr : sc;
+    const int K = (N + 2 * b - 1) / (2 * b);
+    const int nblk = 2 * K;
+    const int Np = nblk * b;
+    const int len = M + Np;
+    const size_t blk = size_t(b) * len;
+    T* G = reinterpret_cast<T*>(Bf.gs);
+    if (G == nullptr) {  // a state sized without the workspace (uniform over the cluster)
+        if (threadIdx.x == 0 && rank == 0) atomicOr(status, kStatusBadShape);
+        return;
+    }
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sA = reinterpret_cast<T*>(smem_raw);
+    T* sB = sA + blk;
+    __shared__ JacobiCtl ctl;
+    __shared__ double red[kJacobiThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int nthreads = blockDim.x;
+    const int nwarps = nthreads / 32;
+    auto src_at = [&](int i, int col) -> double2 {
+        return rows_of_src ? cconj(src[size_t(col) * ld + i]) : src[size_t(i) * ld + col];
+    };
+    if (tid == 0) ctl.rot = 0;
+    // Frobenius norm: CTA r reads columns r, r+C, ...
+    double part = 0;
+    for (int col = rank; col < N; col += C)
+        for (int i = tid; i < M; i += nthreads) part += cnorm2(src_at(i, col));
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if (lane == 0) red[wid] = part;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0;
+        for (int w = 0; w < nwarps; ++w) t += red[w];
+        ctl.fro_part = t;
+    }
+    cluster.sync();
+    double fro2 = 0;
+    for (int r = 0; r < C; ++r) fro2 += cluster.map_shared_rank(&ctl, r)->fro_part;
+    const double dust = sqrt(fro2) * kDustRel;
+    const double dust2 = dust * dust;
+    // W (dust-zeroed, zero padding columns) and Z = identity into the workspace.
+    for (int col = rank; col < Np; col += C) {
+        T* x = G + size_t(col) * len;
+        for (int i = tid; i < len; i += nthreads) {
+            double2 v;
+            if (i < M) {
+                v = col < N ? src_at(i, col) : cmake(0, 0);
+                if (cnorm2(v) < dust2) v = cmake(0, 0);
+            } else {
+                v = cmake(i - M == col ? 1.0 : 0.0, 0.0);
+            }
+            x[i] = to_store<T>(v);
+        }
+    }
+    __threadfence();
+    cluster.sync();
+    const double tol = kF64 ? 1e-14 : 4e-6;
+    const double stop_rel2 = kF64 ? 1e-16 : 4e-6;
+    const double noise_floor = (kF64 ? 1e-32 : 1e-14) * fro2;
+    int sweep = 0;
+    bool converged = false;
+    for (; sweep < max_sweeps; ++sweep) {
+        if (tid == 0) {
+            ctl.rot = 0;
+            ctl.relmax_bits = 0ull;
+        }
+        __syncthreads();
+        int my_rot = 0;
+        double my_rel = 0.0;
+        for (int step = 0; step < nblk - 1; ++step) {
+            for (int ps = rank; ps < K; ps += C) {
+                const int ida = circle_at(ps, step, nblk), idb = circle_at(nblk - 1 - ps, step, nblk);
+                const T* ga = G + size_t(ida) * blk;
+                const T* gb = G + size_t(idb) * blk;
+                for (size_t e = tid; e < blk; e += nthreads) {
+                    sA[e] = __ldcg(ga + e);
+                    sB[e] = __ldcg(gb + e);
+                }
+                __syncthreads();
+                if (step == 0) {  // pairs inside each block, once per sweep
+                    for (int s2 = 0; s2 < b - 1; ++s2) {
+                        for (int pq = wid; pq < b; pq += nwarps) {
+                            const bool top = pq < b / 2;
+                            const int i = top ? pq : pq - b / 2;
+                            T* base = top ? sA : sB;
+                            const int e1 = circle_at(i, s2, b), e2 = circle_at(b - 1 - i, s2, b);
+                            my_rot += jacobi_rotate(base + size_t(e1) * len, base + size_t(e2) * len, M, len, tol,
+                                                    noise_floor, lane, my_rel);
+                        }
+                        __syncthreads();
+                    }
+                }
+                for (int k = 0; k < b; ++k) {
+                    for (int i = wid; i < b; i += nwarps) {
+                        const int e2 = (i + k) % b;
+                        my_rot += jacobi_rotate(sA + size_t(i) * len, sB + size_t(e2) * len, M, len, tol,
+                                                noise_floor, lane, my_rel);
+                    }
+                    __syncthreads();
+                }
+                T* wa = G + size_t(ida) * blk;
+                T* wb = G + size_t(idb) * blk;
+                for (size_t e = tid; e < blk; e += nthreads) {
+                    wa[e] = sA[e];
+                    wb[e] = sB[e];
+                }
+                __syncthreads();  // the next pair's loads overwrite sA, sB
+            }
+            __threadfence();
+            cluster.sync();
+        }
+        if (lane == 0 && my_rot) atomicAdd(&ctl.rot, my_rot);
+        if (lane == 0 && my_rel > 0.0) atomicMax(&ctl.relmax_bits, (unsigned long long)__double_as_longlong(my_rel));
+        __syncthreads();
+        int total = 0;
+        double relmax = 0.0;
+        cluster.sync();
+        for (int r = 0; r < C; ++r) {
+            const JacobiCtl* rc = cluster.map_shared_rank(&ctl, r);
+            total += rc->rot;
+            relmax = fmax(relmax, __longlong_as_double((long long)rc->relmax_bits));
+        }
+        cluster.sync();
+        if (total == 0 || relmax < stop_rel2) {
+            converged = true;
+            break;
+        }
+    }
+    if (tid == 0 && rank == 0) {
+        if (!converged) atomicOr(status, kStatusJacobiNoConvergence);
+        atomicAdd(counters + 0, 1ull);
+        atomicAdd(counters + 1, (unsigned long long)(converged ? sweep + 1 : sweep));
+    }
+    // Write back W, Z (first N rows) and the column norms; CTA r takes
+    // columns r, r+C, ..., one warp per column.
+    for (int col = rank + C * wid; col < N; col += C * nwarps) {
+        const T* x = G + size_t(col) * len;
+        double s2 = 0;
+        for (int r = lane; r < M; r += 32) {
+            const double2 v = to_f64(__ldcg(x + r));
+            s2 = fma(v.x, v.x, fma(v.y, v.y, s2));
+            Bf.w[size_t(col) * M + r] = v;
+        }
+        for (int r = lane; r < N; r += 32) Bf.z[size_t(col) * N + r] = to_f64(__ldcg(x + M + r));
+        for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        if (lane == 0) Bf.sigma[col] = sqrt(s2);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // finalize: stable descending sort, truncation rule, ambiguity test,
 // discarded weight and the split record.
 // ---------------------------------------------------------------------------
@@ -1013,6 +1196,21 @@ namespace wqc {
 const void* jacobi_kernel(bool fp32) {
     return fp32 ? reinterpret_cast<const void*>(jacobi_cluster_kernel<float2>)
                 : reinterpret_cast<const void*>(jacobi_cluster_kernel<double2>);
+}
+
+const void* jacobi_staged(bool fp32) {
+    return fp32 ? reinterpret_cast<const void*>(jacobi_staged_kernel<float2>)
+                : reinterpret_cast<const void*>(jacobi_staged_kernel<double2>);
+}
+
+cudaError_t launch_jacobi_staged(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
+                                 const SplitState* st, const SlotBuffers* slots, const int* idx, int mode,
+                                 int max_sweeps, int b, int* status, unsigned long long* counters) {
+    if (fp32)
+        return cudaLaunchKernelEx(&cfg, jacobi_staged_kernel<float2>, jobs, st, slots, idx, mode, max_sweeps, b,
+                                  status, counters);
+    return cudaLaunchKernelEx(&cfg, jacobi_staged_kernel<double2>, jobs, st, slots, idx, mode, max_sweeps, b, status,
+                              counters);
 }
 
 cudaError_t launch_jacobi(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, const SplitState* st,

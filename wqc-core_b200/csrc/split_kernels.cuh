@@ -31,6 +31,29 @@ const void* jacobi_kernel(bool fp32);
 cudaError_t launch_jacobi(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, const SplitState* st,
                           const SlotBuffers* slots, const int* idx, int mode, int max_sweeps, int* status,
                           unsigned long long* counters);
+// The staged variant for working matrices beyond a cluster's shared memory:
+// columns in the slot's `gs` workspace, blocks of b columns (b even).
+const void* jacobi_staged(bool fp32);
+cudaError_t launch_jacobi_staged(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
+                                 const SplitState* st, const SlotBuffers* slots, const int* idx, int mode,
+                                 int max_sweeps, int b, int* status, unsigned long long* counters);
+// Shape of the staged Jacobi for an M x N working matrix: the largest even
+// b <= 16 whose two blocks fit `smem_limit`; 0 if none.  Also returns the
+// shared memory of that choice.
+inline int jacobi_staged_b(int M, int N, size_t elem, size_t smem_limit, size_t* smem) {
+    for (int b = 16; b >= 2; b -= 2) {
+        const int K = (N + 2 * b - 1) / (2 * b);
+        const size_t len = size_t(M) + size_t(2) * K * b;
+        const size_t bytes = size_t(2) * b * len * elem;
+        if (bytes <= smem_limit) {
+            if (smem) *smem = bytes;
+            return b;
+        }
+    }
+    return 0;
+}
+// Elements (double2) of the `gs` workspace for two-site matrices up to R x R.
+inline size_t jacobi_staged_elems(int R) { return size_t(R + 32) * size_t(2 * R + 32); }
 // noise_rel: singular values below noise_rel * (largest) count as zero (0 in
 // the plain form; the precision form's FP32 rounding level).
 __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const SlotBuffers* slots, int mode,
