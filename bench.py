@@ -268,6 +268,70 @@ def differentiation_leg(W, torch, ctx, flush, cpu_budget: float) -> dict:
     return out
 
 
+def oracle_saturated_splits(budget_s: float):
+    """CPU leg of the large-chi form: the oracle on isolated saturated splits
+    of the chi 256 circuit (512 x 512 theta of random 256-bond sites, one CNOT,
+    reference rule: the range finder at ell 272), one thread, until budget_s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import wqc_cuda as W
+
+    rng = np.random.default_rng(7)
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s:
+        o = O.OracleMps(4, 256)
+        for i, (l, r) in enumerate([(1, 256), (256, 256), (256, 256), (256, 1)]):
+            t = rng.normal(size=(l, 2, r)) + 1j * rng.normal(size=(l, 2, r))
+            o.set_site(i, t / np.linalg.norm(t))
+        o.apply_2q_at(1, W.CNOT4, True)
+        done += 1
+    return done, time.perf_counter() - t0
+
+
+def large_chi_leg(W, torch, ctx, flush, cpu_budget: float) -> dict:
+    """Config 4's workload: 100 qubits, depth 100 blocks (RZ.RY.RZ on both
+    qubits, CNOT, RY on both, CNOT, RZ.RY.RZ on both, alternating pairs; every
+    10th layer a CCNOT on an adjacent triple and an H layer), chi_max 256, in
+    the plain and the precision form, one pass each from |0> to <0|psi>."""
+    w = C.config4()
+    out = {"workload": f"{w.name}: {w.n} qubits, chi_max {w.chi}, {len(w.gates)} gates, split rule reference"}
+    for name, prec in (("fp64", W.PRECISION_FP64), ("fp32", W.PRECISION_FP32)):
+        m = W.CudaMps(w.n, w.chi, ctx=ctx, precision=prec)
+        stream = torch.cuda.ExternalStream(m.stream())
+        flush.fill_(float(np.random.random()))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.apply_gates(w.gates)
+        m.amplitude_at_compact_zero()
+        e1.record(stream)
+        e1.synchronize()
+        sec = e0.elapsed_time(e1) * 1e-3
+        rec = m.split_records()
+        out[name] = {
+            "applies_per_s": len(rec) / sec,
+            "seconds": sec,
+            "splits": int(len(rec)),
+            "splits_512x512": int(np.sum((rec["rows"] == 512) & (rec["cols"] == 512))),
+            "paths": [int(x) for x in np.bincount(rec["path"], minlength=3)],
+            "peak_vram_bytes": m.peak_vram_bytes(),
+        }
+        m.close()
+    out["fp32_speedup"] = out["fp32"]["applies_per_s"] / out["fp64"]["applies_per_s"]
+    if cpu_budget > 0:
+        done, secs = oracle_saturated_splits(cpu_budget)
+        out["cpu_baseline"] = {
+            "value": done / secs,
+            "unit": UNIT,
+            "cores": 1,
+            "kind": "port",
+            "sample": f"FP64 restatement, one thread: {done} isolated saturated 512x512 splits (random 256-bond sites, "
+                      f"CNOT, range finder at ell 272) in {secs:.1f} s; the circuit's own first layers would take "
+                      f"tens of minutes to reach saturation on one thread",
+        }
+    return out
+
+
 def batch_leg(W, torch, ctx, count: int, flush, cpu_budget: float, precision: int = 0) -> dict:
     """The batching form: `count` independent slices (width U[20,60], depth
     U[10,50], chi_max from {16,32,64,128}) in one device state, one pass from
@@ -582,6 +646,8 @@ def run_cuda(args) -> None:
         if world == 1 and args.differentiation_leg:
             line["differentiation"] = differentiation_leg(W, torch, ctx, flush,
                                                           0.0 if args.no_cpu_baseline else args.cpu_budget)
+        if world == 1 and args.large_chi_leg:
+            line["large_chi"] = large_chi_leg(W, torch, ctx, flush, 0.0 if args.no_cpu_baseline else args.cpu_budget)
         if world == 1 and args.precision_leg:
             line["precision_form"] = precision_leg(W, torch, ctx, w, rule, args.steps, flush, value)
             if args.batch_slices > 0:
@@ -607,6 +673,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-differentiation-leg", dest="differentiation_leg", action="store_false",
                     help="skip the parameter-shift gradient of the 32-qubit ansatz run after the timed steps")
+    ap.add_argument("--no-large-chi-leg", dest="large_chi_leg", action="store_false",
+                    help="skip the 100-qubit chi 256 circuit run after the timed steps")
     ap.add_argument("--no-precision-leg", dest="precision_leg", action="store_false",
                     help="skip the precision-form (complex64 Jacobi) leg run after the timed steps")
     ap.add_argument("--batch-slices", type=int, default=512,

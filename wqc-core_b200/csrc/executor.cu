@@ -882,14 +882,25 @@ wqc_status reset_sites(wqc_mps* m) {
 
 wqc_status sync_status(wqc_mps* m) {
     CUDA_TRY(cudaStreamSynchronize(m->stream));
-    int st = 0;
-    CUDA_TRY(cudaMemcpy(&st, m->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    int stv[5] = {0, 0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpy(stv, m->d_status, sizeof(stv), cudaMemcpyDeviceToHost));
+    const int st = stv[0];
     if (*m->h_cancel) return fail(WQC_ERR_CANCELLED, "computation cancelled: the client has gone");
     if (st & kStatusCancelled) return fail(WQC_ERR_CANCELLED, "computation cancelled: the client has gone");
     if (st & kStatusTruncationRejected) return fail(WQC_ERR_TRUNCATION_REJECTED, "mps bond exceeded chi");
     if (st & kStatusNonFinite) return fail(WQC_ERR_SVD_FAILED, "SVD of a two-site matrix produced non-finite values");
-    if (st & kStatusJacobiNoConvergence)
-        return fail(WQC_ERR_SVD_FAILED, "Jacobi SVD of a two-site matrix did not converge in 60 sweeps");
+    if (st & kStatusJacobiNoConvergence) {
+        const unsigned long long bits = (static_cast<unsigned long long>(static_cast<unsigned>(stv[3])) << 32) |
+                                        static_cast<unsigned>(stv[4]);
+        double rel2;
+        std::memcpy(&rel2, &bits, sizeof(rel2));
+        char buf[200];
+        std::snprintf(buf, sizeof(buf),
+                      "Jacobi SVD of a two-site matrix did not converge in 60 sweeps (split %d: last sweep %d "
+                      "rotations, max |gamma|/sqrt(alpha beta) %.3e)",
+                      stv[1] - 1, stv[2], std::sqrt(rel2));
+        return fail(WQC_ERR_SVD_FAILED, buf);
+    }
     if (st & kStatusBadShape) return fail(WQC_ERR_INVALID, "two-site matrix without a Jacobi workspace");
     return WQC_OK;
 }

@@ -33,7 +33,10 @@ __global__ void __launch_bounds__(256) apply_1q_kernel(const OneQubitOp* ops, co
 // Every site back to |0> (mps.rs:101-109): [1, 0] with bonds 1.
 __global__ void reset_sites_kernel(DeviceMps mps) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) *mps.status = 0;
+    if (i == 0) {
+        mps.status[0] = 0;
+        mps.status[1] = 0;
+    }
     if (i >= mps.n) return;
     mps.site[i][0] = cmake(1.0, 0.0);
     mps.site[i][1] = cmake(0.0, 0.0);

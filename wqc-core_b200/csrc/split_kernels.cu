@@ -497,13 +497,16 @@ __device__ __forceinline__ int circle_at(int pos, int step, int b) {
 // warp-uniform.  Returns 1 when a rotation was applied.
 //
 // Two guards keep every applied rotation unitary and the sweep finite:
-// |gamma| is taken with hypot, so the phase stays of unit modulus when the
-// products underflow; and a pair whose Gram scale sqrt(alpha*beta) is below
-// floor = (1e-16 * ||W||_F)^2 is left alone.  Such a pair is a column at
-// rounding-noise level against another column; rotating it moves nothing
-// above 1e-32 ||W||_F^2, while exactly parallel columns (a rank-deficient
-// theta) would otherwise be re-rotated every sweep until their products
-// reach the subnormal range.
+// |gamma| is taken with hypot when |gamma|^2 nears the subnormal range, so
+// the phase stays of unit modulus; and a pair whose smaller column has
+// alpha <= floor = (1e-15 ||W||_F)^2 (FP32 columns: (1e-6 ||W||_F)^2) is left
+// alone.  Such a column is at the storage's rounding level: its direction is
+// noise, rotating it against another column changes nothing above
+// floor * ||W||_F^2, and rotating it anyway lets exactly parallel columns (a
+// rank-deficient theta) be re-rotated every sweep until their products go
+// subnormal, and pairs of noise columns keep |gamma|/sqrt(alpha beta) near
+// 1e-8 forever (seen on a 256 x 144 range-finder matrix of the 50-qubit
+// circuit, which then never met the stop test).
 //
 // The columns are complex128 (double2) in the plain form and complex64
 // (float2) in the precision form.  The precision form accumulates the dot
@@ -545,7 +548,7 @@ __device__ __forceinline__ int jacobi_rotate(T* xp, T* xq, int M, int len, doubl
     // tol^2 alpha beta, one reciprocal square root for the phase.
     const double g2 = fma(gr, gr, gi * gi);
     const double ab = a * bb;
-    if (ab <= noise_floor * noise_floor) return 0;
+    if (fmin(a, bb) <= noise_floor) return 0;  // the smaller column is at the storage's rounding level
     relmax = fmax(relmax, g2 / ab);  // squared ratio; the caller compares with squared bounds
     if (g2 == 0.0 || g2 <= tol * tol * ab) return 0;
     double pr, pi, zeta;
@@ -734,9 +737,11 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
     // storage's rounding level against ||W||_F are left alone (noise floor).
     const double tol = kF64 ? 1e-14 : 4e-6;
     const double stop_rel2 = kF64 ? 1e-16 : 4e-6;  // squared: 1e-8 and 2e-3
-    const double noise_floor = (kF64 ? 1e-32 : 1e-14) * fro2;
+    const double noise_floor = (kF64 ? 1e-30 : 1e-12) * fro2;  // squared column norm: 1e-15 (1e-6) of ||W||_F
     int sweep = 0;
     bool converged = false;
+    int ctl_rot_last = 0;
+    unsigned long long ctl_relmax_bits_last = 0ull;
     for (; sweep < max_sweeps; ++sweep) {
         if (tid == 0) {
             ctl.rot = 0;
@@ -817,13 +822,25 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
         // sweep orthogonal to stop_rel (FP64: 1e-8, leaving them at about
         // 1e-16, below the rotation tolerance, so a verification sweep would
         // rotate nothing).
+        ctl_rot_last = total;
+        ctl_relmax_bits_last = (unsigned long long)__double_as_longlong(relmax);
         if (total == 0 || relmax < stop_rel2) {  // relmax holds squared ratios
             converged = true;
             break;
         }
     }
     if (tid == 0 && rank == 0) {
-        if (!converged) atomicOr(status, kStatusJacobiNoConvergence);
+        if (!converged) {
+            atomicOr(status, kStatusJacobiNoConvergence);
+            // The first such split, its last sweep's rotation count and largest
+            // squared |gamma| / sqrt(alpha beta), for the error message.
+            if (atomicCAS(status + 1, 0, J.seq + 1) == 0) {
+                const unsigned long long bits = ctl_relmax_bits_last;
+                status[2] = ctl_rot_last;
+                status[3] = int(bits >> 32);
+                status[4] = int(bits & 0xffffffffull);
+            }
+        }
         atomicAdd(counters + 0, 1ull);
         atomicAdd(counters + 1, (unsigned long long)(converged ? sweep + 1 : sweep));
     }
@@ -940,9 +957,11 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const Spl
     cluster.sync();
     const double tol = kF64 ? 1e-14 : 4e-6;
     const double stop_rel2 = kF64 ? 1e-16 : 4e-6;
-    const double noise_floor = (kF64 ? 1e-32 : 1e-14) * fro2;
+    const double noise_floor = (kF64 ? 1e-30 : 1e-12) * fro2;  // squared column norm: 1e-15 (1e-6) of ||W||_F
     int sweep = 0;
     bool converged = false;
+    int ctl_rot_last = 0;
+    unsigned long long ctl_relmax_bits_last = 0ull;
     for (; sweep < max_sweeps; ++sweep) {
         if (tid == 0) {
             ctl.rot = 0;
@@ -1005,13 +1024,25 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const Spl
             relmax = fmax(relmax, __longlong_as_double((long long)rc->relmax_bits));
         }
         cluster.sync();
+        ctl_rot_last = total;
+        ctl_relmax_bits_last = (unsigned long long)__double_as_longlong(relmax);
         if (total == 0 || relmax < stop_rel2) {
             converged = true;
             break;
         }
     }
     if (tid == 0 && rank == 0) {
-        if (!converged) atomicOr(status, kStatusJacobiNoConvergence);
+        if (!converged) {
+            atomicOr(status, kStatusJacobiNoConvergence);
+            // The first such split, its last sweep's rotation count and largest
+            // squared |gamma| / sqrt(alpha beta), for the error message.
+            if (atomicCAS(status + 1, 0, J.seq + 1) == 0) {
+                const unsigned long long bits = ctl_relmax_bits_last;
+                status[2] = ctl_rot_last;
+                status[3] = int(bits >> 32);
+                status[4] = int(bits & 0xffffffffull);
+            }
+        }
         atomicAdd(counters + 0, 1ull);
         atomicAdd(counters + 1, (unsigned long long)(converged ? sweep + 1 : sweep));
     }

@@ -209,6 +209,11 @@ def large_chi(n: int = 100, depth: int = 100, seed: int = 20261207) -> list:
     return gates
 
 
+def config4(depth: int = 100, seed: int = 20261207) -> Workload:
+    """100 qubits, depth 100 blocks (large_chi), chi_max = 256: theta up to 512 x 512."""
+    return Workload(f"blocks100_d{depth}_chi256", 100, 256, gates_array(large_chi(100, depth, seed)), seed)
+
+
 def split_plan(gates: np.ndarray) -> int:
     """Number of two-site splits the reference performs for this gate list
     (SWAP routing at mps.rs:353-375, CCNOT as 6 CNOTs at mps.rs:657-677)."""
