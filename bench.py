@@ -388,6 +388,21 @@ def batch_leg(W, torch, ctx, count: int, flush, cpu_budget: float, precision: in
     return out
 
 
+def aggregate_ranks(dist, device, dev_ms: float, wall_s: float):
+    """Max over ranks of the timed steps' device and wall times.  Every rank
+    runs its own replica (a circuit does not shard: weak scaling, no
+    collective on the data path), so the whole job's throughput is the work of
+    all ranks over the slowest rank's time; this reduction, at the end of the
+    timed region, is the only collective."""
+    if dist is None:
+        return dev_ms, wall_s
+    import torch
+
+    t = torch.tensor([dev_ms, wall_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t[0]), float(t[1])
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -574,10 +589,7 @@ def run_cuda(args) -> None:
     stats = m.kernel_stats()
     total_dev_ms = sum(dev_ms)
     total_wall = sum(wall_s)
-    if dist is not None:
-        t = torch.tensor([total_dev_ms, total_wall], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_dev_ms, total_wall = float(t[0]), float(t[1])
+    total_dev_ms, total_wall = aggregate_ranks(dist, "cuda", total_dev_ms, total_wall)
     value = world * splits / (total_dev_ms * 1e-3)
     e2e = world * splits / total_wall
     jac_ms = stats["milliseconds"]["jacobi_svd"]
