@@ -262,10 +262,12 @@ void set_kernel_attributes() {
         if (g_attr_err == cudaSuccess)
             g_attr_err = cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     }
-    if (g_attr_err == cudaSuccess)
-        g_attr_err = cudaFuncSetAttribute(qr_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLimit));
-    if (g_attr_err == cudaSuccess)
-        g_attr_err = cudaFuncSetAttribute(qr_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (const void* f : {qr_cluster(false), qr_cluster(true)}) {
+        if (g_attr_err == cudaSuccess)
+            g_attr_err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLimit));
+        if (g_attr_err == cudaSuccess)
+            g_attr_err = cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
     if (g_attr_err == cudaSuccess)
         g_attr_err = cudaFuncSetAttribute(amplitude_zero_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     if (g_attr_err == cudaSuccess)
@@ -808,17 +810,24 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                 rsvd_gemm_kernel<<<dim3(te, tr, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageY0);
                 rsvd_gemm_kernel<<<dim3(te, tc, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageZ);
                 rsvd_gemm_kernel<<<dim3(te, tr, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageY);
+                // Columns in shared memory on the smallest cluster that holds
+                // them; else in global memory on the largest cluster.
                 int cq = 0;
+                bool qglobal = false;
                 for (int c = 8; c <= m->ctx->max_cluster; c *= 2)
                     if (qr_cluster_smem_bytes(w.max_rows, w.max_ell, c) <= kSmemLimit) {
                         cq = c;
                         break;
                     }
+                if (!cq && qr_cluster_smem_bytes(w.max_rows, w.max_ell, m->ctx->max_cluster, true) <= kSmemLimit) {
+                    cq = m->ctx->max_cluster;
+                    qglobal = true;
+                }
                 if (cq) {
                     cudaLaunchConfig_t cfg = {};
                     cfg.gridDim = dim3(nj * cq);
                     cfg.blockDim = dim3(kQrClusterThreads);
-                    cfg.dynamicSmemBytes = qr_cluster_smem_bytes(w.max_rows, w.max_ell, cq);
+                    cfg.dynamicSmemBytes = qr_cluster_smem_bytes(w.max_rows, w.max_ell, cq, qglobal);
                     cfg.stream = m->stream;
                     cudaLaunchAttribute attr[1];
                     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -827,8 +836,7 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                     attr[0].val.clusterDim.z = 1;
                     cfg.attrs = attr;
                     cfg.numAttrs = 1;
-                    CUDA_TRY(cudaLaunchKernelEx(&cfg, qr_cluster_kernel, d_jobs, (const SplitState*)m->d_state,
-                                                (const SlotBuffers*)m->d_slots));
+                    CUDA_TRY(launch_qr_cluster(qglobal, cfg, d_jobs, m->d_state, m->d_slots));
                 } else {
                     householder_qr_kernel<<<nj, 512, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots);
                 }

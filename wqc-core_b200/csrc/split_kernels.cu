@@ -351,7 +351,10 @@ __global__ void __launch_bounds__(kQrThreads) householder_qr_kernel(const SplitJ
 // columns; after one cluster barrier the CTAs to its right copy v_c through
 // distributed shared memory and update theirs.  Q is then accumulated
 // backward with every reflector read from its owner.  Same arithmetic as the
-// single-CTA kernel above.
+// single-CTA kernel above.  With kGlobalCols the columns stay in the slot's
+// Y and Q buffers (L2-resident) instead of shared memory, for shapes whose
+// columns do not fit (Y of 512 x 272 at chi 256); only the reflector
+// broadcast and the local reflector copy live in shared memory.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void reflect_columns(double2* cols, int ldc, int count, const double2* v, double2 t,
                                                 int c, int m, int lane, int wid, int nw) {
@@ -368,6 +371,7 @@ __device__ __forceinline__ void reflect_columns(double2* cols, int ldc, int coun
     }
 }
 
+template <bool kGlobalCols>
 __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const SplitJob* jobs, const SplitState* st,
                                                                            const SlotBuffers* slots) {
     cg::cluster_group cluster = cg::this_cluster();
@@ -381,15 +385,16 @@ __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const 
     const int cpc = (n + C - 1) / C;
     const int c0 = min(n, rank * cpc), c1 = min(n, c0 + cpc), nloc = c1 - c0;
     extern __shared__ __align__(16) double2 qsm[];
-    double2* Ys = qsm;                              // cpc columns of m
-    double2* Qs = Ys + size_t(cpc) * m;             // cpc columns of m
-    double2* bcast = Qs + size_t(cpc) * m;          // 2 slots of m
-    double2* vloc = bcast + size_t(2) * m;          // m
-    double2* taus = vloc + m;                       // cpc local tau values
+    double2* Ys = kGlobalCols ? B.y + size_t(c0) * m : qsm;                      // cpc columns of m
+    double2* Qs = kGlobalCols ? B.q + size_t(c0) * m : qsm + size_t(cpc) * m;    // cpc columns of m
+    double2* bcast = kGlobalCols ? qsm : qsm + size_t(2) * cpc * m;              // 2 slots of m
+    double2* vloc = bcast + size_t(2) * m;                                        // m
+    double2* taus = vloc + m;                                                     // cpc local tau values
     __shared__ double red[kQrClusterThreads / 32];
     __shared__ double2 s_tau[2];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = kQrClusterThreads / 32;
-    for (int e = tid; e < nloc * m; e += kQrClusterThreads) Ys[e] = B.y[size_t(c0) * m + e];
+    if (!kGlobalCols)
+        for (int e = tid; e < nloc * m; e += kQrClusterThreads) Ys[e] = B.y[size_t(c0) * m + e];
     __syncthreads();
     for (int c = 0; c < n; ++c) {
         const int owner = c / cpc;
@@ -438,6 +443,7 @@ __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const 
             __syncthreads();
         }
     }
+    if (kGlobalCols) __threadfence();
     cluster.sync();  // every reflector is final
     for (int e = tid; e < nloc * m; e += kQrClusterThreads) {
         const int r = e % m, cc = c0 + e / m;
@@ -446,8 +452,13 @@ __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const 
     __syncthreads();
     for (int c = nloc > 0 ? c1 - 1 : -1; c >= 0; --c) {
         const int owner = c / cpc;
-        const double2* rcol = cluster.map_shared_rank(Ys, owner) + size_t(c - owner * cpc) * m;
-        for (int i = c + 1 + tid; i < m; i += kQrClusterThreads) vloc[i] = rcol[i];
+        if (kGlobalCols) {
+            const double2* rcol = B.y + size_t(c) * m;
+            for (int i = c + 1 + tid; i < m; i += kQrClusterThreads) vloc[i] = __ldcg(rcol + i);
+        } else {
+            const double2* rcol = cluster.map_shared_rank(Ys, owner) + size_t(c - owner * cpc) * m;
+            for (int i = c + 1 + tid; i < m; i += kQrClusterThreads) vloc[i] = rcol[i];
+        }
         if (tid == 0) {
             vloc[c] = cmake(1.0, 0.0);
             s_tau[0] = *(cluster.map_shared_rank(taus, owner) + (c - owner * cpc));
@@ -459,8 +470,10 @@ __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const 
             reflect_columns(Qs + size_t(first - c0) * m, m, c1 - first, vloc, t, c, m, lane, wid, nw);
         __syncthreads();
     }
-    for (int e = tid; e < nloc * m; e += kQrClusterThreads) B.q[size_t(c0) * m + e] = Qs[e];
-    for (int e = tid; e < nloc * m; e += kQrClusterThreads) B.y[size_t(c0) * m + e] = Ys[e];
+    if (!kGlobalCols) {
+        for (int e = tid; e < nloc * m; e += kQrClusterThreads) B.q[size_t(c0) * m + e] = Qs[e];
+        for (int e = tid; e < nloc * m; e += kQrClusterThreads) B.y[size_t(c0) * m + e] = Ys[e];
+    }
     if (tid < nloc) B.tau[c0 + tid] = taus[tid];
     cluster.sync();  // no CTA leaves while another may still read its shared memory
 }
@@ -1227,6 +1240,17 @@ namespace wqc {
 const void* jacobi_kernel(bool fp32) {
     return fp32 ? reinterpret_cast<const void*>(jacobi_cluster_kernel<float2>)
                 : reinterpret_cast<const void*>(jacobi_cluster_kernel<double2>);
+}
+
+const void* qr_cluster(bool global_cols) {
+    return global_cols ? reinterpret_cast<const void*>(qr_cluster_kernel<true>)
+                       : reinterpret_cast<const void*>(qr_cluster_kernel<false>);
+}
+
+cudaError_t launch_qr_cluster(bool global_cols, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
+                              const SplitState* st, const SlotBuffers* slots) {
+    if (global_cols) return cudaLaunchKernelEx(&cfg, qr_cluster_kernel<true>, jobs, st, slots);
+    return cudaLaunchKernelEx(&cfg, qr_cluster_kernel<false>, jobs, st, slots);
 }
 
 const void* jacobi_staged(bool fp32) {

@@ -18,11 +18,15 @@ __global__ void omega_kernel(const SplitJob* jobs, const SplitState* st, const S
 __global__ void rsvd_gemm_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots, int stage);
 __global__ void householder_qr_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
 constexpr int kQrClusterThreads = 256;
-__global__ void qr_cluster_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
-// Shared memory of qr_cluster_kernel for an m x n Y on a cluster of C CTAs.
-inline size_t qr_cluster_smem_bytes(int m, int n, int C) {
+// The cluster Householder QR (columns in shared memory, or with global_cols
+// in the slot's Y and Q buffers), reached through these host functions.
+const void* qr_cluster(bool global_cols);
+cudaError_t launch_qr_cluster(bool global_cols, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
+                              const SplitState* st, const SlotBuffers* slots);
+// Shared memory of the cluster QR for an m x n Y on a cluster of C CTAs.
+inline size_t qr_cluster_smem_bytes(int m, int n, int C, bool global_cols = false) {
     const int cpc = (n + C - 1) / C;
-    return (size_t(2) * cpc * m + size_t(3) * m + cpc) * sizeof(double2);
+    return ((global_cols ? size_t(0) : size_t(2) * cpc * m) + size_t(3) * m + cpc) * sizeof(double2);
 }
 // The cluster Jacobi SVD kernel (a template over the column type: complex128
 // in the plain form, complex64 in the precision form), reached from other
