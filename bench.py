@@ -38,9 +38,11 @@ METRIC = "2q-gate applies/s"
 UNIT = "2q applies/s"
 
 
-def workload(name: str):
+def workload(name: str, depth: int = 0):
     if name == "config0":
         w = C.config0()
+    elif name == "config4":
+        w = C.config4(depth or 100)
     else:
         w = C.config1()
     return w
@@ -407,7 +409,7 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w = workload(args.workload)
+    w = workload(args.workload, args.depth)
     threads = os.cpu_count() or 1
     budget = args.reference_budget
     skip = SATURATED_LAYERS.get(args.workload, 0)
@@ -537,7 +539,7 @@ def run_cuda(args) -> None:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    w = workload(args.workload)
+    w = workload(args.workload, args.depth)
     rule = W.SPLIT_RULE_EXACT if args.split_rule == "exact" else W.SPLIT_RULE_REFERENCE
     ctx = W.Context(local)
     m = W.CudaMps(w.n, w.chi, ctx=ctx)
@@ -678,7 +680,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("cuda", "reference"), default="cuda")
-    ap.add_argument("--workload", choices=("config1", "config0"), default="config1")
+    ap.add_argument("--workload", choices=("config1", "config0", "config4"), default="config1",
+                    help="config1: 50 qubits, depth 40, chi 128 (the headline); config0: 16 qubits, chi 32; "
+                         "config4: 100 qubits, chi 256 (--depth layers, default 100)")
+    ap.add_argument("--depth", type=int, default=0, help="layers of the config4 circuit (0: 100)")
     ap.add_argument("--split-rule", choices=("reference", "exact"), default="reference")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--reference-budget", type=float, default=10.0)

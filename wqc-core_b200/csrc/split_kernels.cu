@@ -994,14 +994,19 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const Spl
                 }
                 __syncthreads();
                 if (step == 0) {  // pairs inside each block, once per sweep
-                    for (int s2 = 0; s2 < b - 1; ++s2) {
-                        for (int pq = wid; pq < b; pq += nwarps) {
-                            const bool top = pq < b / 2;
-                            const int i = top ? pq : pq - b / 2;
+                    // Circle method on bb = b rounded up to even positions; for
+                    // an odd b the extra position is a dummy and its pair is
+                    // skipped (uniformly per warp).
+                    const int bb = b + (b & 1);
+                    for (int s2 = 0; s2 < bb - 1; ++s2) {
+                        for (int pq = wid; pq < bb; pq += nwarps) {
+                            const bool top = pq < bb / 2;
+                            const int i = top ? pq : pq - bb / 2;
                             T* base = top ? sA : sB;
-                            const int e1 = circle_at(i, s2, b), e2 = circle_at(b - 1 - i, s2, b);
-                            my_rot += jacobi_rotate(base + size_t(e1) * len, base + size_t(e2) * len, M, len, tol,
-                                                    noise_floor, lane, my_rel);
+                            const int e1 = circle_at(i, s2, bb), e2 = circle_at(bb - 1 - i, s2, bb);
+                            if (e1 < b && e2 < b)
+                                my_rot += jacobi_rotate(base + size_t(e1) * len, base + size_t(e2) * len, M, len,
+                                                        tol, noise_floor, lane, my_rel);
                         }
                         __syncthreads();
                     }

@@ -41,20 +41,29 @@ const void* jacobi_staged(bool fp32);
 cudaError_t launch_jacobi_staged(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
                                  const SplitState* st, const SlotBuffers* slots, const int* idx, int mode,
                                  int max_sweeps, int b, int* status, unsigned long long* counters);
-// Shape of the staged Jacobi for an M x N working matrix: the largest even
-// b <= 16 whose two blocks fit `smem_limit`; 0 if none.  Also returns the
-// shared memory of that choice.
-inline int jacobi_staged_b(int M, int N, size_t elem, size_t smem_limit, size_t* smem) {
-    for (int b = 16; b >= 2; b -= 2) {
+// Shape of the staged Jacobi for an M x N working matrix on a cluster of C
+// CTAs: the block width b <= 16 whose two blocks fit `smem_limit` and whose
+// sweep is shortest, counted in dependent rotation rounds: (2K-1) steps of
+// ceil(K / C) block pairs per CTA, b rounds each, K = ceil(N / 2b) pairs.
+// 0 if none fits.  Also returns the shared memory of that choice.
+inline int jacobi_staged_b(int M, int N, size_t elem, size_t smem_limit, size_t* smem, int C = 16) {
+    int best = 0;
+    long best_rounds = 0;
+    size_t best_bytes = 0;
+    for (int b = 2; b <= 16; ++b) {
         const int K = (N + 2 * b - 1) / (2 * b);
         const size_t len = size_t(M) + size_t(2) * K * b;
         const size_t bytes = size_t(2) * b * len * elem;
-        if (bytes <= smem_limit) {
-            if (smem) *smem = bytes;
-            return b;
+        if (bytes > smem_limit) continue;
+        const long rounds = long(2 * K - 1) * ((K + C - 1) / C) * b;
+        if (!best || rounds < best_rounds) {
+            best = b;
+            best_rounds = rounds;
+            best_bytes = bytes;
         }
     }
-    return 0;
+    if (best && smem) *smem = best_bytes;
+    return best;
 }
 // Elements (double2) of the `gs` workspace for two-site matrices up to R x R.
 inline size_t jacobi_staged_elems(int R) { return size_t(R + 32) * size_t(2 * R + 32); }
