@@ -538,17 +538,36 @@ struct JacobiReal<float2> {
 };
 
 template <typename T>
-__device__ __forceinline__ int jacobi_rotate(T* xp, T* xq, int M, int len, double tol, double noise_floor,
-                                             int lane, double& relmax) {
+__device__ __forceinline__ int jacobi_rotate(T* __restrict__ xp, T* __restrict__ xq, int M, int len, double tol,
+                                             double noise_floor, int lane, double& relmax) {
     using R = typename JacobiReal<T>::R;
-    R a_ = 0, b_ = 0, gr_ = 0, gi_ = 0;
-    for (int r = lane; r < M; r += 32) {
-        const T u = xp[r], v = xq[r];
+    // Two rows per lane per iteration into two accumulator sets: the loads
+    // of the second row overlap the first's FMAs and the dependent chains
+    // are half as long (the columns are distinct, hence __restrict__).
+    R a_ = 0, b_ = 0, gr_ = 0, gi_ = 0, a1 = 0, b1 = 0, gr1 = 0, gi1 = 0;
+    int r0 = lane;
+    for (; r0 + 32 < M; r0 += 64) {
+        const T u = xp[r0], v = xq[r0], u1 = xp[r0 + 32], v1 = xq[r0 + 32];
+        a_ = fma(u.x, u.x, fma(u.y, u.y, a_));
+        b_ = fma(v.x, v.x, fma(v.y, v.y, b_));
+        gr_ = fma(u.x, v.x, fma(u.y, v.y, gr_));
+        gi_ = fma(u.x, v.y, fma(-u.y, v.x, gi_));
+        a1 = fma(u1.x, u1.x, fma(u1.y, u1.y, a1));
+        b1 = fma(v1.x, v1.x, fma(v1.y, v1.y, b1));
+        gr1 = fma(u1.x, v1.x, fma(u1.y, v1.y, gr1));
+        gi1 = fma(u1.x, v1.y, fma(-u1.y, v1.x, gi1));
+    }
+    if (r0 < M) {
+        const T u = xp[r0], v = xq[r0];
         a_ = fma(u.x, u.x, fma(u.y, u.y, a_));
         b_ = fma(v.x, v.x, fma(v.y, v.y, b_));
         gr_ = fma(u.x, v.x, fma(u.y, v.y, gr_));
         gi_ = fma(u.x, v.y, fma(-u.y, v.x, gi_));
     }
+    a_ += a1;
+    b_ += b1;
+    gr_ += gr1;
+    gi_ += gi1;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a_ += __shfl_xor_sync(0xffffffffu, a_, o);
@@ -582,13 +601,32 @@ __device__ __forceinline__ int jacobi_rotate(T* xp, T* xq, int M, int len, doubl
     // With w = s * phase the rephased rotation (svd_guard.rs:189-197) is
     // xp' = c xp - conj(w) xq,  xq' = w xp + c xq   (|phase| = 1).
     const R wr = R(s * pr), wi = R(s * pi), cr = R(c);
-    for (int r = lane; r < len; r += 32) {
-        const T u = xp[r], v = xq[r];
-        T p, q;
+    auto rot = [&](const T u, const T v, T& p, T& q) {
         p.x = fma(cr, u.x, -fma(wr, v.x, wi * v.y));
         p.y = fma(cr, u.y, -fma(wr, v.y, -wi * v.x));
         q.x = fma(wr, u.x, fma(-wi, u.y, cr * v.x));
         q.y = fma(wr, u.y, fma(wi, u.x, cr * v.y));
+    };
+    // Four rows per lane per iteration: all loads issue before the stores.
+    int r = lane;
+    for (; r + 96 < len; r += 128) {
+        T u[4], v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            u[k] = xp[r + 32 * k];
+            v[k] = xq[r + 32 * k];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            T p, q;
+            rot(u[k], v[k], p, q);
+            xp[r + 32 * k] = p;
+            xq[r + 32 * k] = q;
+        }
+    }
+    for (; r < len; r += 32) {
+        T p, q;
+        rot(xp[r], xq[r], p, q);
         xp[r] = p;
         xq[r] = q;
     }
