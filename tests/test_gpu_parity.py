@@ -294,6 +294,30 @@ def test_exact_split_of_full_rank_theta_matches_oracle(cuda_ctx, bond):
     assert abs(float(info["discarded_weight"]) - float(ref["discarded_weight"])) <= DISC_ATOL
 
 
+def test_precision_form_staged_split_at_chi_256(cuda_ctx):
+    """The precision form's staged Jacobi (complex64 columns in the global
+    workspace) on a full-rank 512 x 512 theta under the exact rule: kept
+    product within FP32 accuracy of the oracle, same rank, discarded weight
+    within 1e-5 of the weight's scale."""
+    rng = np.random.default_rng(512)
+    sites = _random_sites(rng, [(1, 256), (256, 256), (256, 256), (256, 1)])
+    m = W.CudaMps(4, 256, ctx=cuda_ctx, precision=W.PRECISION_FP32)
+    m.set_split_rule(W.SPLIT_RULE_EXACT)
+    o = O.OracleMps(4, 256)
+    o.set_split_rule(1)
+    for i, s in enumerate(sites):
+        m.set_site(i, s)
+        o.set_site(i, s)
+    info = m.apply_two_qubit_at_positions(1, 2, W.CZ4, False, want_info=True)
+    o.apply_2q_at(1, W.CZ4, False)
+    ref = o.records()[0]
+    assert int(info["chi"]) == int(ref["chi"]) == 256, (ref, info)
+    got, want = _theta(m.site(1), m.site(2)), _theta(o.site(1), o.site(2))
+    assert np.abs(got - want).max() / np.abs(want).max() <= 1e-4
+    w = float(ref["discarded_weight"])
+    assert abs(float(info["discarded_weight"]) - w) <= 1e-5 * max(w, 1e-3)
+
+
 def test_range_finder_split_at_chi_256_matches_oracle(cuda_ctx):
     """A 512x512 split at chi 256 takes the range finder (ell 272); B^H
     (512 x 272) exceeds a cluster's shared memory and runs on the staged
