@@ -230,7 +230,7 @@ WQC_API wqc_status wqc_expectation_pauli_noalloc(const double* sites, uint64_t s
  * job in that slot) to host memory, at most `bytes`.  which: 0 theta
  * (rows x cols, row-major), 1 Omega, 2 A*Omega, 3 A^H*(A*Omega), 4 Y then
  * Householder vectors (column-major), 5 thin Q (column-major), 6 Q^H A,
- * 7 Jacobi W, 8 Jacobi Z (column-major), 9 column norms, 10 sort
+ * 7 Jacobi W, 8 the range finder's B W (kept columns; column-major), 9 column norms, 10 sort
  * permutation, 11 Householder scalars, 12 the split's device state. */
 WQC_API wqc_status wqc_mps_debug_workspace(wqc_mps* mps, uint32_t slot, int32_t which, void* out, uint64_t bytes);
 

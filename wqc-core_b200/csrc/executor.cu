@@ -290,7 +290,7 @@ int choose_cluster(int M, int N, int max_c, int njobs, int sm_count, size_t elem
         if (jacobi_smem_bytes(M, N, Cc, elem) > kSmemLimit) continue;
         const int Np = round_up(N, 4 * Cc), b = Np / (2 * Cc);
         if (b > 16 && Cc < max_c) continue;  // more pairs than warps
-        const double len = M + Np;
+        const double len = M;
         const double step = std::max(0.3, b * (8.0 * M + 12.0 * len) / 64.0 / 1900.0);
         const double exch = Cc > 1 ? 2.0 + 2.0 * b * len * 16.0 / 1.0e5 : 0.0;
         cands.push_back({Cc, (Np - 1) * step + (2 * Cc - 1) * exch});
@@ -619,9 +619,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                         int rows, cols, ell;
                         shape(j0 + local, rows, cols, ell);
                         const int M = gr.mode != kJacobiRsvd ? std::max(rows, cols) : cols;
-                        const int N = gr.mode != kJacobiRsvd ? std::min(rows, cols) : ell;
-                        const int K = (N + 2 * gr.b - 1) / (2 * gr.b);
-                        sm = std::max(sm, size_t(2) * gr.b * (size_t(M) + size_t(2) * K * gr.b) * elem);
+                        sm = std::max(sm, size_t(2) * gr.b * size_t(M) * elem);
                     }
                     gr.smem = sm;
                     gr.threads = 32 * std::min(kJacobiThreads / 32, std::max(4, gr.b));
@@ -861,6 +859,12 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
         if (fork) CUDA_TRY(cudaStreamWaitEvent(m->stream, m->join_ev, 0));
         {
             Timed t(m, 4);
+            if (w.any_rsvd) {  // B W of the range-finder splits, for the absorb
+                const int tot = w.max_ell * std::min(m->chi, w.max_ell);
+                const int gr = std::max(1, std::min(64, (tot + 255) / 256));
+                rsvd_recover_kernel<<<dim3(gr, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots);
+                count_launch(m, 4);
+            }
             const int per = std::max(w.max_rows, w.max_cols) * std::min(m->chi, std::max(w.max_rows, w.max_cols));
             const int gx = std::max(1, std::min(128, per / 256));
             absorb_kernel<<<dim3(gx, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);

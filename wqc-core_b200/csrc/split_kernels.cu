@@ -481,11 +481,12 @@ __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const 
 // ---------------------------------------------------------------------------
 // One-sided Hestenes Jacobi SVD on a thread-block cluster.
 //
-// The tall working matrix W (M x N, padded to N' = 2*C*b columns) and the
-// rotation accumulator Z (N' x N') are held column by column in the shared
-// memory of the C CTAs of one cluster: CTA r holds block r ("top") and block
-// 2C-1-r ("bottom"), b columns each, one column being W's M entries followed
-// by Z's N' entries.  A sweep orthogonalises the pairs inside each block, then
+// The tall working matrix W (M x N, padded to N' = 2*C*b columns) is held
+// column by column in the shared memory of the C CTAs of one cluster: CTA r
+// holds block r ("top") and block 2C-1-r ("bottom"), b columns each.  The
+// right rotations are not accumulated: at convergence W = X V = U Sigma, and
+// the cut recovers the other side from W and X (absorb_kernel), which keeps
+// the step's shared-memory traffic (its bound) to W's M rows.  A sweep orthogonalises the pairs inside each block, then
 // runs 2C-1 block steps of the b*b cross pairs, rotating the blocks between
 // CTAs by the circle method through distributed shared memory.  Each pair
 // rotation is the reference's rephase-then-real-rotation (svd_guard.rs:
@@ -710,7 +711,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
     const int quantum = 4 * C;
     const int Np = ((N + quantum - 1) / quantum) * quantum;
     const int b = Np / (2 * C);
-    const int len = M + Np;
+    const int len = M;  // W only: the other side's vectors are recovered from W after the SVD
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
@@ -761,7 +762,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
     for (int r = 0; r < C; ++r) fro2 += cluster.map_shared_rank(&ctl, r)->fro_part;
     const double dust = sqrt(fro2) * kDustRel;
     const double dust2 = dust * dust;
-    // Load W (dust-zeroed) and Z = identity.
+    // Load W (dust-zeroed; padding columns zero).
     for (int half = 0; half < 2; ++half) {
         const int id = half == 0 ? rank : 2 * C - 1 - rank;
         T* base = buf(half);
@@ -772,10 +773,6 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
             double2 x = col < N ? src_at(i, col) : cmake(0, 0);
             if (cnorm2(x) < dust2) x = cmake(0, 0);
             base[size_t(c) * len + i] = to_store<T>(x);
-        }
-        for (int e = tid; e < b * Np; e += nthreads) {
-            const int c = e / Np, i = e % Np;
-            base[size_t(c) * len + M + i] = to_store<T>(cmake(i == id * b + c ? 1.0 : 0.0, 0.0));
         }
     }
     __syncthreads();
@@ -897,7 +894,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
         atomicAdd(counters + 0, 1ull);
         atomicAdd(counters + 1, (unsigned long long)(converged ? sweep + 1 : sweep));
     }
-    // Write back: W columns, Z columns (first N rows) and column norms.
+    // Write back: W columns and column norms.
     for (int half = 0; half < 2; ++half) {
         const int id = circle_at(half == 0 ? rank : 2 * C - 1 - rank, xk, 2 * C);
         const T* base = buf(half == 0 ? top_buf_of(rank, xk) : bot_buf_of(rank, xk));
@@ -911,7 +908,6 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
                 s2 = fma(v.x, v.x, fma(v.y, v.y, s2));
                 Bf.w[size_t(col) * M + r] = v;
             }
-            for (int r = lane; r < N; r += 32) Bf.z[size_t(col) * N + r] = to_f64(x[M + r]);
             for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
             if (lane == 0) Bf.sigma[col] = sqrt(s2);
         }
@@ -920,9 +916,9 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
 
 // ---------------------------------------------------------------------------
 // The same Jacobi SVD for working matrices too large for a cluster's shared
-// memory (theta up to 512 x 512 at chi 256: W and Z take 8 MB in FP64, a
-// 16-CTA cluster holds 3.6 MB).  The padded columns (W then Z, `len`
-// entries each) live in the slot's global workspace `gs`, which stays in L2.
+// memory (theta up to 512 x 512 at chi 256: W takes 4 MB in FP64, a 16-CTA
+// cluster holds 3.6 MB with two working blocks per CTA).  The padded W
+// columns live in the slot's global workspace `gs`, which stays in L2.
 // The N' = 2Kb columns form 2K blocks of b; a sweep runs 2K-1 steps of the
 // circle method over the blocks (position 0 fixed, block at position p at
 // step s: circle_at(p, s, 2K)), and at each step CTA r takes the block pairs
@@ -955,7 +951,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const Spl
     const int K = (N + 2 * b - 1) / (2 * b);
     const int nblk = 2 * K;
     const int Np = nblk * b;
-    const int len = M + Np;
+    const int len = M;  // W only, as in jacobi_cluster_kernel
     const size_t blk = size_t(b) * len;
     T* G = reinterpret_cast<T*>(Bf.gs);
     if (G == nullptr) {  // a state sized without the workspace (uniform over the cluster)
@@ -992,17 +988,12 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const Spl
     for (int r = 0; r < C; ++r) fro2 += cluster.map_shared_rank(&ctl, r)->fro_part;
     const double dust = sqrt(fro2) * kDustRel;
     const double dust2 = dust * dust;
-    // W (dust-zeroed, zero padding columns) and Z = identity into the workspace.
+    // W (dust-zeroed, zero padding columns) into the workspace.
     for (int col = rank; col < Np; col += C) {
         T* x = G + size_t(col) * len;
         for (int i = tid; i < len; i += nthreads) {
-            double2 v;
-            if (i < M) {
-                v = col < N ? src_at(i, col) : cmake(0, 0);
-                if (cnorm2(v) < dust2) v = cmake(0, 0);
-            } else {
-                v = cmake(i - M == col ? 1.0 : 0.0, 0.0);
-            }
+            double2 v = col < N ? src_at(i, col) : cmake(0, 0);
+            if (cnorm2(v) < dust2) v = cmake(0, 0);
             x[i] = to_store<T>(v);
         }
     }
@@ -1104,8 +1095,8 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const Spl
         atomicAdd(counters + 0, 1ull);
         atomicAdd(counters + 1, (unsigned long long)(converged ? sweep + 1 : sweep));
     }
-    // Write back W, Z (first N rows) and the column norms; CTA r takes
-    // columns r, r+C, ..., one warp per column.
+    // Write back W and the column norms; CTA r takes columns r, r+C, ...,
+    // one warp per column.
     for (int col = rank + C * wid; col < N; col += C * nwarps) {
         const T* x = G + size_t(col) * len;
         double s2 = 0;
@@ -1114,7 +1105,6 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const Spl
             s2 = fma(v.x, v.x, fma(v.y, v.y, s2));
             Bf.w[size_t(col) * M + r] = v;
         }
-        for (int r = lane; r < N; r += 32) Bf.z[size_t(col) * N + r] = to_f64(__ldcg(x + M + r));
         for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
         if (lane == 0) Bf.sigma[col] = sqrt(s2);
     }
@@ -1205,8 +1195,39 @@ __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const Slot
 }
 
 // ---------------------------------------------------------------------------
+// Range finder: T = B W_k, the kept left vectors of B times sigma^2 (B = U_B
+// Sigma V_B^H with V_B = W / sigma, so U_B = B W / sigma^2), into the slot's
+// z buffer, column pc (length ell) for each kept m (pc = perm[m]).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) rsvd_recover_kernel(const SplitJob* jobs, const SplitState* st,
+                                                           const SlotBuffers* slots) {
+    const int j = blockIdx.y;
+    const SplitState S = st[j];
+    if (S.skip || S.final_kind != 1) return;
+    const SlotBuffers B = slots[jobs[j].slot];
+    const int ell = S.ell, cols = S.cols, chi = S.chi;
+    const long n = long(ell) * chi;
+    for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += long(gridDim.x) * blockDim.x) {
+        const int m = int(e / ell), jj = int(e % ell);
+        const int pc = B.perm[m];
+        const double2* brow = B.b + size_t(jj) * cols;
+        const double2* w = B.w + size_t(pc) * cols;
+        double2 acc = cmake(0, 0);
+        for (int c = 0; c < cols; ++c) cfma(acc, brow[c], w[c]);
+        B.z[size_t(pc) * ell + jj] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // absorb: L = U sqrt(S), R = sqrt(S) V^H written into the two sites, new bond
-// dims published (mps.rs:1156-1168, 1039-1051).
+// dims published (mps.rs:1156-1168, 1039-1051).  The Jacobi gives W = X V =
+// U_X Sigma for X = theta, theta^H or B^H; the other side follows from W and
+// X (for the kept columns, sigma > 0):
+//   theta (rows >= cols):  L = W / sqrt(s),          R = s^-3/2 W^H theta
+//   theta^H (rows < cols): L = theta W s^-3/2,      R = W^H / sqrt(s)
+//   B^H (range finder):    L = Q (B W) s^-3/2,      R = W^H / sqrt(s)
+// so L R = U_k U_k^H theta (or its Q-projected form), accurate to eps
+// ||theta|| whatever the small singular values.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const SplitState* st,
                                                      const SlotBuffers* slots, DeviceMps mps) {
@@ -1215,23 +1236,22 @@ __global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const
     const SplitState S = st[j];
     if (S.skip) return;
     const SlotBuffers B = slots[J.slot];
-    const int chi = S.chi, dl = S.dl, dr = S.dr, rows = S.rows, cols = S.cols;
+    const int chi = S.chi, rows = S.rows, cols = S.cols;
     double2* Ls = mps.site[J.p];
     double2* Rs = mps.site[J.p + 1];
     const long nl = long(rows) * chi, nr = long(chi) * cols;
     const long stride = long(gridDim.x) * blockDim.x;
     const long t0 = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    auto inv_s32 = [](double sg) { return sg > 0.0 ? 1.0 / (sg * sqrt(sg)) : 0.0; };
     if (S.final_kind == 1) {
-        // Range finder: W = B^H (cols x ell), U_B = Z (ell x ell), V_B = W / sigma.
         const int ell = S.ell;
         for (long e = t0; e < nl; e += stride) {
             const int r = int(e / chi), m = int(e % chi);
             const int pc = B.perm[m];
-            const double sg = B.sigma[pc];
             double2 acc = cmake(0, 0);
-            const double2* zc = B.z + size_t(pc) * ell;
-            for (int t = 0; t < ell; ++t) cfma(acc, B.q[size_t(t) * rows + r], zc[t]);
-            Ls[e] = cscale(acc, sqrt(sg));  // L[(r/2)][r%2][m] at r*chi + m
+            const double2* tc = B.z + size_t(pc) * ell;
+            for (int t = 0; t < ell; ++t) cfma(acc, B.q[size_t(t) * rows + r], tc[t]);
+            Ls[e] = cscale(acc, inv_s32(B.sigma[pc]));  // L[(r/2)][r%2][m] at r*chi + m
         }
         for (long e = t0; e < nr; e += stride) {
             const int m = int(e / cols), c = int(e % cols);
@@ -1241,7 +1261,7 @@ __global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const
             Rs[e] = sg > 0.0 ? cscale(cconj(w), 1.0 / sqrt(sg)) : cmake(0, 0);  // R[m][c/dr][c%dr]
         }
     } else if (!S.w_rows_of_src) {
-        // W = theta (rows x cols), U = W / sigma, V = Z (cols x cols).
+        // W = theta V (rows x cols): L = W / sqrt(s), R[m][c] = s^-3/2 sum_r conj(W[r][m]) theta[r][c].
         for (long e = t0; e < nl; e += stride) {
             const int r = int(e / chi), m = int(e % chi);
             const int pc = B.perm[m];
@@ -1252,16 +1272,21 @@ __global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const
         for (long e = t0; e < nr; e += stride) {
             const int m = int(e / cols), c = int(e % cols);
             const int pc = B.perm[m];
-            const double sg = B.sigma[pc];
-            Rs[e] = cscale(cconj(B.z[size_t(pc) * cols + c]), sqrt(sg));
+            const double2* w = B.w + size_t(pc) * rows;
+            double2 acc = cmake(0, 0);
+            for (int r = 0; r < rows; ++r) cfma_conj(acc, w[r], B.theta[size_t(r) * cols + c]);
+            Rs[e] = cscale(acc, inv_s32(B.sigma[pc]));
         }
     } else {
-        // W = theta^H (cols x rows), U = Z (rows x rows), V = W / sigma.
+        // W = theta^H U (cols x rows): L[r][m] = s^-3/2 sum_c theta[r][c] W[c][m], R = W^H / sqrt(s).
         for (long e = t0; e < nl; e += stride) {
             const int r = int(e / chi), m = int(e % chi);
             const int pc = B.perm[m];
-            const double sg = B.sigma[pc];
-            Ls[e] = cscale(B.z[size_t(pc) * rows + r], sqrt(sg));
+            const double2* w = B.w + size_t(pc) * cols;
+            const double2* th = B.theta + size_t(r) * cols;
+            double2 acc = cmake(0, 0);
+            for (int c = 0; c < cols; ++c) cfma(acc, th[c], w[c]);
+            Ls[e] = cscale(acc, inv_s32(B.sigma[pc]));
         }
         for (long e = t0; e < nr; e += stride) {
             const int m = int(e / cols), c = int(e % cols);
@@ -1274,8 +1299,6 @@ __global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         mps.dr[J.p] = chi;
         mps.dl[J.p + 1] = chi;
-        (void)dl;
-        (void)dr;
     }
 }
 

@@ -52,7 +52,7 @@ inline int jacobi_staged_b(int M, int N, size_t elem, size_t smem_limit, size_t*
     size_t best_bytes = 0;
     for (int b = 2; b <= 16; ++b) {
         const int K = (N + 2 * b - 1) / (2 * b);
-        const size_t len = size_t(M) + size_t(2) * K * b;
+        const size_t len = size_t(M);
         const size_t bytes = size_t(2) * b * len * elem;
         if (bytes > smem_limit) continue;
         const long rounds = long(2 * K - 1) * ((K + C - 1) / C) * b;
@@ -66,11 +66,12 @@ inline int jacobi_staged_b(int M, int N, size_t elem, size_t smem_limit, size_t*
     return best;
 }
 // Elements (double2) of the `gs` workspace for two-site matrices up to R x R.
-inline size_t jacobi_staged_elems(int R) { return size_t(R + 32) * size_t(2 * R + 32); }
+inline size_t jacobi_staged_elems(int R) { return size_t(R + 32) * size_t(R); }
 // noise_rel: singular values below noise_rel * (largest) count as zero (0 in
 // the plain form; the precision form's FP32 rounding level).
 __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const SlotBuffers* slots, int mode,
                                 int chi_max, double noise_rel, wqc_split_info* records, int* status);
+__global__ void rsvd_recover_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
 __global__ void absorb_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
                               DeviceMps mps);
 
@@ -94,7 +95,7 @@ inline size_t jacobi_smem_bytes(int M, int N, int C, size_t elem = sizeof(double
     const int Np = ((N + quantum - 1) / quantum) * quantum;
     const int b = Np / (2 * C);
     const int nbuf = C == 1 ? 2 : 3;
-    return size_t(nbuf) * b * (M + Np) * elem;
+    return size_t(nbuf) * b * M * elem;  // W columns only (plus padding columns)
 }
 
 }  // namespace wqc
