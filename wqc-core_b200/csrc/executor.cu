@@ -859,12 +859,21 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
         if (fork) CUDA_TRY(cudaStreamWaitEvent(m->stream, m->join_ev, 0));
         {
             Timed t(m, 4);
-            if (w.any_rsvd) {  // B W of the range-finder splits, for the absorb
-                const int tot = w.max_ell * std::min(m->chi, w.max_ell);
-                const int gr = std::max(1, std::min(64, (tot + 255) / 256));
-                rsvd_recover_kernel<<<dim3(gr, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots);
+            // The side the Jacobi does not accumulate, as tiled GEMMs over the
+            // kept columns (chi <= min(chi_max, rows, cols)).
+            const int kmax = std::min(m->chi, std::min(w.max_rows, w.max_cols));
+            auto tiles = [](int x) { return (x + 31) / 32; };
+            if (w.any_rsvd) {
+                recover_gemm_kernel<<<dim3(tiles(kmax), tiles(w.max_ell), nj), 256, 0, m->stream>>>(
+                    d_jobs, m->d_state, m->d_slots, m->dev, kRecoverBW);
+                recover_gemm_kernel<<<dim3(tiles(kmax), tiles(w.max_rows), nj), 256, 0, m->stream>>>(
+                    d_jobs, m->d_state, m->d_slots, m->dev, kRecoverQT);
+                count_launch(m, 4);
                 count_launch(m, 4);
             }
+            recover_gemm_kernel<<<dim3(tiles(std::max(w.max_cols, kmax)), tiles(std::max(w.max_rows, kmax)), nj), 256,
+                                  0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev, kRecoverExact);
+            count_launch(m, 4);
             const int per = std::max(w.max_rows, w.max_cols) * std::min(m->chi, std::max(w.max_rows, w.max_cols));
             const int gx = std::max(1, std::min(128, per / 256));
             absorb_kernel<<<dim3(gx, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);

@@ -1195,39 +1195,104 @@ __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const Slot
 }
 
 // ---------------------------------------------------------------------------
-// Range finder: T = B W_k, the kept left vectors of B times sigma^2 (B = U_B
-// Sigma V_B^H with V_B = W / sigma, so U_B = B W / sigma^2), into the slot's
-// z buffer, column pc (length ell) for each kept m (pc = perm[m]).
+// Recovery of the side the Jacobi does not accumulate, as tiled batched
+// GEMMs over the kept columns (m < chi, W column pc = perm[m]), with the
+// s^-3/2 scale in the epilogue.  W = X V = U_X Sigma for X = theta, theta^H
+// or B^H, so (kept columns, sigma > 0):
+//   kRecoverBW:   T = B W_k                  (ell x chi, into the slot's z, column pc)
+//   kRecoverQT:   L = Q T s^-3/2             (range finder, rows x chi, into site p)
+//   kRecoverExact: R = s^-3/2 W_k^H theta    (theta, rows >= cols, into site p+1)
+//                  L = theta W_k s^-3/2      (theta^H, rows < cols, into site p)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) rsvd_recover_kernel(const SplitJob* jobs, const SplitState* st,
-                                                           const SlotBuffers* slots) {
-    const int j = blockIdx.y;
+__global__ void __launch_bounds__(256) recover_gemm_kernel(const SplitJob* jobs, const SplitState* st,
+                                                           const SlotBuffers* slots, DeviceMps mps, int stage) {
+    const int j = blockIdx.z;
+    const SplitJob& J = jobs[j];
     const SplitState S = st[j];
-    if (S.skip || S.final_kind != 1) return;
-    const SlotBuffers B = slots[jobs[j].slot];
-    const int ell = S.ell, cols = S.cols, chi = S.chi;
-    const long n = long(ell) * chi;
-    for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += long(gridDim.x) * blockDim.x) {
-        const int m = int(e / ell), jj = int(e % ell);
-        const int pc = B.perm[m];
-        const double2* brow = B.b + size_t(jj) * cols;
-        const double2* w = B.w + size_t(pc) * cols;
-        double2 acc = cmake(0, 0);
-        for (int c = 0; c < cols; ++c) cfma(acc, brow[c], w[c]);
-        B.z[size_t(pc) * ell + jj] = acc;
+    if (S.skip) return;
+    const bool rf = S.final_kind == 1;
+    if ((stage == kRecoverExact) == rf) return;
+    const SlotBuffers B = slots[J.slot];
+    const int rows = S.rows, cols = S.cols, ell = S.ell, chi = S.chi;
+    // C[i][n] = sum_k A(i, k) Bm(k, n); which operand is gathered by perm
+    // depends on the stage.
+    int m, n, k, kind;
+    if (stage == kRecoverBW) {
+        m = ell; n = chi; k = cols; kind = 0;
+    } else if (stage == kRecoverQT) {
+        m = rows; n = chi; k = ell; kind = 1;
+    } else if (!S.w_rows_of_src) {
+        m = chi; n = cols; k = rows; kind = 2;
+    } else {
+        m = rows; n = chi; k = cols; kind = 3;
     }
+    const int i0 = blockIdx.y * kGemmT, n0 = blockIdx.x * kGemmT;
+    if (i0 >= m || n0 >= n) return;
+    auto a_at = [&](int i, int kk) -> double2 {
+        switch (kind) {
+            case 0: return B.b[size_t(i) * cols + kk];                          // B[j][c]
+            case 1: return B.q[size_t(kk) * rows + i];                          // Q[r][t]
+            case 2: return cconj(B.w[size_t(B.perm[i]) * rows + kk]);          // conj W[r][pc(m)]
+            default: return B.theta[size_t(i) * cols + kk];                     // theta[r][c]
+        }
+    };
+    auto b_at = [&](int kk, int nn) -> double2 {
+        switch (kind) {
+            case 0: return B.w[size_t(B.perm[nn]) * cols + kk];                 // W[c][pc(m)]
+            case 1: return B.z[size_t(B.perm[nn]) * ell + kk];                  // T[t][pc(m)]
+            case 2: return B.theta[size_t(kk) * cols + nn];                     // theta[r][c]
+            default: return B.w[size_t(B.perm[nn]) * cols + kk];                // W[c][pc(m)]
+        }
+    };
+    __shared__ double2 As[kGemmT][kGemmK + 1];
+    __shared__ double2 Bs[kGemmK][kGemmT + 1];
+    const int tid = threadIdx.x;
+    const int tr = tid / 16, tc = tid % 16;
+    double2 acc[2][2] = {{cmake(0, 0), cmake(0, 0)}, {cmake(0, 0), cmake(0, 0)}};
+    for (int k0 = 0; k0 < k; k0 += kGemmK) {
+        for (int e = tid; e < kGemmT * kGemmK; e += 256) {
+            const int r = e / kGemmK, c = e % kGemmK;
+            As[r][c] = (i0 + r < m && k0 + c < k) ? a_at(i0 + r, k0 + c) : cmake(0, 0);
+        }
+        for (int e = tid; e < kGemmK * kGemmT; e += 256) {
+            const int r = e / kGemmT, c = e % kGemmT;
+            Bs[r][c] = (k0 + r < k && n0 + c < n) ? b_at(k0 + r, n0 + c) : cmake(0, 0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int c = 0; c < kGemmK; ++c) {
+            const double2 a0 = As[tr][c], a1 = As[tr + 16][c];
+            const double2 b0 = Bs[c][tc], b1 = Bs[c][tc + 16];
+            cfma(acc[0][0], a0, b0);
+            cfma(acc[0][1], a0, b1);
+            cfma(acc[1][0], a1, b0);
+            cfma(acc[1][1], a1, b1);
+        }
+        __syncthreads();
+    }
+    auto inv_s32 = [&](int mm) {
+        const double sg = B.sigma[B.perm[mm]];
+        return sg > 0.0 ? 1.0 / (sg * sqrt(sg)) : 0.0;
+    };
+    for (int x = 0; x < 2; ++x)
+        for (int y = 0; y < 2; ++y) {
+            const int i = i0 + tr + 16 * x, nn = n0 + tc + 16 * y;
+            if (i >= m || nn >= n) continue;
+            const double2 v = acc[x][y];
+            switch (kind) {
+                case 0: B.z[size_t(B.perm[nn]) * ell + i] = v; break;
+                case 1: mps.site[J.p][size_t(i) * chi + nn] = cscale(v, inv_s32(nn)); break;
+                case 2: mps.site[J.p + 1][size_t(i) * cols + nn] = cscale(v, inv_s32(i)); break;
+                default: mps.site[J.p][size_t(i) * chi + nn] = cscale(v, inv_s32(nn)); break;
+            }
+        }
 }
 
 // ---------------------------------------------------------------------------
-// absorb: L = U sqrt(S), R = sqrt(S) V^H written into the two sites, new bond
-// dims published (mps.rs:1156-1168, 1039-1051).  The Jacobi gives W = X V =
-// U_X Sigma for X = theta, theta^H or B^H; the other side follows from W and
-// X (for the kept columns, sigma > 0):
-//   theta (rows >= cols):  L = W / sqrt(s),          R = s^-3/2 W^H theta
-//   theta^H (rows < cols): L = theta W s^-3/2,      R = W^H / sqrt(s)
-//   B^H (range finder):    L = Q (B W) s^-3/2,      R = W^H / sqrt(s)
-// so L R = U_k U_k^H theta (or its Q-projected form), accurate to eps
-// ||theta|| whatever the small singular values.
+// absorb: the sides that are plain copies of W (L = W / sqrt(s) for theta,
+// R = W^H / sqrt(s) for theta^H and B^H), and the new bond dims
+// (mps.rs:1156-1168, 1039-1051).  The other side comes from
+// recover_gemm_kernel.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const SplitState* st,
                                                      const SlotBuffers* slots, DeviceMps mps) {
@@ -1237,63 +1302,27 @@ __global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const
     if (S.skip) return;
     const SlotBuffers B = slots[J.slot];
     const int chi = S.chi, rows = S.rows, cols = S.cols;
-    double2* Ls = mps.site[J.p];
-    double2* Rs = mps.site[J.p + 1];
-    const long nl = long(rows) * chi, nr = long(chi) * cols;
     const long stride = long(gridDim.x) * blockDim.x;
     const long t0 = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    auto inv_s32 = [](double sg) { return sg > 0.0 ? 1.0 / (sg * sqrt(sg)) : 0.0; };
-    if (S.final_kind == 1) {
-        const int ell = S.ell;
-        for (long e = t0; e < nl; e += stride) {
+    if (S.final_kind == 0 && !S.w_rows_of_src) {
+        // L = W / sqrt(s), W rows x cols; R comes from recover_gemm_kernel.
+        double2* Ls = mps.site[J.p];
+        for (long e = t0; e < long(rows) * chi; e += stride) {
             const int r = int(e / chi), m = int(e % chi);
             const int pc = B.perm[m];
-            double2 acc = cmake(0, 0);
-            const double2* tc = B.z + size_t(pc) * ell;
-            for (int t = 0; t < ell; ++t) cfma(acc, B.q[size_t(t) * rows + r], tc[t]);
-            Ls[e] = cscale(acc, inv_s32(B.sigma[pc]));  // L[(r/2)][r%2][m] at r*chi + m
+            const double sg = B.sigma[pc];
+            const double2 w = B.w[size_t(pc) * rows + r];
+            Ls[e] = sg > 0.0 ? cscale(w, 1.0 / sqrt(sg)) : cmake(0, 0);  // L[(r/2)][r%2][m] at r*chi + m
         }
-        for (long e = t0; e < nr; e += stride) {
+    } else {
+        // R = W^H / sqrt(s), W cols x (ell or rows); L comes from recover_gemm_kernel.
+        double2* Rs = mps.site[J.p + 1];
+        for (long e = t0; e < long(chi) * cols; e += stride) {
             const int m = int(e / cols), c = int(e % cols);
             const int pc = B.perm[m];
             const double sg = B.sigma[pc];
             const double2 w = B.w[size_t(pc) * cols + c];
             Rs[e] = sg > 0.0 ? cscale(cconj(w), 1.0 / sqrt(sg)) : cmake(0, 0);  // R[m][c/dr][c%dr]
-        }
-    } else if (!S.w_rows_of_src) {
-        // W = theta V (rows x cols): L = W / sqrt(s), R[m][c] = s^-3/2 sum_r conj(W[r][m]) theta[r][c].
-        for (long e = t0; e < nl; e += stride) {
-            const int r = int(e / chi), m = int(e % chi);
-            const int pc = B.perm[m];
-            const double sg = B.sigma[pc];
-            const double2 w = B.w[size_t(pc) * rows + r];
-            Ls[e] = sg > 0.0 ? cscale(w, 1.0 / sqrt(sg)) : cmake(0, 0);
-        }
-        for (long e = t0; e < nr; e += stride) {
-            const int m = int(e / cols), c = int(e % cols);
-            const int pc = B.perm[m];
-            const double2* w = B.w + size_t(pc) * rows;
-            double2 acc = cmake(0, 0);
-            for (int r = 0; r < rows; ++r) cfma_conj(acc, w[r], B.theta[size_t(r) * cols + c]);
-            Rs[e] = cscale(acc, inv_s32(B.sigma[pc]));
-        }
-    } else {
-        // W = theta^H U (cols x rows): L[r][m] = s^-3/2 sum_c theta[r][c] W[c][m], R = W^H / sqrt(s).
-        for (long e = t0; e < nl; e += stride) {
-            const int r = int(e / chi), m = int(e % chi);
-            const int pc = B.perm[m];
-            const double2* w = B.w + size_t(pc) * cols;
-            const double2* th = B.theta + size_t(r) * cols;
-            double2 acc = cmake(0, 0);
-            for (int c = 0; c < cols; ++c) cfma(acc, th[c], w[c]);
-            Ls[e] = cscale(acc, inv_s32(B.sigma[pc]));
-        }
-        for (long e = t0; e < nr; e += stride) {
-            const int m = int(e / cols), c = int(e % cols);
-            const int pc = B.perm[m];
-            const double sg = B.sigma[pc];
-            const double2 w = B.w[size_t(pc) * cols + c];
-            Rs[e] = sg > 0.0 ? cscale(cconj(w), 1.0 / sqrt(sg)) : cmake(0, 0);
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -71,7 +71,9 @@ inline size_t jacobi_staged_elems(int R) { return size_t(R + 32) * size_t(R); }
 // the plain form; the precision form's FP32 rounding level).
 __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const SlotBuffers* slots, int mode,
                                 int chi_max, double noise_rel, wqc_split_info* records, int* status);
-__global__ void rsvd_recover_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
+enum { kRecoverBW = 0, kRecoverQT = 1, kRecoverExact = 2 };
+__global__ void recover_gemm_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
+                                    DeviceMps mps, int stage);
 __global__ void absorb_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
                               DeviceMps mps);
 
