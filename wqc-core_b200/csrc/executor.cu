@@ -148,6 +148,7 @@ struct Group {
     size_t smem;
     int threads;          // one warp per column pair of a block, at most kJacobiThreads
     bool staged = false;  // jacobi_staged_kernel with blocks of b columns
+    bool reg = false;     // cluster Jacobi variant with register-resident top columns
     int b = 0;
 };
 
@@ -256,7 +257,8 @@ std::once_flag g_attr_once;
 cudaError_t g_attr_err = cudaSuccess;
 
 void set_kernel_attributes() {
-    for (const void* f : {jacobi_kernel(false), jacobi_kernel(true), jacobi_staged(false), jacobi_staged(true)}) {
+    for (const void* f : {jacobi_kernel(false, false), jacobi_kernel(true, false), jacobi_kernel(false, true),
+                          jacobi_kernel(true, true), jacobi_staged(false), jacobi_staged(true)}) {
         if (g_attr_err == cudaSuccess)
             g_attr_err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLimit));
         if (g_attr_err == cudaSuccess)
@@ -289,7 +291,7 @@ int choose_cluster(int M, int N, int max_c, int njobs, int sm_count, size_t elem
     for (int Cc = 1; Cc <= max_c; ++Cc) {
         if (jacobi_smem_bytes(M, N, Cc, elem) > kSmemLimit) continue;
         const int Np = round_up(N, 4 * Cc), b = Np / (2 * Cc);
-        if (b > 16 && Cc < max_c) continue;  // more pairs than warps
+        if (b > jacobi_max_warps(M) && Cc < max_c) continue;  // more pairs than warps
         const double len = M;
         const double step = std::max(0.3, b * (8.0 * M + 12.0 * len) / 64.0 / 1900.0);
         const double exch = Cc > 1 ? 2.0 + 2.0 * b * len * 16.0 / 1.0e5 : 0.0;
@@ -622,7 +624,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                         sm = std::max(sm, size_t(2) * gr.b * size_t(M) * elem);
                     }
                     gr.smem = sm;
-                    gr.threads = 32 * std::min(kJacobiThreads / 32, std::max(4, gr.b));
+                    gr.threads = 32 * std::min(kJacobiStagedThreads / 32, std::max(4, gr.b));
                     for (int local : g.second) plan.idx.push_back(local);
                     w.groups.push_back(gr);
                     continue;
@@ -640,15 +642,18 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                     sm = std::max(sm, sz);
                 }
                 gr.smem = sm;
-                int bmax = 1;
+                int bmax = 1, mmax = 1;
                 for (int local : g.second) {
                     int rows, cols, ell;
                     shape(j0 + local, rows, cols, ell);
                     const int N = gr.mode != kJacobiRsvd ? std::min(rows, cols) : ell;
                     const int Cc = std::max(gr.C, 1);
                     bmax = std::max(bmax, round_up(N, 4 * Cc) / (2 * Cc));
+                    mmax = std::max(mmax, gr.mode != kJacobiRsvd ? std::max(rows, cols) : cols);
                 }
-                gr.threads = 32 * std::min(kJacobiThreads / 32, std::max(2, bmax));
+                // Register-resident variant when every column of the group fits.
+                gr.reg = mmax <= kJacobiRegMaxRows;
+                gr.threads = 32 * std::min(jacobi_max_warps(mmax), std::max(2, bmax));
                 for (int local : g.second) plan.idx.push_back(local);
                 w.groups.push_back(gr);
             }
@@ -778,7 +783,7 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                     CUDA_TRY(launch_jacobi_staged(m->fp32, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off,
                                                   mode, kMaxSweeps, gr.b, m->d_status, m->d_counters));
                 else
-                    CUDA_TRY(launch_jacobi(m->fp32, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off, mode,
+                    CUDA_TRY(launch_jacobi(m->fp32, gr.reg, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off, mode,
                                            kMaxSweeps, m->d_status, m->d_counters));
                 count_launch(m, 0);
             }
@@ -977,7 +982,7 @@ wqc_status wqc_cuda_open(int device, wqc_cuda_ctx** out) {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, jacobi_kernel(false), &cfg) == cudaSuccess && clusters > 0)
+        if (cudaOccupancyMaxActiveClusters(&clusters, jacobi_kernel(false, false), &cfg) == cudaSuccess && clusters > 0)
             ctx->max_cluster = 16;
         cudaGetLastError();
     }

@@ -538,6 +538,40 @@ struct JacobiReal<float2> {
     using R = float;
 };
 
+// Rotation parameters from alpha = |p|^2, beta = |q|^2, gamma = <p, q>:
+// returns false when the pair is left alone (noise-level column, or already
+// orthogonal to tol), else c and w = s * phase.
+__device__ __forceinline__ bool jacobi_params(double a, double bb, double gr, double gi, double tol, double noise_floor,
+                                              double& relmax, double& c, double& wr, double& wi) {
+    // Squared forms keep the dependent chain short: |gamma|^2 against
+    // tol^2 alpha beta, one reciprocal square root for the phase.
+    const double g2 = fma(gr, gr, gi * gi);
+    const double ab = a * bb;
+    if (fmin(a, bb) <= noise_floor) return false;  // the smaller column is at the storage's rounding level
+    relmax = fmax(relmax, g2 / ab);  // squared ratio; the caller compares with squared bounds
+    if (g2 == 0.0 || g2 <= tol * tol * ab) return false;
+    double pr, pi, zeta;
+    if (g2 > 1e-290) {
+        const double inv_g = rsqrt(g2);
+        pr = gr * inv_g;
+        pi = gi * inv_g;
+        zeta = 0.5 * (bb - a) * inv_g;
+    } else {  // |gamma|^2 near the subnormal range: hypot keeps the phase of unit modulus
+        const double g = hypot(gr, gi);
+        pr = gr / g;
+        pi = gi / g;
+        zeta = (bb - a) / (2.0 * g);
+    }
+    const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
+    c = rsqrt(fma(t, t, 1.0));
+    const double s = c * t;
+    // With w = s * phase the rephased rotation (svd_guard.rs:189-197) is
+    // xp' = c xp - conj(w) xq,  xq' = w xp + c xq   (|phase| = 1).
+    wr = s * pr;
+    wi = s * pi;
+    return true;
+}
+
 template <typename T>
 __device__ __forceinline__ int jacobi_rotate(T* __restrict__ xp, T* __restrict__ xq, int M, int len, double tol,
                                              double noise_floor, int lane, double& relmax) {
@@ -576,32 +610,9 @@ __device__ __forceinline__ int jacobi_rotate(T* __restrict__ xp, T* __restrict__
         gr_ += __shfl_xor_sync(0xffffffffu, gr_, o);
         gi_ += __shfl_xor_sync(0xffffffffu, gi_, o);
     }
-    const double a = a_, bb = b_, gr = gr_, gi = gi_;
-    // Squared forms keep the dependent chain short: |gamma|^2 against
-    // tol^2 alpha beta, one reciprocal square root for the phase.
-    const double g2 = fma(gr, gr, gi * gi);
-    const double ab = a * bb;
-    if (fmin(a, bb) <= noise_floor) return 0;  // the smaller column is at the storage's rounding level
-    relmax = fmax(relmax, g2 / ab);  // squared ratio; the caller compares with squared bounds
-    if (g2 == 0.0 || g2 <= tol * tol * ab) return 0;
-    double pr, pi, zeta;
-    if (g2 > 1e-290) {
-        const double inv_g = rsqrt(g2);
-        pr = gr * inv_g;
-        pi = gi * inv_g;
-        zeta = 0.5 * (bb - a) * inv_g;
-    } else {  // |gamma|^2 near the subnormal range: hypot keeps the phase of unit modulus
-        const double g = hypot(gr, gi);
-        pr = gr / g;
-        pi = gi / g;
-        zeta = (bb - a) / (2.0 * g);
-    }
-    const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
-    const double c = rsqrt(fma(t, t, 1.0));
-    const double s = c * t;
-    // With w = s * phase the rephased rotation (svd_guard.rs:189-197) is
-    // xp' = c xp - conj(w) xq,  xq' = w xp + c xq   (|phase| = 1).
-    const R wr = R(s * pr), wi = R(s * pi), cr = R(c);
+    double c64, wr64, wi64;
+    if (!jacobi_params(a_, b_, gr_, gi_, tol, noise_floor, relmax, c64, wr64, wi64)) return 0;
+    const R wr = R(wr64), wi = R(wi64), cr = R(c64);
     auto rot = [&](const T u, const T v, T& p, T& q) {
         p.x = fma(cr, u.x, -fma(wr, v.x, wi * v.y));
         p.y = fma(cr, u.y, -fma(wr, v.y, -wi * v.x));
@@ -630,6 +641,68 @@ __device__ __forceinline__ int jacobi_rotate(T* __restrict__ xp, T* __restrict__
         rot(xp[r], xq[r], p, q);
         xp[r] = p;
         xq[r] = q;
+    }
+    return 1;
+}
+
+// The same rotation with p held in registers (rows lane + 32 k, M <= 32 *
+// kJacobiRegRows): in a block step warp i keeps its top column for all b
+// rounds, so only the partner q moves through shared memory (the step is
+// bound by shared-memory bandwidth).
+constexpr int kJacobiRegRows = 8;
+
+template <typename T>
+__device__ __forceinline__ int jacobi_rotate_reg(T (&u)[kJacobiRegRows], T* __restrict__ xq, int M, double tol,
+                                                 double noise_floor, int lane, double& relmax) {
+    using R = typename JacobiReal<T>::R;
+    T v[kJacobiRegRows];
+#pragma unroll
+    for (int k = 0; k < kJacobiRegRows; ++k) {
+        const int r = lane + 32 * k;
+        if (r < M) {
+            v[k] = xq[r];
+        } else {
+            v[k].x = v[k].y = R(0);
+        }
+    }
+    R a_ = 0, b_ = 0, gr_ = 0, gi_ = 0, a1 = 0, b1 = 0, gr1 = 0, gi1 = 0;
+#pragma unroll
+    for (int k = 0; k < kJacobiRegRows; k += 2) {
+        a_ = fma(u[k].x, u[k].x, fma(u[k].y, u[k].y, a_));
+        b_ = fma(v[k].x, v[k].x, fma(v[k].y, v[k].y, b_));
+        gr_ = fma(u[k].x, v[k].x, fma(u[k].y, v[k].y, gr_));
+        gi_ = fma(u[k].x, v[k].y, fma(-u[k].y, v[k].x, gi_));
+        a1 = fma(u[k + 1].x, u[k + 1].x, fma(u[k + 1].y, u[k + 1].y, a1));
+        b1 = fma(v[k + 1].x, v[k + 1].x, fma(v[k + 1].y, v[k + 1].y, b1));
+        gr1 = fma(u[k + 1].x, v[k + 1].x, fma(u[k + 1].y, v[k + 1].y, gr1));
+        gi1 = fma(u[k + 1].x, v[k + 1].y, fma(-u[k + 1].y, v[k + 1].x, gi1));
+    }
+    a_ += a1;
+    b_ += b1;
+    gr_ += gr1;
+    gi_ += gi1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a_ += __shfl_xor_sync(0xffffffffu, a_, o);
+        b_ += __shfl_xor_sync(0xffffffffu, b_, o);
+        gr_ += __shfl_xor_sync(0xffffffffu, gr_, o);
+        gi_ += __shfl_xor_sync(0xffffffffu, gi_, o);
+    }
+    double c64, wr64, wi64;
+    if (!jacobi_params(a_, b_, gr_, gi_, tol, noise_floor, relmax, c64, wr64, wi64)) return 0;
+    const R wr = R(wr64), wi = R(wi64), cr = R(c64);
+#pragma unroll
+    for (int k = 0; k < kJacobiRegRows; ++k) {
+        const int r = lane + 32 * k;
+        if (r < M) {
+            T p, q;
+            p.x = fma(cr, u[k].x, -fma(wr, v[k].x, wi * v[k].y));
+            p.y = fma(cr, u[k].y, -fma(wr, v[k].y, -wi * v[k].x));
+            q.x = fma(wr, u[k].x, fma(-wi, u[k].y, cr * v[k].x));
+            q.y = fma(wr, u[k].y, fma(wi, u[k].x, cr * v[k].y));
+            u[k] = p;
+            xq[r] = q;
+        }
     }
     return 1;
 }
@@ -689,8 +762,9 @@ __device__ __forceinline__ float2 to_store<float2>(double2 x) {
 __device__ __forceinline__ double2 to_f64(double2 x) { return x; }
 __device__ __forceinline__ double2 to_f64(float2 x) { return make_double2(x.x, x.y); }
 
-template <typename T>
-__global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const SplitJob* jobs, const SplitState* st,
+template <typename T, bool kReg>
+__global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jacobi_cluster_kernel(
+    const SplitJob* jobs, const SplitState* st,
                                                                           const SlotBuffers* slots, const int* idx,
                                                                           int mode, int max_sweeps, int* status,
                                                                           unsigned long long* counters) {
@@ -809,16 +883,51 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
             }
             __syncthreads();
         }
-        // Cross pairs between the two blocks, 2C-1 block steps.
+        // Cross pairs between the two blocks, 2C-1 block steps.  Warp i pairs
+        // its top column i with bottom column (i + k) % b in round k; when
+        // every warp owns one top column and it fits, the column stays in
+        // registers for the b rounds.
+        const bool reg_path = kReg && M <= 32 * kJacobiRegRows && nwarps >= b;
         for (int bs = 0; bs < 2 * C - 1; ++bs) {
-            for (int k = 0; k < b; ++k) {
-                T* tb = buf(top_buf_of(rank, xk));
-                T* bb = buf(bot_buf_of(rank, xk));
-                for (int i = wid; i < b; i += nwarps) {
-                    const int e2 = (i + k) % b;
-                    my_rot += jacobi_rotate(tb + size_t(i) * len, bb + size_t(e2) * len, M, len, tol, noise_floor, lane, my_rel);
+            T* tb = buf(top_buf_of(rank, xk));
+            T* bb = buf(bot_buf_of(rank, xk));
+            if (reg_path) {
+                T u[kJacobiRegRows];
+                T* col = tb + size_t(wid) * len;
+                if (wid < b) {
+#pragma unroll
+                    for (int kk = 0; kk < kJacobiRegRows; ++kk) {
+                        const int r = lane + 32 * kk;
+                        if (r < M) {
+                            u[kk] = col[r];
+                        } else {
+                            u[kk].x = u[kk].y = 0;
+                        }
+                    }
+                }
+                for (int k = 0; k < b; ++k) {
+                    if (wid < b)
+                        my_rot += jacobi_rotate_reg(u, bb + size_t((wid + k) % b) * len, M, tol, noise_floor, lane,
+                                                    my_rel);
+                    __syncthreads();
+                }
+                if (wid < b) {
+#pragma unroll
+                    for (int kk = 0; kk < kJacobiRegRows; ++kk) {
+                        const int r = lane + 32 * kk;
+                        if (r < M) col[r] = u[kk];
+                    }
                 }
                 __syncthreads();
+            } else {
+                for (int k = 0; k < b; ++k) {
+                    for (int i = wid; i < b; i += nwarps) {
+                        const int e2 = (i + k) % b;
+                        my_rot += jacobi_rotate(tb + size_t(i) * len, bb + size_t(e2) * len, M, len, tol, noise_floor,
+                                                lane, my_rel);
+                    }
+                    __syncthreads();
+                }
             }
             if (C == 1) continue;
             // Circle rotation of blocks between CTAs (push protocol, one spare
@@ -930,7 +1039,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_cluster_kernel(const Sp
 // outputs are those of jacobi_cluster_kernel.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const SplitJob* jobs, const SplitState* st,
+__global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(const SplitJob* jobs, const SplitState* st,
                                                                          const SlotBuffers* slots, const int* idx,
                                                                          int mode, int max_sweeps, int b, int* status,
                                                                          unsigned long long* counters) {
@@ -963,7 +1072,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_staged_kernel(const Spl
     T* sA = reinterpret_cast<T*>(smem_raw);
     T* sB = sA + blk;
     __shared__ JacobiCtl ctl;
-    __shared__ double red[kJacobiThreads / 32];
+    __shared__ double red[kJacobiStagedThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int nthreads = blockDim.x;
     const int nwarps = nthreads / 32;
@@ -1334,9 +1443,12 @@ __global__ void __launch_bounds__(256) absorb_kernel(const SplitJob* jobs, const
 }  // namespace wqc
 
 namespace wqc {
-const void* jacobi_kernel(bool fp32) {
-    return fp32 ? reinterpret_cast<const void*>(jacobi_cluster_kernel<float2>)
-                : reinterpret_cast<const void*>(jacobi_cluster_kernel<double2>);
+const void* jacobi_kernel(bool fp32, bool reg) {
+    if (reg)
+        return fp32 ? reinterpret_cast<const void*>(jacobi_cluster_kernel<float2, true>)
+                    : reinterpret_cast<const void*>(jacobi_cluster_kernel<double2, true>);
+    return fp32 ? reinterpret_cast<const void*>(jacobi_cluster_kernel<float2, false>)
+                : reinterpret_cast<const void*>(jacobi_cluster_kernel<double2, false>);
 }
 
 const void* qr_cluster(bool global_cols) {
@@ -1365,13 +1477,19 @@ cudaError_t launch_jacobi_staged(bool fp32, const cudaLaunchConfig_t& cfg, const
                               counters);
 }
 
-cudaError_t launch_jacobi(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, const SplitState* st,
-                          const SlotBuffers* slots, const int* idx, int mode, int max_sweeps, int* status,
-                          unsigned long long* counters) {
+cudaError_t launch_jacobi(bool fp32, bool reg, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
+                          const SplitState* st, const SlotBuffers* slots, const int* idx, int mode, int max_sweeps,
+                          int* status, unsigned long long* counters) {
+    if (fp32 && reg)
+        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<float2, true>, jobs, st, slots, idx, mode, max_sweeps,
+                                  status, counters);
     if (fp32)
-        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<float2>, jobs, st, slots, idx, mode, max_sweeps, status,
-                                  counters);
-    return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<double2>, jobs, st, slots, idx, mode, max_sweeps, status,
-                              counters);
+        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<float2, false>, jobs, st, slots, idx, mode, max_sweeps,
+                                  status, counters);
+    if (reg)
+        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<double2, true>, jobs, st, slots, idx, mode, max_sweeps,
+                                  status, counters);
+    return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<double2, false>, jobs, st, slots, idx, mode, max_sweeps,
+                              status, counters);
 }
 }  // namespace wqc

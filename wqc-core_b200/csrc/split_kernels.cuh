@@ -9,7 +9,16 @@ enum { kStageY0 = 0, kStageZ = 1, kStageY = 2, kStageB = 3 };
 // Jacobi / finalize modes: the range finder's B^H; theta of a split that takes
 // the exact path from the start; theta of a range-finder split that fell back.
 enum { kJacobiRsvd = 0, kJacobiExact = 1, kJacobiFallback = 2 };
-constexpr int kJacobiThreads = 512;  // 16 warps: one column pair per warp per step (blocks of <= 16 pairs)
+// Threads of the cluster Jacobi: one warp per column pair of a block per step.
+// The variant for columns of at most kJacobiRegMaxRows rows keeps each
+// warp's top column in registers through a block step and is limited to 12
+// warps (170 registers per thread); the other variant, like the staged
+// Jacobi, takes up to 16 warps.
+constexpr int kJacobiThreads = 512;
+constexpr int kJacobiRegThreads = 384;
+constexpr int kJacobiRegMaxRows = 256;
+constexpr int kJacobiStagedThreads = 512;
+inline int jacobi_max_warps(int M) { return (M <= kJacobiRegMaxRows ? kJacobiRegThreads : kJacobiThreads) / 32; }
 
 __global__ void prepare_kernel(const SplitJob* jobs, SplitState* st, int njobs, DeviceMps mps);
 __global__ void merge_gate_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots,
@@ -31,10 +40,10 @@ inline size_t qr_cluster_smem_bytes(int m, int n, int C, bool global_cols = fals
 // The cluster Jacobi SVD kernel (a template over the column type: complex128
 // in the plain form, complex64 in the precision form), reached from other
 // files through these host functions.
-const void* jacobi_kernel(bool fp32);
-cudaError_t launch_jacobi(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, const SplitState* st,
-                          const SlotBuffers* slots, const int* idx, int mode, int max_sweeps, int* status,
-                          unsigned long long* counters);
+const void* jacobi_kernel(bool fp32, bool reg);
+cudaError_t launch_jacobi(bool fp32, bool reg, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
+                          const SplitState* st, const SlotBuffers* slots, const int* idx, int mode, int max_sweeps,
+                          int* status, unsigned long long* counters);
 // The staged variant for working matrices beyond a cluster's shared memory:
 // columns in the slot's `gs` workspace, blocks of b columns (b even).
 const void* jacobi_staged(bool fp32);
