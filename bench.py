@@ -44,7 +44,7 @@ def workload(name: str, depth: int = 0):
     elif name == "config4":
         w = C.config4(depth or 100)
     else:
-        w = C.config1()
+        w = C.config1(depth=depth or 40)
     return w
 
 
@@ -683,7 +683,8 @@ def main():
     ap.add_argument("--workload", choices=("config1", "config0", "config4"), default="config1",
                     help="config1: 50 qubits, depth 40, chi 128 (the headline); config0: 16 qubits, chi 32; "
                          "config4: 100 qubits, chi 256 (--depth layers, default 100)")
-    ap.add_argument("--depth", type=int, default=0, help="layers of the config4 circuit (0: 100)")
+    ap.add_argument("--depth", type=int, default=0,
+                    help="layers of the config1 / config4 circuit (0: their full 40 / 100; a prefix for profiling)")
     ap.add_argument("--split-rule", choices=("reference", "exact"), default="reference")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--reference-budget", type=float, default=10.0)
