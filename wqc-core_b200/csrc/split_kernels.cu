@@ -562,9 +562,16 @@ __device__ __forceinline__ bool jacobi_params(double a, double bb, double gr, do
         pi = gi / g;
         zeta = (bb - a) / (2.0 * g);
     }
-    const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
-    c = rsqrt(fma(t, t, 1.0));
-    const double s = c * t;
+    // tan = sign(zeta) / (|zeta| + u) with u = sqrt(1 + zeta^2) gives
+    // c^2 = (u + |zeta|) / (2u) and s^2 = 1 / (2u (u + |zeta|)): after one
+    // reciprocal square root, c and s are two independent ones, no division.
+    const double az = fabs(zeta);
+    const double q = fma(zeta, zeta, 1.0);
+    const double ru = rsqrt(q);
+    const double u = q * ru;
+    const double c2 = fma(0.5 * az, ru, 0.5);
+    c = c2 * rsqrt(c2);
+    const double s = copysign(rsqrt(2.0 * u * (u + az)), zeta);
     // With w = s * phase the rephased rotation (svd_guard.rs:189-197) is
     // xp' = c xp - conj(w) xq,  xq' = w xp + c xq   (|phase| = 1).
     wr = s * pr;
