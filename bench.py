@@ -626,9 +626,10 @@ def run_cuda(args) -> None:
                 "peak": peak,
                 "unit": "TFLOP/s",
                 "frac": (achieved / peak) if (achieved and peak) else None,
-                "traffic": 334848,
+                "traffic": 767232,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one saturated launch "
-                                  "(profiles/jacobi_svd_random50_d40_chi128.md); W and Z stay in shared memory",
+                                  "(five exact 256 x 256 splits on 16-CTA clusters; "
+                                  "profiles/jacobi_svd_random50_d40_chi128.md); W stays in shared memory",
                 "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
                 "flops_per_step": flops / args.steps,
                 "kernel_ms_per_step": jac_ms / args.steps,

@@ -814,15 +814,18 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                 rsvd_gemm_kernel<<<dim3(te, tc, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageZ);
                 rsvd_gemm_kernel<<<dim3(te, tr, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, kStageY);
                 // Columns in shared memory on the smallest cluster that holds
-                // them; else in global memory on the largest cluster.
+                // them; else in global memory on the largest cluster; Y taller
+                // than the cluster kernel's reflector registers hold: one CTA.
                 int cq = 0;
                 bool qglobal = false;
-                for (int c = 8; c <= m->ctx->max_cluster; c *= 2)
+                const bool qfits = w.max_rows <= kQrRowsPerThread * kQrClusterThreads;
+                for (int c = 8; qfits && c <= m->ctx->max_cluster; c *= 2)
                     if (qr_cluster_smem_bytes(w.max_rows, w.max_ell, c) <= kSmemLimit) {
                         cq = c;
                         break;
                     }
-                if (!cq && qr_cluster_smem_bytes(w.max_rows, w.max_ell, m->ctx->max_cluster, true) <= kSmemLimit) {
+                if (qfits && !cq &&
+                    qr_cluster_smem_bytes(w.max_rows, w.max_ell, m->ctx->max_cluster, true) <= kSmemLimit) {
                     cq = m->ctx->max_cluster;
                     qglobal = true;
                 }

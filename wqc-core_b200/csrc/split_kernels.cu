@@ -371,6 +371,15 @@ __device__ __forceinline__ void reflect_columns(double2* cols, int ldc, int coun
     }
 }
 
+// Split cluster barrier: arrive (releasing this thread's writes) and wait
+// (acquiring the others') as two steps, so a CTA can work between them.
+__device__ __forceinline__ void cluster_arrive_release() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait_acquire() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
 template <bool kGlobalCols>
 __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const SplitJob* jobs, const SplitState* st,
                                                                            const SlotBuffers* slots) {
@@ -430,17 +439,26 @@ __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const 
                 s_tau[slot] = t;
             }
             __syncthreads();
+            // v_c and tau_c are published: release them to the cluster, then
+            // update this CTA's trailing columns while the others copy v_c.
+            cluster_arrive_release();
             if (!trivial)
                 reflect_columns(Ys + size_t(c - c0 + 1) * m, m, c1 - c - 1, bv, cconj(t), c, m, lane, wid, nw);
-        }
-        cluster.sync();
-        if (rank > owner && nloc > 0) {
-            const double2* rv = cluster.map_shared_rank(bcast, owner) + size_t(slot) * m;
-            for (int i = c + tid; i < m; i += kQrClusterThreads) vloc[i] = rv[i];
-            const double2 t = *cluster.map_shared_rank(&s_tau[slot], owner);
+            // The wait below orders nothing written after the arrive: the
+            // next column's norm must not start before every warp's update.
             __syncthreads();
-            if (t.x != 0.0 || t.y != 0.0) reflect_columns(Ys, m, nloc, vloc, cconj(t), c, m, lane, wid, nw);
-            __syncthreads();
+            cluster_wait_acquire();
+        } else {
+            cluster_arrive_release();
+            cluster_wait_acquire();
+            if (rank > owner && nloc > 0) {
+                const double2* rv = cluster.map_shared_rank(bcast, owner) + size_t(slot) * m;
+                for (int i = c + tid; i < m; i += kQrClusterThreads) vloc[i] = rv[i];
+                const double2 t = *cluster.map_shared_rank(&s_tau[slot], owner);
+                __syncthreads();
+                if (t.x != 0.0 || t.y != 0.0) reflect_columns(Ys, m, nloc, vloc, cconj(t), c, m, lane, wid, nw);
+                __syncthreads();
+            }
         }
     }
     if (kGlobalCols) __threadfence();
@@ -449,26 +467,50 @@ __global__ void __launch_bounds__(kQrClusterThreads, 1) qr_cluster_kernel(const 
         const int r = e % m, cc = c0 + e / m;
         Qs[e] = cmake(r == cc ? 1.0 : 0.0, 0.0);
     }
-    __syncthreads();
-    for (int c = nloc > 0 ? c1 - 1 : -1; c >= 0; --c) {
+    // Backward accumulation, Q = H_0 ... H_{n-1} E.  Reflector c-1 is read
+    // from its owner into registers before reflector c is applied, and
+    // stored into the other half of a double buffer (vloc / bcast) after,
+    // so the distributed-shared-memory latency overlaps the update.
+    double2 pv[kQrRowsPerThread];
+    double2 ptau = cmake(0, 0);
+    auto pull = [&](int c) {
         const int owner = c / cpc;
-        if (kGlobalCols) {
-            const double2* rcol = B.y + size_t(c) * m;
-            for (int i = c + 1 + tid; i < m; i += kQrClusterThreads) vloc[i] = __ldcg(rcol + i);
-        } else {
-            const double2* rcol = cluster.map_shared_rank(Ys, owner) + size_t(c - owner * cpc) * m;
-            for (int i = c + 1 + tid; i < m; i += kQrClusterThreads) vloc[i] = rcol[i];
+        const double2* rcol = kGlobalCols ? B.y + size_t(c) * m
+                                          : cluster.map_shared_rank(Ys, owner) + size_t(c - owner * cpc) * m;
+#pragma unroll
+        for (int k = 0; k < kQrRowsPerThread; ++k) {
+            const int i = c + 1 + tid + k * kQrClusterThreads;
+            if (i < m) pv[k] = kGlobalCols ? __ldcg(rcol + i) : rcol[i];
+        }
+        if (tid == 0) ptau = *(cluster.map_shared_rank(taus, owner) + (c - owner * cpc));
+    };
+    auto place = [&](int c, double2* dst, int sl) {
+#pragma unroll
+        for (int k = 0; k < kQrRowsPerThread; ++k) {
+            const int i = c + 1 + tid + k * kQrClusterThreads;
+            if (i < m) dst[i] = pv[k];
         }
         if (tid == 0) {
-            vloc[c] = cmake(1.0, 0.0);
-            s_tau[0] = *(cluster.map_shared_rank(taus, owner) + (c - owner * cpc));
+            dst[c] = cmake(1.0, 0.0);
+            s_tau[sl] = ptau;
         }
-        __syncthreads();
-        const double2 t = s_tau[0];
+    };
+    int cur = 0;
+    if (nloc > 0) {
+        pull(c1 - 1);
+        place(c1 - 1, vloc, 0);
+    }
+    __syncthreads();
+    for (int c = nloc > 0 ? c1 - 1 : -1; c >= 0; --c) {
+        if (c > 0) pull(c - 1);
+        const double2 t = s_tau[cur];
         const int first = max(c, c0);
         if ((t.x != 0.0 || t.y != 0.0) && first < c1)
-            reflect_columns(Qs + size_t(first - c0) * m, m, c1 - first, vloc, t, c, m, lane, wid, nw);
+            reflect_columns(Qs + size_t(first - c0) * m, m, c1 - first, cur ? bcast : vloc, t, c, m, lane, wid,
+                            nw);
+        if (c > 0) place(c - 1, cur ? vloc : bcast, cur ^ 1);
         __syncthreads();
+        cur ^= 1;
     }
     if (!kGlobalCols) {
         for (int e = tid; e < nloc * m; e += kQrClusterThreads) B.q[size_t(c0) * m + e] = Qs[e];

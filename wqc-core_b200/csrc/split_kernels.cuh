@@ -27,6 +27,7 @@ __global__ void omega_kernel(const SplitJob* jobs, const SplitState* st, const S
 __global__ void rsvd_gemm_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots, int stage);
 __global__ void householder_qr_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots);
 constexpr int kQrClusterThreads = 256;
+constexpr int kQrRowsPerThread = 8;  // rows of one reflector each thread holds: Y of at most 2048 rows
 // The cluster Householder QR (columns in shared memory, or with global_cols
 // in the slot's Y and Q buffers), reached through these host functions.
 const void* qr_cluster(bool global_cols);
