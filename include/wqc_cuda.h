@@ -93,8 +93,12 @@ WQC_API void wqc_mps_destroy(wqc_mps* mps);
  * sites are concatenated, so every wave of splits mixes ready splits from all
  * slices; each slice still sees exactly its own MpsState sequence.
  * max_concurrent_splits bounds the split workspace (0: one slot per two
- * sites).  No reference counterpart: the reference runs one slice per
- * request (src/api.rs:336-697); this is how one B200 takes many at once. */
+ * sites).  SVD launch shapes are sized for throughput and depend on each
+ * split's shape only, so a slice gives bit for bit the same results in any
+ * batch (a batch of one included); against a single-state run of the same
+ * circuit they agree to rounding.  No reference counterpart: the reference
+ * runs one slice per request (src/api.rs:336-697); this is how one B200
+ * takes many at once. */
 WQC_API wqc_status wqc_batch_create(wqc_cuda_ctx* ctx, uint32_t count, const uint32_t* qubit_counts,
                                     const uint32_t* max_bond_dims, int32_t precision, uint32_t max_concurrent_splits,
                                     wqc_mps** out);

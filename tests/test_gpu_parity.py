@@ -414,14 +414,19 @@ def test_time_split_rejects_truncation(cuda_ctx):
 
 def test_batch_of_uneven_slices_matches_single_runs_and_oracle(cuda_ctx):
     """The batching form: slices of different width, depth and chi_max in one
-    state.  Every slice must give bit for bit what the single-state path gives
-    for it (the same kernels on the same data), and match its own oracle run:
-    amplitude within AMP_RTOL, split shapes, paths and kept chi bit-exact over
-    the whole run, discarded weights within the per-split tolerance over the
+    state.  Every slice must give bit for bit what a batch holding only that
+    slice gives (batch invariance: SVD launch shapes depend on each split's
+    shape, not on the other slices), agree with the single-state path (whose
+    SVD clusters are sized for latency, so the rotation order and the last
+    bits differ) in split shapes, paths and kept chi exactly and in the
+    amplitude within AMP_RTOL, and match its own oracle run: amplitude
+    within AMP_RTOL, split shapes, paths and kept chi bit-exact over the
+    whole run, discarded weights within the per-split tolerance over the
     first 500 splits.  The deepest slices (about 1000 truncating splits at
     chi 32) drift from the oracle beyond that, exponentially, to a few 1e-9
-    relative in their last weights; the single-state path drifts identically,
-    so that is rounding amplified by repeated truncation, not batching."""
+    relative in their last weights; the single-state path drifts the same
+    way, so that is rounding amplified by repeated truncation, not
+    batching."""
     slices = C.config2_slices(12, seed=99)
     for s in slices:  # keep the oracle side short
         s.chi = min(s.chi, 32)
@@ -433,11 +438,16 @@ def test_batch_of_uneven_slices_matches_single_runs_and_oracle(cuda_ctx):
     times = b.slice_times_ms()
     assert np.all(times > 0)
     for i, s in enumerate(slices):
+        one = W.CudaBatch([s.n], [s.chi], ctx=cuda_ctx)
+        one.apply_slices([s.gates])
+        assert np.array_equal(recs[i], one.slice_records()[0]), i
+        assert amps[i] == one.amplitudes()[0], i
         m = W.CudaMps(s.n, s.chi, ctx=cuda_ctx)
         m.apply_gates(s.gates)
         single = m.split_records()
-        assert np.array_equal(recs[i], single), i
-        assert amps[i] == m.amplitude_zero(), i
+        for k in ("left_site", "rows", "cols", "ell", "path", "chi"):
+            assert np.array_equal(recs[i][k], single[k]), (i, k)
+        assert amp_err(amps[i], m.amplitude_zero(), s.n) < AMP_RTOL, (i, amps[i], m.amplitude_zero())
         o = O.run(s.n, s.chi, s.gates)
         ref = o.records()
         assert amp_err(amps[i], o.amplitude_zero(), s.n) < AMP_RTOL, (i, amps[i], o.amplitude_zero())

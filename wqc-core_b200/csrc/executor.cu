@@ -180,6 +180,7 @@ struct wqc_mps {
     bool reject = false;
     bool exact_only = false;  // WQC_SPLIT_RULE_EXACT
     bool fp32 = false;        // WQC_PRECISION_FP32: complex64 Jacobi columns
+    bool batch = false;       // made by wqc_batch_create: Jacobi clusters sized for throughput
     cudaStream_t stream = nullptr;
     // Second stream of a wave: the exact-path SVDs run there while the range
     // finder runs on `stream`; fork after the merge, join before the absorb.
@@ -285,27 +286,46 @@ int round_up(int x, int q) { return ((x + q - 1) / q) * q; }
 // for one pair's latency, a fixed cost per exchange plus its DSMEM traffic)
 // picks the fastest sweep when the wave's splits cannot fill the GPU, and the
 // least SM-time per split when they can.
-int choose_cluster(int M, int N, int max_c, int njobs, int sm_count, size_t elem) {
-    struct Cand { int C; double sweep_us; };
-    std::vector<Cand> cands;
+// Cluster size of a Jacobi group, from clock64 measurements of the kernel.
+// A single state is latency-bound (a few splits per level): a round costs
+// its shared-memory traffic at 64 B/clk (at least ~0.3 us) and a block
+// exchange ~2 us plus its DSMEM stores; blocks wider than the register
+// variant's 12 warps are not considered for columns it can hold, and once
+// the wave's clusters would fill the GPU the cost counts SM time.  A batch
+// is throughput-bound (its waves fill the GPU), so SM time (sweep time x C)
+// decides for every wave, with the round cost of the variant that runs it:
+// the dependent rotation chain (~1900 cycles with the top column in
+// registers, ~1300 without) or 3 or 6 passes of the partner columns at
+// 128 B/clk, whichever is larger, and ~4600 cycles per exchange.  That
+// choice depends on the shape alone, so a slice's results do not depend on
+// the other slices of its batch.
+bool jacobi_reg_variant(int M, int b) { return M <= kJacobiRegMaxRows && b <= kJacobiRegThreads / 32; }
+
+int choose_cluster(int M, int N, int max_c, int njobs, int sm_count, size_t elem, bool throughput) {
+    int best = -1;
+    double best_cost = 1e300;
     for (int Cc = 1; Cc <= max_c; ++Cc) {
         if (jacobi_smem_bytes(M, N, Cc, elem) > kSmemLimit) continue;
         const int Np = round_up(N, 4 * Cc), b = Np / (2 * Cc);
-        if (b > jacobi_max_warps(M) && Cc < max_c) continue;  // more pairs than warps
-        const double len = M;
-        const double step = std::max(0.3, b * (8.0 * M + 12.0 * len) / 64.0 / 1900.0);
-        const double exch = Cc > 1 ? 2.0 + 2.0 * b * len * 16.0 / 1.0e5 : 0.0;
-        cands.push_back({Cc, (Np - 1) * step + (2 * Cc - 1) * exch});
-    }
-    if (cands.empty()) return -1;
-    int best = cands[0].C;
-    double best_cost = 1e300;
-    for (const Cand& c : cands) {
-        const bool fills = double(njobs) * c.C >= 1.5 * sm_count;
-        const double cost = fills ? c.sweep_us * c.C : c.sweep_us;
+        const int max_b = throughput ? kJacobiThreads / 32 : jacobi_max_warps(M);
+        if (b > max_b && Cc < max_c) continue;  // more pairs than warps
+        double cost;
+        if (throughput) {
+            const bool reg = jacobi_reg_variant(M, b);
+            const double traffic = (reg ? 3.0 : 6.0) * double(elem) * b * M / 128.0;
+            const double round = std::max(reg ? 1900.0 : 1300.0, traffic);
+            const double cycles = Np * round + (Cc > 1 ? (2 * Cc - 1) * 4600.0 : 0.0);
+            cost = cycles / 1900.0 * Cc;  // SM-microseconds at ~1.9 GHz
+        } else {
+            const double len = M;
+            const double step = std::max(0.3, b * (8.0 * M + 12.0 * len) / 64.0 / 1900.0);
+            const double exch = Cc > 1 ? 2.0 + 2.0 * b * len * 16.0 / 1.0e5 : 0.0;
+            cost = (Np - 1) * step + (2 * Cc - 1) * exch;
+            if (double(njobs) * Cc >= 1.5 * sm_count) cost *= Cc;
+        }
         if (cost < best_cost) {
             best_cost = cost;
-            best = c.C;
+            best = Cc;
         }
     }
     return best;
@@ -594,7 +614,8 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 // A shape beyond every cluster's shared memory goes to the
                 // staged kernel: group key -b (0: no kernel takes it).
                 auto cluster_or_staged = [&](int M, int N) {
-                    const int c = choose_cluster(M, N, m->ctx->max_cluster, nj_wave, m->ctx->sm_count, elem);
+                    const int c =
+                        choose_cluster(M, N, m->ctx->max_cluster, nj_wave, m->ctx->sm_count, elem, m->batch);
                     return c >= 1 ? c : -jacobi_staged_b(M, N, elem, kSmemLimit, nullptr);
                 };
                 const int c_exact = cluster_or_staged(std::max(rows, cols), std::min(rows, cols));
@@ -651,9 +672,9 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                     bmax = std::max(bmax, round_up(N, 4 * Cc) / (2 * Cc));
                     mmax = std::max(mmax, gr.mode != kJacobiRsvd ? std::max(rows, cols) : cols);
                 }
-                // Register-resident variant when every column of the group fits.
-                gr.reg = mmax <= kJacobiRegMaxRows;
-                gr.threads = 32 * std::min(jacobi_max_warps(mmax), std::max(2, bmax));
+                // Register-resident variant when every job of the group fits it.
+                gr.reg = jacobi_reg_variant(mmax, bmax);
+                gr.threads = 32 * std::min((gr.reg ? kJacobiRegThreads : kJacobiThreads) / 32, std::max(2, bmax));
                 for (int local : g.second) plan.idx.push_back(local);
                 w.groups.push_back(gr);
             }
@@ -1066,8 +1087,8 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     // theta, w, z + range finder + tau (+ the staged Jacobi's workspace when a
     // two-site matrix can exceed a cluster's shared memory)
     const size_t el = precision == WQC_PRECISION_FP32 ? sizeof(float2) : sizeof(double2);
-    const bool staged = choose_cluster(R, R, ctx->max_cluster, 1, ctx->sm_count, el) < 1 ||
-                        choose_cluster(R, E, ctx->max_cluster, 1, ctx->sm_count, el) < 1;
+    const bool staged = choose_cluster(R, R, ctx->max_cluster, 1, ctx->sm_count, el, false) < 1 ||
+                        choose_cluster(R, E, ctx->max_cluster, 1, ctx->sm_count, el, false) < 1;
     const size_t gs_c = staged ? jacobi_staged_elems(R) : 0;
     const size_t slot_c = size_t(R) * R * 3 + size_t(R) * E * 6 + E + gs_c;
     const size_t slot_bytes = ((slot_c * sizeof(double2) + size_t(R) * (sizeof(double) + sizeof(int)) + 4095) / 4096) * 4096;
@@ -1167,7 +1188,9 @@ wqc_status wqc_batch_create(wqc_cuda_ctx* ctx, uint32_t count, const uint32_t* q
         ns[i] = int(qubit_counts[i]);
         chis[i] = int(max_bond_dims[i]);
     }
-    return create_state(ctx, ns, chis, precision, false, int(max_concurrent_splits), out);
+    const wqc_status st = create_state(ctx, ns, chis, precision, false, int(max_concurrent_splits), out);
+    if (st == WQC_OK) (*out)->batch = true;
+    return st;
 }
 
 wqc_status wqc_mps_reset(wqc_mps* m) {
