@@ -194,6 +194,18 @@ WQC_API wqc_status wqc_mps_bond_dims(wqc_mps* mps, uint32_t* out);
 WQC_API wqc_status wqc_mps_download_site(wqc_mps* mps, uint32_t site, uint32_t* l, uint32_t* r, double* buf);
 WQC_API wqc_status wqc_mps_upload_site(wqc_mps* mps, uint32_t site, uint32_t l, uint32_t r, const double* buf);
 
+/* `shots` draws from |<b|psi>|^2 / <psi|psi>, computed on the device from
+ * the MPS (site-by-site conditional sampling against right environments), so
+ * not limited to 20 qubits as the reference's dense route is
+ * (sample_terminal_measurements, src/sample.rs:192-211, which builds the
+ * outcome table of compute_outcome_probabilities, src/sample.rs:85-131).
+ * out[k] bit j is the outcome of qubits[j] in shot k (count <= 64 distinct
+ * qubits); the host forms the reference's Qiskit-order keys from them.  The
+ * draws come from SplitMix64 keyed by (seed, shot, qubit): deterministic for
+ * a seed, but not the reference's StdRng stream.  Single states only. */
+WQC_API wqc_status wqc_mps_sample(wqc_mps* mps, const uint32_t* qubits, uint32_t count, uint32_t shots, uint64_t seed,
+                                  uint64_t* out);
+
 /* Sum_t coeff_t <psi|P_t|psi> for Pauli strings (labels: nterms strings of
  * qubit_count characters in IXYZ, character n-1-q acting on qubit q as in
  * src/expectation.rs:98-132; coeffs: re,im pairs).  Computed on the device

@@ -51,6 +51,30 @@ def test_open_without_device_reports_no_device():
     assert W.lib().wqc_cuda_last_error()
 
 
+def test_bindings_reach_the_library_with_a_null_state():
+    """Every binding that takes a state handle passes its arguments through
+    ctypes to the library, which rejects a null handle before any device
+    work: this checks the Python side of the boundary without a GPU."""
+    fake = W.CudaMps.__new__(W.CudaMps)
+    fake._h = None
+    fake.n = 4
+    calls = [
+        lambda: fake.sample([0, 2], 3, 7),
+        lambda: fake.sample_counts([(0, 0)], 1, 3, 7),
+        lambda: fake.expectation(["ZZZZ"], [1.0]),
+    ]
+    for call in calls:
+        with pytest.raises(W.WqcCudaError) as e:
+            call()
+        assert e.value.code == W.ERR_INVALID and "null" in str(e.value)
+    with pytest.raises(W.WqcCudaError) as e:
+        fake.sample_counts([(4, 0)], 1, 3, 7)  # checked on the host, as compute_outcome_probabilities does
+    assert e.value.code == W.ERR_QUBIT_OUT_OF_RANGE
+    with pytest.raises(W.WqcCudaError) as e:
+        fake.sample_counts([(0, 2)], 2, 3, 7)
+    assert e.value.code == W.ERR_INVALID and "classical bit index 2" in str(e.value)
+
+
 def test_workspace_bytes_matches_reference_formula():
     assert W.workspace_bytes(100, 128) == 52_428_800  # mps.rs:1870-1889
     assert W.workspace_bytes(50, 128) == 50 * 128 * 128 * 32

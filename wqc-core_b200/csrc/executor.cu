@@ -1522,6 +1522,85 @@ wqc_status wqc_mps_upload_site(wqc_mps* m, uint32_t site, uint32_t l, uint32_t r
     return WQC_OK;
 }
 
+wqc_status wqc_mps_sample(wqc_mps* m, const uint32_t* qubits, uint32_t count, uint32_t shots, uint64_t seed,
+                          uint64_t* out) {
+    if (!m || (!qubits && count) || (!out && shots)) return fail(WQC_ERR_INVALID, "null argument");
+    if (m->seg_first.size() != 1) return fail(WQC_ERR_INVALID, "sampling takes a single state, not a batch");
+    if (count > 64) return fail(WQC_ERR_INVALID, "at most 64 measured qubits per shot");
+    std::vector<int> bitpos(m->n, -1);
+    for (uint32_t j = 0; j < count; ++j) {
+        if (int(qubits[j]) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "measured qubit out of range");
+        if (bitpos[qubits[j]] >= 0) return fail(WQC_ERR_INVALID, "a qubit is listed twice");
+        bitpos[qubits[j]] = int(j);
+    }
+    if (shots == 0) return WQC_OK;
+    if (wqc_status s = sync_status(m)) return s;
+    const int n = m->n;
+    std::vector<int> dl(n), dr(n);
+    CUDA_TRY(cudaMemcpy(dl.data(), m->d_dl, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(dr.data(), m->d_dr, n * sizeof(int), cudaMemcpyDeviceToHost));
+    // E_q (dl[q] x dl[q]) at env_off[q]; E_n = 1 at env_off[n].
+    std::vector<unsigned long long> env_off(n + 1);
+    unsigned long long total = 0;
+    for (int q = 0; q < n; ++q) {
+        env_off[q] = total;
+        total += (unsigned long long)dl[q] * dl[q];
+    }
+    env_off[n] = total;
+    total += 1;
+    const size_t env_bytes = total * sizeof(double2);
+    const size_t tmp_bytes = size_t(2) * m->chi * m->chi * sizeof(double2);
+    const size_t aux_bytes = (n + 1) * sizeof(unsigned long long) + n * sizeof(int) + 64;
+    const size_t out_bytes = size_t(shots) * sizeof(uint64_t);
+    void *d_env = nullptr, *d_tmp = nullptr, *d_aux = nullptr, *d_out = nullptr;
+    auto release = [&]() {
+        if (d_env) dfree(m, d_env, env_bytes);
+        if (d_tmp) dfree(m, d_tmp, tmp_bytes);
+        if (d_aux) dfree(m, d_aux, aux_bytes);
+        if (d_out) dfree(m, d_out, out_bytes);
+    };
+    for (auto& pr : {std::make_pair(&d_env, env_bytes), std::make_pair(&d_tmp, tmp_bytes),
+                     std::make_pair(&d_aux, aux_bytes), std::make_pair(&d_out, out_bytes)})
+        if (wqc_status st = dmalloc(m, pr.first, pr.second)) {
+            release();
+            return st;
+        }
+    double2* env = static_cast<double2*>(d_env);
+    double2* tmp = static_cast<double2*>(d_tmp);
+    unsigned long long* d_off = static_cast<unsigned long long*>(d_aux);
+    int* d_bitpos = reinterpret_cast<int*>(d_off + n + 1);
+    const double2 one = cmake(1.0, 0.0);
+    cudaError_t e = cudaMemcpyAsync(env + env_off[n], &one, sizeof(double2), cudaMemcpyHostToDevice, m->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_off, env_off.data(), (n + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                            m->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_bitpos, bitpos.data(), n * sizeof(int), cudaMemcpyHostToDevice, m->stream);
+    // Right environments, from the last site down to site 1 (E_0 is not drawn from).
+    for (int q = n - 1; q >= 1 && e == cudaSuccess; --q) {
+        const int l = dl[q], r = dr[q];
+        const int g1 = int(std::min<long>((2L * l * r + 255) / 256, 4L * m->ctx->sm_count));
+        const int g2 = int(std::min<long>((long(l) * l + 255) / 256, 4L * m->ctx->sm_count));
+        sample_env_half_kernel<<<g1, 256, 0, m->stream>>>(m->site_ptr[q], l, r, env + env_off[q + 1], tmp);
+        sample_env_kernel<<<g2, 256, 0, m->stream>>>(m->site_ptr[q], l, r, tmp, env + env_off[q]);
+        count_launch(m, -1);
+        count_launch(m, -1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        const int grid = int(std::min<long>(long(shots), 8L * m->ctx->sm_count));
+        sample_shots_kernel<<<grid, 256, 3 * m->chi * sizeof(double2), m->stream>>>(
+            m->dev, env, d_off, d_bitpos, (unsigned long long)seed, int(shots), static_cast<unsigned long long*>(d_out));
+        count_launch(m, -1);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, m->stream);
+    m->stats.d2h_bytes += out_bytes;
+    wqc_status rc = e == cudaSuccess ? sync_status(m) : fail(WQC_ERR_CUDA, cudaGetErrorString(e));
+    release();
+    return rc;
+}
+
 wqc_status wqc_mps_expectation_pauli(wqc_mps* m, const char* labels, const double* coeffs, uint32_t nterms,
                                      double out[2]) {
     if (!m || !labels || !coeffs || !out) return fail(WQC_ERR_INVALID, "null argument");

@@ -209,4 +209,127 @@ __global__ void __launch_bounds__(256) pauli_expectation_kernel(DeviceMps mps, c
     if (threadIdx.x == 0) out[t] = env[0];
 }
 
+// ---------------------------------------------------------------------------
+// Shot sampling from the MPS.  The reference samples terminal measurements
+// from the dense statevector (src/sample.rs:85-131, 192-211), so only up to
+// 20 qubits; on the MPS the same distribution |<b|psi>|^2 / <psi|psi> is
+// drawn site by site (qubit q is site q).  With right environments
+// E_q = sum_s A_q[s] E_{q+1} A_q[s]^H (E_n = 1), a shot carries a row vector
+// v (v = 1 before site 0), draws s at site q with probability
+// p_s / (p_0 + p_1), p_s = w_s E_{q+1} w_s^H, w_s = v A_q[s], and goes on
+// with v = w_s / sqrt(p_s).  Every site is drawn, so the measured qubits get
+// their marginal distribution.
+// ---------------------------------------------------------------------------
+
+// tmp[a][s][c'] = sum_c A[a][s][c] E[c][c'] for one site (l x 2 x r).
+__global__ void __launch_bounds__(256) sample_env_half_kernel(const double2* site, int l, int r,
+                                                              const double2* env_next, double2* tmp) {
+    const long total = 2L * l * r;
+    for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += long(gridDim.x) * blockDim.x) {
+        const int cp = int(e % r);
+        const double2* arow = site + (e / r) * r;
+        double2 acc = cmake(0, 0);
+        for (int c = 0; c < r; ++c) cfma(acc, arow[c], env_next[size_t(c) * r + cp]);
+        tmp[e] = acc;
+    }
+}
+
+// env[a][a'] = sum_{s, c'} tmp[a][s][c'] conj(A[a'][s][c'])  (l x l).
+__global__ void __launch_bounds__(256) sample_env_kernel(const double2* site, int l, int r, const double2* tmp,
+                                                         double2* env) {
+    const long total = long(l) * l;
+    for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += long(gridDim.x) * blockDim.x) {
+        const double2* t = tmp + (e / l) * 2 * r;
+        const double2* k = site + (e % l) * 2 * r;
+        double2 acc = cmake(0, 0);
+        for (int x = 0; x < 2 * r; ++x) cfma_conj(acc, k[x], t[x]);
+        env[e] = acc;
+    }
+}
+
+// SplitMix64 (Steele, Lea and Flood, OOPSLA 2014): the uniform draw of shot
+// `shot` at site q is the top 53 bits of mix(mix(seed ^ mix(shot)) + q).
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double sample_uniform(unsigned long long seed, unsigned long long shot, int q) {
+    const unsigned long long key = splitmix64(seed ^ splitmix64(shot));
+    return double(splitmix64(key + (unsigned long long)q) >> 11) * 0x1.0p-53;
+}
+
+// One CTA per shot (grid-stride over shots).  envs + env_off[q] holds E_q
+// (dl[q] x dl[q]; E_n is 1 x 1); bitpos[q] is the output bit of qubit q, or
+// -1 when q is not measured.  Dynamic shared memory: 3 * chi_max complex.
+__global__ void __launch_bounds__(256) sample_shots_kernel(DeviceMps mps, const double2* envs,
+                                                           const unsigned long long* env_off, const int* bitpos,
+                                                           unsigned long long seed, int shots,
+                                                           unsigned long long* out) {
+    extern __shared__ __align__(16) double2 sv[];
+    double2* v = sv;
+    double2* w0 = sv + mps.chi_max;
+    double2* w1 = w0 + mps.chi_max;
+    __shared__ double red[2][256 / 32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    for (int shot = blockIdx.x; shot < shots; shot += gridDim.x) {
+        if (tid == 0) v[0] = cmake(1.0, 0.0);
+        __syncthreads();
+        unsigned long long bits = 0;
+        for (int q = 0; q < mps.n; ++q) {
+            const int l = mps.dl[q], r = mps.dr[q];
+            const double2* A = mps.site[q];
+            const double2* E = envs + env_off[q + 1];  // r x r
+            for (int c = tid; c < r; c += blockDim.x) {
+                double2 a0 = cmake(0, 0), a1 = cmake(0, 0);
+                for (int a = 0; a < l; ++a) {
+                    cfma(a0, v[a], A[(size_t(a) * 2 + 0) * r + c]);
+                    cfma(a1, v[a], A[(size_t(a) * 2 + 1) * r + c]);
+                }
+                w0[c] = a0;
+                w1[c] = a1;
+            }
+            __syncthreads();
+            double part0 = 0, part1 = 0;
+            for (int cp = tid; cp < r; cp += blockDim.x) {
+                double2 x0 = cmake(0, 0), x1 = cmake(0, 0);
+                for (int c = 0; c < r; ++c) {
+                    const double2 e = E[size_t(c) * r + cp];
+                    cfma(x0, w0[c], e);
+                    cfma(x1, w1[c], e);
+                }
+                part0 += x0.x * w0[cp].x + x0.y * w0[cp].y;  // Re(x conj(w))
+                part1 += x1.x * w1[cp].x + x1.y * w1[cp].y;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                part0 += __shfl_xor_sync(0xffffffffu, part0, o);
+                part1 += __shfl_xor_sync(0xffffffffu, part1, o);
+            }
+            if (lane == 0) {
+                red[0][wid] = part0;
+                red[1][wid] = part1;
+            }
+            __syncthreads();
+            double p0 = 0, p1 = 0;
+            for (int w = 0; w < nw; ++w) {  // every thread sums in the same order
+                p0 += red[0][w];
+                p1 += red[1][w];
+            }
+            p0 = fmax(p0, 0.0);
+            p1 = fmax(p1, 0.0);
+            const double u = sample_uniform(seed, (unsigned long long)shot, q);
+            const int s = (p0 + p1 > 0.0 && u * (p0 + p1) >= p0) ? 1 : 0;
+            const double ps = s ? p1 : p0;
+            const double scale = ps > 0.0 ? rsqrt(ps) : 1.0;
+            const double2* ws = s ? w1 : w0;
+            for (int c = tid; c < r; c += blockDim.x) v[c] = cscale(ws[c], scale);
+            if (s && bitpos[q] >= 0) bits |= 1ull << bitpos[q];
+            __syncthreads();
+        }
+        if (tid == 0) out[shot] = bits;
+    }
+}
+
 }  // namespace wqc

@@ -47,7 +47,7 @@ EXPORTS = (
     "wqc_mps_peak_vram_bytes", "wqc_mps_backend_label", "wqc_mps_set_profiling", "wqc_mps_kernel_stats",
     "wqc_mps_reset_stats", "wqc_mps_stream", "wqc_schedule_gates", "wqc_mps_reset", "wqc_mps_debug_workspace",
     "wqc_batch_create", "wqc_batch_apply_gates", "wqc_batch_amplitudes", "wqc_batch_slice_times",
-    "wqc_expectation_pauli_noalloc", "wqc_batch_expectation_pauli",
+    "wqc_expectation_pauli_noalloc", "wqc_batch_expectation_pauli", "wqc_mps_sample",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
@@ -113,6 +113,8 @@ def lib():
         L.wqc_mps_download_site.argtypes = [P, U32, ctypes.POINTER(U32), ctypes.POINTER(U32), D]
         L.wqc_mps_upload_site.argtypes = [P, U32, U32, U32, D]
         L.wqc_mps_expectation_pauli.argtypes = [P, ctypes.c_char_p, D, U32, D]
+        L.wqc_mps_sample.argtypes = [P, ctypes.POINTER(U32), U32, U32, ctypes.c_uint64,
+                                     ctypes.POINTER(ctypes.c_uint64)]
         L.wqc_mps_split_count.argtypes = [P]
         L.wqc_mps_split_count.restype = U32
         L.wqc_mps_split_records.argtypes = [P, P, U32, ctypes.POINTER(U32)]
@@ -324,6 +326,39 @@ class CudaMps:
         out = np.zeros(2)
         _check(lib().wqc_mps_expectation_pauli(self._h, joined, _dp(c.view(np.float64)), len(labels), _dp(out)))
         return complex(out[0], out[1])
+
+    def sample(self, qubits, shots: int, seed: int) -> np.ndarray:
+        """`shots` draws of the listed (distinct) qubits from |<b|psi>|^2:
+        element k, bit j is the outcome of qubits[j] in shot k."""
+        q = np.ascontiguousarray(qubits, dtype=np.uint32)
+        out = np.zeros(int(shots), dtype=np.uint64)
+        _check(lib().wqc_mps_sample(self._h, q.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(q), int(shots),
+                                    int(seed) & 0xFFFFFFFFFFFFFFFF,
+                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))))
+        return out
+
+    def sample_counts(self, measures, classical_bit_count: int, shots: int, seed: int) -> dict:
+        """Counts keyed like the reference's outcome_key (src/sample.rs:133-156):
+        measures are (qubit, cbit) pairs applied in order, the key has
+        classical_bit_count characters with cbit 0 rightmost."""
+        if classical_bit_count <= 0:
+            raise WqcCudaError(ERR_INVALID, "classical_bit_count must be > 0 for sample_counts")
+        for q, c in measures:
+            if q >= self.n:
+                raise WqcCudaError(ERR_QUBIT_OUT_OF_RANGE, f"qubit {q} out of range (limit {self.n})")
+            if c >= classical_bit_count:
+                raise WqcCudaError(ERR_INVALID, f"classical bit index {c} out of bounds (limit: {classical_bit_count})")
+        qubits = sorted({int(q) for q, _ in measures})
+        col = {q: j for j, q in enumerate(qubits)}
+        draws = self.sample(qubits, shots, seed)
+        counts: dict = {}
+        for b in np.unique(draws):
+            bits = [0] * classical_bit_count
+            for q, c in measures:
+                bits[c] = int(b >> np.uint64(col[q])) & 1
+            key = "".join(str(bits[classical_bit_count - 1 - i]) for i in range(classical_bit_count))
+            counts[key] = counts.get(key, 0) + int(np.count_nonzero(draws == b))
+        return counts
 
     def split_count(self) -> int:
         return int(lib().wqc_mps_split_count(self._h))
