@@ -194,6 +194,17 @@ WQC_API wqc_status wqc_mps_bond_dims(wqc_mps* mps, uint32_t* out);
 WQC_API wqc_status wqc_mps_download_site(wqc_mps* mps, uint32_t site, uint32_t* l, uint32_t* r, double* buf);
 WQC_API wqc_status wqc_mps_upload_site(wqc_mps* mps, uint32_t site, uint32_t l, uint32_t r, const double* buf);
 
+/* <bra|ket> = sum over all indices of ket sites times conjugated bra sites
+ * (overlap, mps.rs:1423-1474; the time split's final step,
+ * contract_time_split, mps.rs:1241-1281), by a left environment on the
+ * device.  Fails like the reference on registers of different width
+ * (EngineError::MismatchedRegister), mismatched site shapes and, with
+ * env_limit > 0, an environment of more than env_limit entries (the
+ * reference passes 256, its STARK witness limit, "mps overlap environment
+ * exceeds 256"); env_limit = 0 bounds it only by chi_ket x chi_bra.  Both
+ * states must come from the same context; single states only. */
+WQC_API wqc_status wqc_mps_overlap(wqc_mps* ket, wqc_mps* bra, uint32_t env_limit, double out[2]);
+
 /* `shots` draws from |<b|psi>|^2 / <psi|psi>, computed on the device from
  * the MPS (site-by-site conditional sampling against right environments), so
  * not limited to 20 qubits as the reference's dense route is

@@ -1522,6 +1522,79 @@ wqc_status wqc_mps_upload_site(wqc_mps* m, uint32_t site, uint32_t l, uint32_t r
     return WQC_OK;
 }
 
+wqc_status wqc_mps_overlap(wqc_mps* ket, wqc_mps* bra, uint32_t env_limit, double out[2]) {
+    if (!ket || !bra || !out) return fail(WQC_ERR_INVALID, "null argument");
+    if (ket->seg_first.size() != 1 || bra->seg_first.size() != 1)
+        return fail(WQC_ERR_INVALID, "the overlap takes single states, not batches");
+    if (ket->n != bra->n) return fail(WQC_ERR_INVALID, "mismatched register");  // EngineError::MismatchedRegister
+    if (ket->ctx != bra->ctx) return fail(WQC_ERR_INVALID, "the two states live on different contexts");
+    if (wqc_status s = sync_status(bra)) return s;
+    if (wqc_status s = sync_status(ket)) return s;
+    const int n = ket->n;
+    std::vector<int> kdl(n), kdr(n), bdl(n), bdr(n);
+    CUDA_TRY(cudaMemcpy(kdl.data(), ket->d_dl, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(kdr.data(), ket->d_dr, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(bdl.data(), bra->d_dl, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(bdr.data(), bra->d_dr, n * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int q = 0; q < n; ++q) {
+        if (kdl[q] != (q ? kdr[q - 1] : 1) || bdl[q] != (q ? bdr[q - 1] : 1))
+            return fail(WQC_ERR_INVALID, "mps site shape does not match the overlap");
+        if (env_limit && (unsigned long long)kdr[q] * bdr[q] > env_limit)  // mps.rs:1443-1448
+            return fail(WQC_ERR_INVALID, "mps overlap environment exceeds " + std::to_string(env_limit));
+    }
+    const size_t env_bytes = size_t(ket->chi) * bra->chi * sizeof(double2);
+    const size_t tmp_bytes = 2 * env_bytes;
+    void *d_a = nullptr, *d_b = nullptr, *d_t = nullptr;
+    auto release = [&]() {
+        if (d_a) dfree(ket, d_a, env_bytes);
+        if (d_b) dfree(ket, d_b, env_bytes);
+        if (d_t) dfree(ket, d_t, tmp_bytes);
+    };
+    for (auto& pr : {std::make_pair(&d_a, env_bytes), std::make_pair(&d_b, env_bytes), std::make_pair(&d_t, tmp_bytes)})
+        if (wqc_status st = dmalloc(ket, pr.first, pr.second)) {
+            release();
+            return st;
+        }
+    double2* env = static_cast<double2*>(d_a);
+    double2* nxt = static_cast<double2*>(d_b);
+    double2* tmp = static_cast<double2*>(d_t);
+    const double2 one = cmake(1.0, 0.0);
+    cudaError_t e = cudaMemcpyAsync(env, &one, sizeof(double2), cudaMemcpyHostToDevice, ket->stream);
+    int kl = 1, bl = 1;
+    for (int q = 0; q < n && e == cudaSuccess; ++q) {
+        if (kdl[q] != kl || bdl[q] != bl) {
+            e = cudaErrorInvalidValue;
+            break;
+        }
+        const int kr = kdr[q], br = bdr[q];
+        const long cap = 4L * ket->ctx->sm_count;
+        overlap_half_kernel<<<int(std::min<long>((2L * bl * kr + 255) / 256, cap)), 256, 0, ket->stream>>>(
+            env, kl, bl, ket->site_ptr[q], kr, tmp);
+        overlap_next_kernel<<<int(std::min<long>((long(kr) * br + 255) / 256, cap)), 256, 0, ket->stream>>>(
+            tmp, bl, kr, bra->site_ptr[q], br, nxt);
+        count_launch(ket, -1);
+        count_launch(ket, -1);
+        std::swap(env, nxt);
+        kl = kr;
+        bl = br;
+        e = cudaGetLastError();
+    }
+    double2 res = cmake(0, 0);
+    wqc_status rc = WQC_OK;
+    if (e == cudaErrorInvalidValue)
+        rc = fail(WQC_ERR_INVALID, "mps site shape does not match the overlap");
+    else if (e == cudaSuccess && (kl != 1 || bl != 1))
+        rc = fail(WQC_ERR_INVALID, "mps overlap left an open bond");
+    else if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&res, env, sizeof(double2), cudaMemcpyDeviceToHost, ket->stream);
+    if (rc == WQC_OK) rc = e == cudaSuccess ? sync_status(ket) : fail(WQC_ERR_CUDA, cudaGetErrorString(e));
+    release();
+    if (rc != WQC_OK) return rc;
+    out[0] = res.x;
+    out[1] = res.y;
+    return WQC_OK;
+}
+
 wqc_status wqc_mps_sample(wqc_mps* m, const uint32_t* qubits, uint32_t count, uint32_t shots, uint64_t seed,
                           uint64_t* out) {
     if (!m || (!qubits && count) || (!out && shots)) return fail(WQC_ERR_INVALID, "null argument");

@@ -209,6 +209,37 @@ __global__ void __launch_bounds__(256) pauli_expectation_kernel(DeviceMps mps, c
     if (threadIdx.x == 0) out[t] = env[0];
 }
 
+// <bra|ket> of two states by a left environment env[a][b] (ket bond a, bra
+// bond b), as the time split's overlap (mps.rs:1423-1474), two launches per
+// site so every step spreads over the GPU.  The reference caps the
+// environment at 256 entries (its CPU cost); here it is bounded only by the
+// scratch, chi_ket x chi_bra.
+// tmp[b][s][a'] = sum_a env[a][b] K[a][s][a']   (bl x 2 x kr)
+__global__ void __launch_bounds__(256) overlap_half_kernel(const double2* env, int kl, int bl, const double2* ket,
+                                                           int kr, double2* tmp) {
+    const long total = 2L * bl * kr;
+    for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += long(gridDim.x) * blockDim.x) {
+        const int ar = int(e % kr);
+        const int s = int((e / kr) & 1);
+        const int b = int(e / (2L * kr));
+        double2 acc = cmake(0, 0);
+        for (int a = 0; a < kl; ++a) cfma(acc, env[size_t(a) * bl + b], ket[(size_t(a) * 2 + s) * kr + ar]);
+        tmp[e] = acc;
+    }
+}
+
+// next[a'][b'] = sum_{b, s} tmp[b][s][a'] conj(B[b][s][b'])   (kr x br)
+__global__ void __launch_bounds__(256) overlap_next_kernel(const double2* tmp, int bl, int kr, const double2* bra,
+                                                           int br, double2* next) {
+    const long total = long(kr) * br;
+    for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += long(gridDim.x) * blockDim.x) {
+        const int bp = int(e % br), ar = int(e / br);
+        double2 acc = cmake(0, 0);
+        for (int bs = 0; bs < 2 * bl; ++bs) cfma_conj(acc, bra[size_t(bs) * br + bp], tmp[size_t(bs) * kr + ar]);
+        next[e] = acc;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Shot sampling from the MPS.  The reference samples terminal measurements
 // from the dense statevector (src/sample.rs:85-131, 192-211), so only up to

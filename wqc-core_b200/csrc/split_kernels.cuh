@@ -99,6 +99,8 @@ __global__ void reset_sites_kernel(DeviceMps mps);
 __global__ void site_amplitudes_kernel(DeviceMps mps, int target, double2* out);
 __global__ void pauli_expectation_kernel(DeviceMps mps, const char* labels, int nterms, double2* scratch,
                                          int env_cap, double2* out);
+__global__ void overlap_half_kernel(const double2* env, int kl, int bl, const double2* ket, int kr, double2* tmp);
+__global__ void overlap_next_kernel(const double2* tmp, int bl, int kr, const double2* bra, int br, double2* next);
 __global__ void sample_env_half_kernel(const double2* site, int l, int r, const double2* env_next, double2* tmp);
 __global__ void sample_env_kernel(const double2* site, int l, int r, const double2* tmp, double2* env);
 __global__ void sample_shots_kernel(DeviceMps mps, const double2* envs, const unsigned long long* env_off,

@@ -34,6 +34,7 @@ ERR_INVALID_QUBIT_COUNT = 10
 
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1
+OVERLAP_ENV_LIMIT = 256  # mps.rs:1443-1448 (the STARK witness limit)
 SPLIT_RULE_REFERENCE = 0
 SPLIT_RULE_EXACT = 1
 
@@ -48,6 +49,7 @@ EXPORTS = (
     "wqc_mps_reset_stats", "wqc_mps_stream", "wqc_schedule_gates", "wqc_mps_reset", "wqc_mps_debug_workspace",
     "wqc_batch_create", "wqc_batch_apply_gates", "wqc_batch_amplitudes", "wqc_batch_slice_times",
     "wqc_expectation_pauli_noalloc", "wqc_batch_expectation_pauli", "wqc_mps_sample",
+    "wqc_mps_overlap",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
@@ -113,6 +115,7 @@ def lib():
         L.wqc_mps_download_site.argtypes = [P, U32, ctypes.POINTER(U32), ctypes.POINTER(U32), D]
         L.wqc_mps_upload_site.argtypes = [P, U32, U32, U32, D]
         L.wqc_mps_expectation_pauli.argtypes = [P, ctypes.c_char_p, D, U32, D]
+        L.wqc_mps_overlap.argtypes = [P, P, U32, D]
         L.wqc_mps_sample.argtypes = [P, ctypes.POINTER(U32), U32, U32, ctypes.c_uint64,
                                      ctypes.POINTER(ctypes.c_uint64)]
         L.wqc_mps_split_count.argtypes = [P]
@@ -327,6 +330,13 @@ class CudaMps:
         _check(lib().wqc_mps_expectation_pauli(self._h, joined, _dp(c.view(np.float64)), len(labels), _dp(out)))
         return complex(out[0], out[1])
 
+    def overlap(self, bra: "CudaMps", env_limit: int = OVERLAP_ENV_LIMIT) -> complex:
+        """<bra|self> (overlap, mps.rs:1423-1474), computed on the device;
+        env_limit 0 lifts the reference's cap on the environment."""
+        out = np.zeros(2)
+        _check(lib().wqc_mps_overlap(self._h, bra._h, int(env_limit), _dp(out)))
+        return complex(out[0], out[1])
+
     def sample(self, qubits, shots: int, seed: int) -> np.ndarray:
         """`shots` draws of the listed (distinct) qubits from |<b|psi>|^2:
         element k, bit j is the outcome of qubits[j] in shot k."""
@@ -501,6 +511,52 @@ def run(n: int, chi: int, gates: np.ndarray, ctx: Context | None = None, rule: i
     m.set_split_rule(rule)
     m.apply_gates(gates)
     return m
+
+
+def bra_unitary_gates(second_half: np.ndarray):
+    """The adjoint of `second_half` in reverse as plain gates (mps.rs:1393-1421):
+    rotations negated, S^H = S Z, T^H = T T T Z, the rest self-inverse; None
+    when a MEASURE, RESET or IF is present."""
+    from . import circuits as C
+
+    out = []
+    for g in np.asarray(second_half, dtype=GATE_DTYPE)[::-1]:
+        k = int(g["kind"])
+        if k in (C.MEASURE, C.RESET, C.IF):
+            return None
+        if k in (C.RX, C.RY, C.RZ):
+            h = g.copy()
+            h["angle"] = -g["angle"]
+            out.append(h)
+        elif k == C.S:
+            z = g.copy()
+            z["kind"] = C.Z
+            out += [g, z]
+        elif k == C.T:
+            z = g.copy()
+            z["kind"] = C.Z
+            out += [g, g, g, z]
+        else:
+            out.append(g)
+    return np.array(out, dtype=GATE_DTYPE)
+
+
+def contract_time_split(n: int, gates: np.ndarray, split: int, max_bond: int, ctx: Context | None = None) -> complex:
+    """contract_time_split (mps.rs:1241-1249, 1358-1384): the ket runs the first
+    `split` gates, the bra the adjoint of the rest, both rejecting truncation,
+    and the result is their overlap under the reference's environment cap."""
+    gates = np.asarray(gates, dtype=GATE_DTYPE)
+    if split > len(gates):
+        raise WqcCudaError(ERR_INVALID, "time-split index past the gate list")
+    ket = CudaMps(n, max_bond, reject_truncation=True, ctx=ctx)
+    ket.apply_gates(gates[:split])
+    bra = CudaMps(n, max_bond, reject_truncation=True, ctx=ctx)
+    seq = bra_unitary_gates(gates[split:])
+    if seq is not None:
+        bra.apply_gates(seq)
+    else:
+        bra.apply_gates_adjoint(gates[split:][::-1].copy())
+    return ket.overlap(bra)
 
 
 def svd_flops(rows: int, cols: int) -> float:
