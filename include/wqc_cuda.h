@@ -103,7 +103,9 @@ WQC_API wqc_status wqc_batch_create(wqc_cuda_ctx* ctx, uint32_t count, const uin
                                     const uint32_t* max_bond_dims, int32_t precision, uint32_t max_concurrent_splits,
                                     wqc_mps** out);
 /* Gates of slice s are gates[offsets[s] .. offsets[s+1]); qubits are local to
- * the slice.  Semantics per slice as wqc_mps_apply_gates. */
+ * the slice.  Semantics per slice as wqc_mps_apply_gates.  Returns once the
+ * work is queued on the state's stream (a submit); wqc_mps_synchronize, or
+ * any call that hands results to the host, waits for it. */
 WQC_API wqc_status wqc_batch_apply_gates(wqc_mps* batch, const wqc_gate* gates, const uint32_t* offsets);
 /* <0...0|psi_s> of every slice: out[2s], out[2s+1]. */
 WQC_API wqc_status wqc_batch_amplitudes(wqc_mps* batch, double* out);

@@ -3,6 +3,8 @@
 * libwqc_cuda.so loads and exports every entry point include/*.h declares;
 * without a device, opening a context fails with WQC_ERR_NO_DEVICE instead
   of crashing or falling back to the CPU;
+* the Python bindings pass their arguments through ctypes to the library,
+  which rejects a null state before any device work;
 * the host scheduler expands gates into the reference's split sequence and
   keeps every site's operations in program order;
 * the circuit generators match their stated shapes.
