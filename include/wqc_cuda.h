@@ -121,7 +121,8 @@ WQC_API wqc_status wqc_batch_expectation_pauli(wqc_mps* batch, const char* label
                                                uint32_t nterms, double* out);
 
 /* Back to |0...0> with the split records cleared, keeping the device memory
- * (a fresh MpsState for the next request without reallocating). */
+ * (a fresh MpsState for the next request without reallocating); also after
+ * a cancelled or failed request, whose cancel word and status it clears. */
 WQC_API wqc_status wqc_mps_reset(wqc_mps* mps);
 
 /* MpsState::apply_gate (mps.rs:278-297) for each gate in order: 1q gates,

@@ -1195,11 +1195,14 @@ wqc_status wqc_batch_create(wqc_cuda_ctx* ctx, uint32_t count, const uint32_t* q
 
 wqc_status wqc_mps_reset(wqc_mps* m) {
     if (!m) return fail(WQC_ERR_INVALID, "null argument");
-    if (wqc_status st = sync_status(m)) return st;
+    // A reset starts the next request whatever the last one ended with (an
+    // error status, a cancellation): the queue drains, the cancel word and the
+    // device status word are cleared and the sites return to |0...0>.
+    CUDA_TRY(cudaStreamSynchronize(m->stream));
+    *m->h_cancel = 0;
     if (wqc_status st = reset_sites(m)) return st;
     std::fill(m->ub.begin(), m->ub.end(), 1);
     m->rec_count = 0;
-    *m->h_cancel = 0;
     return WQC_OK;
 }
 
