@@ -58,6 +58,7 @@ enum : int {
     kStatusBadShape = 1 << 2,
     kStatusNonFinite = 1 << 3,
     kStatusCancelled = 1 << 4,
+    kStatusSvdCheck = 1 << 5,  // sum sigma^2 != ||X||_F^2 (svd_guard.rs:234-255)
 };
 
 // ---------------------------------------------------------------------------

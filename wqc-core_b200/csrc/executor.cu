@@ -939,6 +939,7 @@ wqc_status sync_status(wqc_mps* m) {
     if (st & kStatusCancelled) return fail(WQC_ERR_CANCELLED, "computation cancelled: the client has gone");
     if (st & kStatusTruncationRejected) return fail(WQC_ERR_TRUNCATION_REJECTED, "mps bond exceeded chi");
     if (st & kStatusNonFinite) return fail(WQC_ERR_SVD_FAILED, "SVD of a two-site matrix produced non-finite values");
+    if (st & kStatusSvdCheck) return fail(WQC_ERR_SVD_FAILED, "SVD of a two-site matrix failed its check");
     if (st & kStatusJacobiNoConvergence) {
         const unsigned long long bits = (static_cast<unsigned long long>(static_cast<unsigned>(stv[3])) << 32) |
                                         static_cast<unsigned>(stv[4]);

@@ -538,7 +538,27 @@ struct JacobiCtl {
     int rot;
     unsigned long long relmax_bits;  // largest |gamma|/sqrt(alpha beta) seen this sweep (non-negative double bits)
     double fro_part;
+    double chk_in, chk_out;  // this CTA's share of ||X||_F^2 (after dust zeroing) and of sum sigma^2
 };
+
+// The Frobenius part of the reference's factorisation check (svd_reproduces,
+// svd_guard.rs:234-255): sum sigma^2 must equal ||X||_F^2 of the dust-zeroed
+// matrix to SVD_CHECK_TOL = 1e-9 relative (plus 1e-28).  The precision form's
+// complex64 columns carry ~1e-6 of rounding, so it is held to 1e-4.  The
+// probe-vector part needs V, which this Jacobi does not accumulate.
+constexpr double kSvdCheckTol = 1e-9;
+constexpr double kSvdCheckTolFp32 = 1e-4;
+
+__device__ __forceinline__ double block_total(double v, double* red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double t = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[w];
+    return t;
+}
 
 __device__ __forceinline__ int circle_at(int pos, int step, int b) {
     if (pos == 0) return 0;
@@ -885,6 +905,7 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
     for (int r = 0; r < C; ++r) fro2 += cluster.map_shared_rank(&ctl, r)->fro_part;
     const double dust = sqrt(fro2) * kDustRel;
     const double dust2 = dust * dust;
+    double chk_in = 0, chk_out = 0;
     // Load W (dust-zeroed; padding columns zero).
     for (int half = 0; half < 2; ++half) {
         const int id = half == 0 ? rank : 2 * C - 1 - rank;
@@ -895,6 +916,7 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
             const int col = id * b + c;
             double2 x = col < N ? src_at(i, col) : cmake(0, 0);
             if (cnorm2(x) < dust2) x = cmake(0, 0);
+            chk_in += cnorm2(x);
             base[size_t(c) * len + i] = to_store<T>(x);
         }
     }
@@ -1067,8 +1089,33 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
                 Bf.w[size_t(col) * M + r] = v;
             }
             for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-            if (lane == 0) Bf.sigma[col] = sqrt(s2);
+            if (lane == 0) {
+                Bf.sigma[col] = sqrt(s2);
+                chk_out += s2;
+            }
         }
+    }
+    // Factorisation check over the cluster (every CTA reaches it: the loop
+    // above ends on a cluster-uniform decision).
+    {
+        const double in_cta = block_total(chk_in, red);
+        const double out_cta = block_total(chk_out, red);
+        if (tid == 0) {
+            ctl.chk_in = in_cta;
+            ctl.chk_out = out_cta;
+        }
+        cluster.sync();
+        if (rank == 0 && tid == 0) {
+            double tin = 0, tout = 0;
+            for (int r = 0; r < C; ++r) {
+                const JacobiCtl* rc = cluster.map_shared_rank(&ctl, r);
+                tin += rc->chk_in;
+                tout += rc->chk_out;
+            }
+            const double tol = kF64 ? kSvdCheckTol : kSvdCheckTolFp32;
+            if (fabs(tout - tin) > tol * tin + 1e-28) atomicOr(status, kStatusSvdCheck);
+        }
+        cluster.sync();  // no CTA leaves while rank 0 reads its shared memory
     }
 }
 
@@ -1147,11 +1194,13 @@ __global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(con
     const double dust = sqrt(fro2) * kDustRel;
     const double dust2 = dust * dust;
     // W (dust-zeroed, zero padding columns) into the workspace.
+    double chk_in = 0, chk_out = 0;
     for (int col = rank; col < Np; col += C) {
         T* x = G + size_t(col) * len;
         for (int i = tid; i < len; i += nthreads) {
             double2 v = col < N ? src_at(i, col) : cmake(0, 0);
             if (cnorm2(v) < dust2) v = cmake(0, 0);
+            chk_in += cnorm2(v);
             x[i] = to_store<T>(v);
         }
     }
@@ -1264,7 +1313,31 @@ __global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(con
             Bf.w[size_t(col) * M + r] = v;
         }
         for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-        if (lane == 0) Bf.sigma[col] = sqrt(s2);
+        if (lane == 0) {
+            Bf.sigma[col] = sqrt(s2);
+            chk_out += s2;
+        }
+    }
+    // Factorisation check over the cluster, as in jacobi_cluster_kernel.
+    {
+        const double in_cta = block_total(chk_in, red);
+        const double out_cta = block_total(chk_out, red);
+        if (tid == 0) {
+            ctl.chk_in = in_cta;
+            ctl.chk_out = out_cta;
+        }
+        cluster.sync();
+        if (rank == 0 && tid == 0) {
+            double tin = 0, tout = 0;
+            for (int r = 0; r < C; ++r) {
+                const JacobiCtl* rc = cluster.map_shared_rank(&ctl, r);
+                tin += rc->chk_in;
+                tout += rc->chk_out;
+            }
+            const double tol = kF64 ? kSvdCheckTol : kSvdCheckTolFp32;
+            if (fabs(tout - tin) > tol * tin + 1e-28) atomicOr(status, kStatusSvdCheck);
+        }
+        cluster.sync();  // no CTA leaves while rank 0 reads its shared memory
     }
 }
 
