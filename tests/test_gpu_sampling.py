@@ -141,6 +141,12 @@ def test_sampling_argument_errors(cuda_ctx):
         m.sample([3], 4, 1)
     assert e.value.code == W.ERR_QUBIT_OUT_OF_RANGE
     assert m.sample([0, 1], 0, 1).size == 0
+    with pytest.raises(W.WqcCudaError) as e:  # an index past 2^31 must not wrap negative
+        m.sample([2 ** 31], 4, 1)
+    assert e.value.code == W.ERR_QUBIT_OUT_OF_RANGE
+    with pytest.raises(W.WqcCudaError) as e:
+        m.site(2 ** 31)
+    assert e.value.code == W.ERR_QUBIT_OUT_OF_RANGE
     b = W.CudaBatch([3, 4], [4, 4], ctx=cuda_ctx)
     with pytest.raises(W.WqcCudaError) as e:
         b.sample([0], 4, 1)

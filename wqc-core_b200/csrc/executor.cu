@@ -1393,7 +1393,7 @@ wqc_status wqc_batch_slice_times(wqc_mps* m, double* out_ms) {
 
 wqc_status wqc_mps_apply_1q(wqc_mps* m, uint32_t site, const double u[8]) {
     if (!m || !u) return fail(WQC_ERR_INVALID, "null argument");
-    if (int(site) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
+    if (site >= uint32_t(m->n)) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
     Expander ex;
     Mat2 mm;
     for (int i = 0; i < 4; ++i) mm.u[i] = make_double2(u[2 * i], u[2 * i + 1]);
@@ -1409,7 +1409,7 @@ static Mat4 mat4_from(const double u[32]) {
 
 wqc_status wqc_mps_apply_2q(wqc_mps* m, uint32_t left, const double u[32], uint8_t cf, wqc_split_info* info) {
     if (!m || !u) return fail(WQC_ERR_INVALID, "null argument");
-    if (int(left) + 1 >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "two-site apply needs adjacent positions");
+    if (uint64_t(left) + 1 >= uint64_t(m->n)) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "two-site apply needs adjacent positions");
     Expander ex;
     ex.two_at(int(left), mat4_from(u), cf != 0);
     const uint32_t seq = m->rec_count;
@@ -1423,7 +1423,7 @@ wqc_status wqc_mps_apply_2q(wqc_mps* m, uint32_t left, const double u[32], uint8
 
 wqc_status wqc_mps_apply_2q_routed(wqc_mps* m, uint32_t ctrl, uint32_t tgt, const double u[32]) {
     if (!m || !u) return fail(WQC_ERR_INVALID, "null argument");
-    if (int(ctrl) >= m->n || int(tgt) >= m->n || ctrl == tgt) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "bad qubit pair");
+    if (ctrl >= uint32_t(m->n) || tgt >= uint32_t(m->n) || ctrl == tgt) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "bad qubit pair");
     Expander ex;
     ex.two_routed(int(ctrl), int(tgt), mat4_from(u));
     return run_ops(m, ex.ops);
@@ -1474,7 +1474,7 @@ wqc_status wqc_mps_amplitude_zero(wqc_mps* m, double out[2]) {
 
 wqc_status wqc_mps_site_amplitudes(wqc_mps* m, uint32_t target, double out[4]) {
     if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
-    if (int(target) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "target out of range");
+    if (target >= uint32_t(m->n)) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "target out of range");
     site_amplitudes_kernel<<<1, 512, 4 * m->chi * sizeof(double2), m->stream>>>(m->dev, int(target), m->d_small);
     count_launch(m, -1);
     CUDA_TRY(cudaGetLastError());
@@ -1499,7 +1499,7 @@ wqc_status wqc_mps_bond_dims(wqc_mps* m, uint32_t* out) {
 
 wqc_status wqc_mps_download_site(wqc_mps* m, uint32_t site, uint32_t* l, uint32_t* r, double* buf) {
     if (!m || !l || !r) return fail(WQC_ERR_INVALID, "null argument");
-    if (int(site) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
+    if (site >= uint32_t(m->n)) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
     if (wqc_status s = sync_status(m)) return s;
     int dl = 0, dr = 0;
     CUDA_TRY(cudaMemcpy(&dl, m->d_dl + site, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1514,7 +1514,7 @@ wqc_status wqc_mps_download_site(wqc_mps* m, uint32_t site, uint32_t* l, uint32_
 
 wqc_status wqc_mps_upload_site(wqc_mps* m, uint32_t site, uint32_t l, uint32_t r, const double* buf) {
     if (!m || !buf) return fail(WQC_ERR_INVALID, "null argument");
-    if (int(site) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
+    if (site >= uint32_t(m->n)) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
     if (l == 0 || r == 0 || int(l) > m->chi || int(r) > m->chi) return fail(WQC_ERR_INVALID, "site shape exceeds max_bond_dim");
     if (wqc_status s = sync_status(m)) return s;
     CUDA_TRY(cudaMemcpy(m->site_ptr[site], buf, size_t(l) * 2 * r * sizeof(double2), cudaMemcpyHostToDevice));
@@ -1606,7 +1606,7 @@ wqc_status wqc_mps_sample(wqc_mps* m, const uint32_t* qubits, uint32_t count, ui
     if (count > 64) return fail(WQC_ERR_INVALID, "at most 64 measured qubits per shot");
     std::vector<int> bitpos(m->n, -1);
     for (uint32_t j = 0; j < count; ++j) {
-        if (int(qubits[j]) >= m->n) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "measured qubit out of range");
+        if (qubits[j] >= uint32_t(m->n)) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "measured qubit out of range");
         if (bitpos[qubits[j]] >= 0) return fail(WQC_ERR_INVALID, "a qubit is listed twice");
         bitpos[qubits[j]] = int(j);
     }
@@ -1736,7 +1736,7 @@ wqc_status wqc_mps_expectation_pauli(wqc_mps* m, const char* labels, const doubl
 
 wqc_status wqc_mps_debug_workspace(wqc_mps* m, uint32_t slot, int32_t which, void* out, uint64_t bytes) {
     if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
-    if (int(slot) >= m->nslots) return fail(WQC_ERR_INVALID, "slot out of range");
+    if (slot >= uint32_t(m->nslots)) return fail(WQC_ERR_INVALID, "slot out of range");
     if (wqc_status s = sync_status(m)) return s;
     SlotBuffers b;
     CUDA_TRY(cudaMemcpy(&b, m->d_slots + slot, sizeof(b), cudaMemcpyDeviceToHost));
