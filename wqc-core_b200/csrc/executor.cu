@@ -1515,7 +1515,9 @@ wqc_status wqc_mps_download_site(wqc_mps* m, uint32_t site, uint32_t* l, uint32_
 wqc_status wqc_mps_upload_site(wqc_mps* m, uint32_t site, uint32_t l, uint32_t r, const double* buf) {
     if (!m || !buf) return fail(WQC_ERR_INVALID, "null argument");
     if (site >= uint32_t(m->n)) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "site out of range");
-    if (l == 0 || r == 0 || int(l) > m->chi || int(r) > m->chi) return fail(WQC_ERR_INVALID, "site shape exceeds max_bond_dim");
+    // Against the site's own capacity (a batch slice may have a smaller chi_max than the state).
+    const uint32_t cap = uint32_t(m->site_chi[site]);
+    if (l == 0 || r == 0 || l > cap || r > cap) return fail(WQC_ERR_INVALID, "site shape exceeds max_bond_dim");
     if (wqc_status s = sync_status(m)) return s;
     CUDA_TRY(cudaMemcpy(m->site_ptr[site], buf, size_t(l) * 2 * r * sizeof(double2), cudaMemcpyHostToDevice));
     const int il = int(l), ir = int(r);
