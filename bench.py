@@ -1,19 +1,28 @@
 """Benchmark of the cuda MPS backend: two-site applies per second.
 
-One step is one whole circuit through the backend from |0...0> to
-<0...0|psi> on one GPU: by default the 50-qubit, depth-40 random circuit at
-chi_max 128 (random 1q layer, CZ/CNOT brickwork, 10% long-range CNOTs routed
-with SWAPs) in the plain FP64 form with the reference's split rule.  The
-metric counts every merge + gate + split (SWAPs and CCNOT-internal CNOTs
-included), the unit the reference's cost is made of.
+The workload is the 50-qubit, depth-40 random circuit at chi_max 128 (random
+1q layer, CZ/CNOT brickwork, 10% long-range CNOTs routed with SWAPs) in the
+plain FP64 form with the reference's split rule, from |0...0> to
+<0...0|psi>.  The metric counts every merge + gate + split (SWAPs and
+CCNOT-internal CNOTs included), the unit the reference's cost is made of.
+
+Both arms time the same gates.  The first 10 layers (the bonds grow to
+chi_max there) run untimed; the remaining gates are cut into K consecutive
+windows, and step k times window k on the state the previous windows left,
+ending with a read of <0...0|psi>.  The CUDA arm times each window with CUDA
+events on the state's stream (`value`) and with the wall clock around the C
+ABI calls, plan upload and result read included (`e2e`); `--impl reference`
+runs the same prefix and the same K windows on the FP64 CPU restatement of
+the reference path, one independent replica per host core.  The whole
+circuit from |0...0> is reported beside the windows (`whole_circuit`), and
+the same circuit under the exact split rule, checked against the committed
+oracle fixture, as `exact_rule`.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 
 With N > 1 (torchrun, one rank per GPU) every rank runs its own replica: a
 single circuit is a chain of dependent splits and does not shard, so the
 scaling is weak and there is no collective on the data path.
-`--impl reference` times the FP64 CPU restatement of the reference path on
-the host cores instead (rank 0 only).
 """
 from __future__ import annotations
 
@@ -48,14 +57,31 @@ def workload(name: str, depth: int = 0):
     return w
 
 
-def workload_config(w, rule: str) -> dict:
+def timed_windows(w, skip_layers: int, k: int):
+    """(g0, windows): the first `skip_layers` layers end at gate g0 and run
+    untimed; gates g0.. are cut into k consecutive windows of about equal
+    gate count, one per timed step."""
+    starts = w.layer_starts()
+    g0 = starts[skip_layers] if 0 < skip_layers < len(starts) else 0
+    k = max(1, min(k, len(w.gates) - g0))
+    edges = np.linspace(g0, len(w.gates), k + 1).round().astype(int)
+    return g0, [(int(edges[i]), int(edges[i + 1])) for i in range(k)]
+
+
+def workload_config(w, rule: str, g0: int, windows) -> dict:
+    timed = w.gates[g0:]
     return {
         "workload": f"{w.name}: {w.n} qubits, chi_max {w.chi}, plain FP64 (complex128), split rule {rule}",
         "qubits": w.n,
         "chi_max": w.chi,
         "gates": int(len(w.gates)),
         "logical_2q_gates": w.logical_two_qubit,
-        "splits_per_step": C.split_plan(w.gates),
+        "splits_per_circuit": C.split_plan(w.gates),
+        "timed_gates": [g0, int(len(w.gates))],
+        "timed_splits": C.split_plan(timed),
+        "steps_are": f"{len(windows)} consecutive windows of gates {g0}..{len(w.gates)} (one per step) after an "
+                     f"untimed prefix of gates 0..{g0} (the layers in which the bonds grow to chi_max); "
+                     f"both arms time these same windows",
         "seed": w.seed,
         "split_rule": rule,
         "l2": "flushed between steps (256 MiB device write outside the timed events)",
@@ -66,45 +92,45 @@ def workload_config(w, rule: str) -> dict:
 # ---------------------------------------------------------------------------
 # CPU leg: the oracle (FP64 restatement of the reference CPU path)
 # ---------------------------------------------------------------------------
-def oracle_sample(w, budget_s: float, threads: int = 1, skip_layers: int = 0):
-    """Run the workload's gate list on `threads` independent oracle replicas:
-    the first `skip_layers` layers untimed (bonds grow to chi_max there), then
-    whole gate chunks until `budget_s` seconds of timed work.  Returns (splits
-    in the timed window, window seconds, (first gate, last gate) of thread 0's
-    window)."""
+def oracle_windows(w, g0: int, windows, threads: int, budget_s: float = 0.0):
+    """The CPU restatement on `threads` independent replicas (one thread
+    each): gates 0..g0 untimed, then the windows in order, each timed with its
+    closing <0...0|psi> read.  With budget_s > 0 a replica stops after the
+    window that crosses the budget.  Returns (splits of the timed windows
+    over all replicas, the slowest replica's timed seconds, windows done by
+    replica 0)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
     O.lib()
-    starts = w.layer_starts()
-    g0 = starts[skip_layers] if 0 < skip_layers < len(starts) else 0
     done = [0] * threads
     secs = [0.0] * threads
-    window = [(g0, g0)] * threads
-    chunk = 16
+    wins = [0] * threads
     barrier = threading.Barrier(threads)
 
     def worker(t):
         m = O.OracleMps(w.n, w.chi)
         if g0:
             m.apply_gates(w.gates[:g0])
+        m.amplitude_zero()
         before = len(m.records())
         barrier.wait()
-        t0 = time.perf_counter()
-        i = g0
-        while i < len(w.gates) and time.perf_counter() - t0 < budget_s:
-            m.apply_gates(w.gates[i:i + chunk])
-            i += chunk
-        secs[t] = time.perf_counter() - t0
+        for a, b in windows:
+            t0 = time.perf_counter()
+            m.apply_gates(w.gates[a:b])
+            m.amplitude_zero()
+            secs[t] += time.perf_counter() - t0
+            wins[t] += 1
+            if budget_s > 0 and secs[t] >= budget_s:
+                break
         done[t] = len(m.records()) - before
-        window[t] = (g0, min(i, len(w.gates)))
 
     ths = [threading.Thread(target=worker, args=(t,)) for t in range(threads)]
     for th in ths:
         th.start()
     for th in ths:
         th.join()
-    return sum(done), max(secs), window[0]
+    return sum(done), max(secs), wins[0]
 
 
 SATURATED_LAYERS = {"config1": 10, "config0": 4}
@@ -410,34 +436,29 @@ def run_reference(args) -> None:
     if rank != 0:
         return
     w = workload(args.workload, args.depth)
+    g0, windows = timed_windows(w, SATURATED_LAYERS.get(args.workload, 0), args.steps)
     threads = os.cpu_count() or 1
-    budget = args.reference_budget
-    skip = SATURATED_LAYERS.get(args.workload, 0)
-    rates = []
-    for step in range(args.warmup + args.steps):
-        timed = step >= args.warmup
-        splits, secs, win = oracle_sample(w, budget if timed else 1.0, threads, skip if timed else 0)
-        if timed:
-            rates.append(splits / secs)
-    value = statistics.median(rates)
-    sample = (f"each step: {threads} independent replicas (one thread each) of the FP64 restatement; the first "
-              f"{skip} layers run untimed so the bonds reach chi_max, then gates {win[0]}..{win[1]} of "
-              f"{len(w.gates)} are timed (~{budget:.0f} s window per replica)")
+    splits, secs, _ = oracle_windows(w, g0, windows, threads)
+    value = splits / secs
+    sample = (f"{threads} independent replicas (one thread each) of the FP64 restatement of the reference CPU path; "
+              f"each runs gates 0..{g0} untimed, then the {len(windows)} timed windows of gates {g0}..{len(w.gates)} "
+              f"(one per step, each closed by a <0...0|psi> read): {splits} splits over all replicas in "
+              f"{secs:.1f} s (slowest replica)")
     line = {
         "impl": "reference",
         "metric": METRIC,
         "value": value,
         "unit": UNIT,
         "n_gpus": args.gpus,
-        "steps": args.steps,
+        "steps": len(windows),
         "warmup": args.warmup,
-        "ms_per_step": 1000.0 * budget,
+        "ms_per_step": 1000.0 * secs / len(windows),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": workload_config(w, "reference"),
+        "config": workload_config(w, "reference", g0, windows),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -523,6 +544,65 @@ def measured_fp64_peak(torch) -> float:
     return best
 
 
+def record_flops(W, recs) -> float:
+    """Algorithmic SVD flops of the splits in `recs` (the Jacobi's work)."""
+    flops = 0.0
+    for r in recs:
+        if int(r["path"]) == 1:
+            flops += W.svd_flops(int(r["ell"]), int(r["cols"]))
+        elif int(r["path"]) == 2:
+            flops += W.svd_flops(int(r["ell"]), int(r["cols"])) + W.svd_flops(int(r["rows"]), int(r["cols"]))
+        else:
+            flops += W.svd_flops(int(r["rows"]), int(r["cols"]))
+    return flops
+
+
+def exact_rule_leg(W, torch, ctx, flush) -> dict:
+    """The headline circuit under the exact split rule (an exact SVD on every
+    split, so the result does not depend on the range finder's rank-48 test
+    matrix), one pass from |0...0>, checked against the oracle's fixture
+    (tests/golden/config1_exact.npz): kept chi and split paths per split,
+    discarded weights, the norm and the amplitude."""
+    w = C.config1()
+    m = W.CudaMps(w.n, w.chi, ctx=ctx)
+    m.set_split_rule(W.SPLIT_RULE_EXACT)
+    stream = torch.cuda.ExternalStream(m.stream())
+    flush.fill_(float(np.random.random()))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.apply_gates(w.gates)
+    amp = m.amplitude_at_compact_zero()
+    e1.record(stream)
+    e1.synchronize()
+    sec = e0.elapsed_time(e1) * 1e-3
+    rec = m.split_records()
+    norm2 = m.expectation(["I" * w.n], [1.0]).real
+    out = {
+        "workload": f"{w.name}: {w.n} qubits, chi_max {w.chi}, plain FP64, split rule exact",
+        "applies_per_s": len(rec) / sec,
+        "seconds": sec,
+        "amplitude": [amp.real, amp.imag],
+        "norm2": norm2,
+    }
+    fx = os.path.join(ROOT, "tests", "golden", "config1_exact.npz")
+    if os.path.exists(fx):
+        ref = np.load(fx)
+        rr = ref["records"]
+        out["vs_oracle"] = {
+            "splits_equal": bool(len(rr) == len(rec)),
+            "chi_path_shape_bit_exact": bool(len(rr) == len(rec) and all(
+                np.array_equal(rr[k], rec[k]) for k in ("left_site", "rows", "cols", "path", "chi"))),
+            "max_weight_diff": float(np.max(np.abs(rr["discarded_weight"] - rec["discarded_weight"])))
+            if len(rr) == len(rec) else None,
+            "norm2_rel_err": abs(norm2 - float(ref["norm2"])) / float(ref["norm2"]) if "norm2" in ref else None,
+            "amp_abs_err": abs(amp - complex(ref["amplitude"])),
+            "oracle_amplitude": [complex(ref["amplitude"]).real, complex(ref["amplitude"]).imag],
+        }
+    m.close()
+    return out
+
+
 def run_cuda(args) -> None:
     import torch
 
@@ -540,6 +620,7 @@ def run_cuda(args) -> None:
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     w = workload(args.workload, args.depth)
+    g0, windows = timed_windows(w, SATURATED_LAYERS.get(args.workload, 0), args.steps)
     rule = W.SPLIT_RULE_EXACT if args.split_rule == "exact" else W.SPLIT_RULE_REFERENCE
     ctx = W.Context(local)
     m = W.CudaMps(w.n, w.chi, ctx=ctx)
@@ -548,8 +629,33 @@ def run_cuda(args) -> None:
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     peak = measured_fp64_peak(torch) if rank == 0 else None
 
-    def one_step(timed: bool):
+    def whole_pass():
         m.reset()
+        flush.fill_(float(np.random.random()))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.apply_gates(w.gates)
+        amp = m.amplitude_at_compact_zero()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), amp
+
+    for _ in range(args.warmup):
+        whole_pass()
+    # Timed steps: the untimed prefix, then one window per step.
+    m.reset()
+    if g0:
+        m.apply_gates(w.gates[:g0])
+    m.amplitude_at_compact_zero()
+    prefix_splits = m.split_count()
+    m.reset_stats()
+    m.set_profiling(True)
+    dev_ms, wall_s = [], []
+    clocks = ClockSampler(local)
+    clocks.start()
+    amp = 0j
+    for a, b in windows:
         flush.fill_(float(np.random.random()))
         torch.cuda.synchronize()
         if dist is not None:
@@ -557,70 +663,52 @@ def run_cuda(args) -> None:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
         e0.record(stream)
-        m.apply_gates(w.gates)
+        m.apply_gates(w.gates[a:b])
         amp = m.amplitude_at_compact_zero()
         e1.record(stream)
         e1.synchronize()
-        wall = time.perf_counter() - t0
-        return e0.elapsed_time(e1), wall, amp
-
-    for _ in range(args.warmup):
-        one_step(False)
-    m.reset_stats()
-    m.set_profiling(True)
-    dev_ms, wall_s, amps = [], [], []
-    clocks = ClockSampler(local)
-    clocks.start()
-    splits = 0
-    flops = 0.0
-    for _ in range(args.steps):
-        d, wl, amp = one_step(True)
-        dev_ms.append(d)
-        wall_s.append(wl)
-        amps.append(amp)
-        recs = m.split_records()
-        splits += len(recs)
-        for r in recs:
-            if int(r["path"]) == 1:
-                flops += W.svd_flops(int(r["ell"]), int(r["cols"]))
-            elif int(r["path"]) == 2:
-                flops += W.svd_flops(int(r["ell"]), int(r["cols"])) + W.svd_flops(int(r["rows"]), int(r["cols"]))
-            else:
-                flops += W.svd_flops(int(r["rows"]), int(r["cols"]))
+        wall_s.append(time.perf_counter() - t0)
+        dev_ms.append(e0.elapsed_time(e1))
     clk = clocks.stop()
+    m.set_profiling(False)
     stats = m.kernel_stats()
-    total_dev_ms = sum(dev_ms)
-    total_wall = sum(wall_s)
-    total_dev_ms, total_wall = aggregate_ranks(dist, "cuda", total_dev_ms, total_wall)
+    recs = m.split_records()[prefix_splits:]
+    splits = len(recs)
+    flops = record_flops(W, recs)
+    steps = len(windows)
+    total_dev_ms, total_wall = aggregate_ranks(dist, "cuda", sum(dev_ms), sum(wall_s))
     value = world * splits / (total_dev_ms * 1e-3)
     e2e = world * splits / total_wall
     jac_ms = stats["milliseconds"]["jacobi_svd"]
     jac_n = stats["launches"]["jacobi_svd"]
     achieved = flops / (jac_ms * 1e-3) / 1e12 if jac_ms > 0 else None
+    whole_ms, whole_amp = whole_pass()
+    whole_splits = m.split_count()
     if rank == 0:
         line = {
             "metric": METRIC,
             "value": value,
             "unit": UNIT,
             "n_gpus": world,
-            "steps": args.steps,
+            "steps": steps,
             "warmup": args.warmup,
-            "ms_per_step": total_dev_ms / args.steps,
+            "ms_per_step": total_dev_ms / steps,
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f64",
-            "data": "synthetic (seeded generator, same circuit every step)",
-            "config": workload_config(w, args.split_rule),
+            "data": "synthetic (seeded generator, same circuit every run)",
+            "config": workload_config(w, args.split_rule, g0, windows),
             "e2e": {
                 "value": e2e,
                 "unit": UNIT,
-                "h2d_bytes_per_step": stats["h2d_bytes"] // args.steps,
-                "d2h_bytes_per_step": stats["d2h_bytes"] // args.steps,
-                "note": "wall clock of wqc_mps_apply_gates(host gate list) + wqc_mps_amplitude_zero (host result)",
+                "h2d_bytes_per_step": stats["h2d_bytes"] // steps,
+                "d2h_bytes_per_step": stats["d2h_bytes"] // steps,
+                "note": "wall clock of wqc_mps_apply_gates(host gate list of the window) + wqc_mps_amplitude_zero "
+                        "(host result) per step",
             },
             "roofline": {
-                "bound": "tensor",
+                "bound": "fp64",
                 "kernel": "jacobi_cluster_kernel (FP64 one-sided Jacobi SVD)",
                 "achieved": achieved,
                 "peak": peak,
@@ -628,33 +716,40 @@ def run_cuda(args) -> None:
                 "frac": (achieved / peak) if (achieved and peak) else None,
                 "traffic": 767232,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one saturated launch "
-                                  "(five exact 256 x 256 splits on 16-CTA clusters; "
-                                  "profiles/jacobi_svd_random50_d40_chi128.md); W stays in shared memory",
-                "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
-                "flops_per_step": flops / args.steps,
-                "kernel_ms_per_step": jac_ms / args.steps,
-                "launches_per_step": jac_n / args.steps,
-                "svds_per_step": stats["jacobi_tasks"] / args.steps,
+                                  "(five exact 256 x 256 splits on 16-CTA clusters); W stays in shared memory",
+                "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (the FP64 pipe: no tensor-core "
+                               "instruction is issued; MEASURED_PEAKS.json has no FP64 figure)",
+                "flops_per_step": flops / steps,
+                "kernel_ms_per_step": jac_ms / steps,
+                "launches_per_step": jac_n / steps,
+                "svds_per_step": stats["jacobi_tasks"] / steps,
                 "sweeps_per_svd": (stats["jacobi_sweeps"] / stats["jacobi_tasks"]) if stats["jacobi_tasks"] else None,
                 "flop_count": "4*(14*q*p^2 + 8*p^3) per decomposed p x q matrix (Golub-Van Loan), complex",
             },
-            "kernel_ms_per_step": {k: v / args.steps for k, v in stats["milliseconds"].items()},
+            "kernel_ms_per_step": {k: v / steps for k, v in stats["milliseconds"].items()},
             "gpu_launches": stats["total_launches"],
             "clocks": clk,
-            "amplitude": [amps[-1].real, amps[-1].imag],
+            "amplitude": [amp.real, amp.imag],
+            "whole_circuit": {
+                "applies_per_s": whole_splits / (whole_ms * 1e-3),
+                "seconds": whole_ms * 1e-3,
+                "splits": whole_splits,
+                "amplitude": [whole_amp.real, whole_amp.imag],
+                "note": "one pass of the whole circuit from |0...0>, CUDA events, L2 flushed before",
+            },
         }
         if world == 1 and not args.no_cpu_baseline:
-            skip = SATURATED_LAYERS.get(args.workload, 0)
-            s, secs, win = oracle_sample(w, args.cpu_budget, 1, skip)
+            s1, secs, nwin = oracle_windows(w, g0, windows, 1, budget_s=args.cpu_budget)
             line["cpu_baseline"] = {
-                "value": s / secs,
+                "value": s1 / secs,
                 "unit": UNIT,
                 "cores": 1,
                 "kind": "port",
-                "sample": f"FP64 restatement on 1 thread (the reference MPS path is single-threaded): first {skip} "
-                          f"layers untimed (bonds reach chi_max), then gates {win[0]}..{win[1]} of {len(w.gates)} "
-                          f"({s} splits) timed in {secs:.1f} s",
+                "sample": f"FP64 restatement on 1 thread (the reference MPS path is single-threaded): gates 0..{g0} "
+                          f"untimed, then the first {nwin} of the {steps} timed windows ({s1} splits) in {secs:.1f} s",
             }
+        if world == 1 and args.workload == "config1" and args.exact_rule_leg:
+            line["exact_rule"] = exact_rule_leg(W, torch, ctx, flush)
         if world == 1 and args.batch_slices > 0:
             line["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush,
                                       0.0 if args.no_cpu_baseline else args.cpu_budget)
@@ -664,7 +759,7 @@ def run_cuda(args) -> None:
         if world == 1 and args.large_chi_leg:
             line["large_chi"] = large_chi_leg(W, torch, ctx, flush, 0.0 if args.no_cpu_baseline else args.cpu_budget)
         if world == 1 and args.precision_leg:
-            line["precision_form"] = precision_leg(W, torch, ctx, w, rule, args.steps, flush, value)
+            line["precision_form"] = precision_leg(W, torch, ctx, w, rule, 2, flush, whole_splits / (whole_ms * 1e-3))
             if args.batch_slices > 0:
                 line["precision_form"]["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush, 0.0,
                                                             W.PRECISION_FP32)
@@ -688,8 +783,9 @@ def main():
                     help="layers of the config1 / config4 circuit (0: their full 40 / 100; a prefix for profiling)")
     ap.add_argument("--split-rule", choices=("reference", "exact"), default="reference")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
-    ap.add_argument("--reference-budget", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-exact-rule-leg", dest="exact_rule_leg", action="store_false",
+                    help="skip the headline circuit under the exact split rule, checked against the oracle fixture")
     ap.add_argument("--no-differentiation-leg", dest="differentiation_leg", action="store_false",
                     help="skip the parameter-shift gradient of the 32-qubit ansatz run after the timed steps")
     ap.add_argument("--no-large-chi-leg", dest="large_chi_leg", action="store_false",

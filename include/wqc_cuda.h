@@ -65,6 +65,14 @@ typedef struct wqc_mps wqc_mps;
 /* Message of the last failing call on this thread (thread-local, never NULL). */
 WQC_API const char* wqc_cuda_last_error(void);
 
+/* Byte counts of the last call on this thread that returned WQC_ERR_OOM:
+ * the device memory it needed and the free device memory it saw (0, 0
+ * before any).  They fill EngineError::InsufficientMemory { required,
+ * available } (src/engine.rs:72), which the reference raises from
+ * ensure_mps_workspace_budget (src/tn/mps.rs:36-48).  Either pointer may be
+ * NULL. */
+WQC_API void wqc_cuda_last_oom(uint64_t* required, uint64_t* available);
+
 /* Open the process-wide context on `device` (-1: WQC_CUDA_DEVICE or 0).
  * Replaces the shared device probe (engine_status.rs:40-102). */
 WQC_API wqc_status wqc_cuda_open(int device, wqc_cuda_ctx** out);
@@ -185,15 +193,40 @@ WQC_API void wqc_mps_cancel(wqc_mps* mps);
 WQC_API wqc_status wqc_mps_amplitude_zero(wqc_mps* mps, double out[2]);
 
 /* site_amplitudes (mps.rs:679-693), the trace feeder of trace.rs:401:
- * out = a0.re, a0.im, a1.re, a1.im.  control_probability is |a1|^2. */
+ * out = a0.re, a0.im, a1.re, a1.im.  control_probability is |a1|^2.
+ * Single states only.  The left and right environments (left_environment,
+ * right_environment, mps.rs:700-740) stay cached on the device between
+ * calls: a call recomputes only the ones that operations since the last
+ * call have touched, so the per-gate reads of trace.rs cost one chain over
+ * the sites an operation changed rather than over the whole register. */
 WQC_API wqc_status wqc_mps_site_amplitudes(wqc_mps* mps, uint32_t target, double out[4]);
+
+/* site_amplitudes for `count` targets in one call (one launch, one
+ * synchronisation): out[4k .. 4k+3] for targets[k].  resolve_pre_amps
+ * (trace.rs:375-411) reads the control probabilities and the target's
+ * amplitudes of one step; a disjoint layer (emit_disjoint_layer,
+ * trace.rs:264-315) reads every gate's before applying any. */
+WQC_API wqc_status wqc_mps_site_amplitudes_many(wqc_mps* mps, const uint32_t* targets, uint32_t count, double* out);
+
+/* The dense state, 2^n complex values (re,im pairs) with basis bit q =
+ * qubit q, contracted on the device.  WQC_DENSE_TO_DENSE_STATE follows
+ * to_dense_state (mps.rs:742-780), which skips site entries with |x|^2 <
+ * 1e-30; WQC_DENSE_STATEVECTOR follows contract_to_statevector
+ * (mps.rs:215-260): every entry, and qubit_count <= 20 or the reference's
+ * error.  At most 28 qubits; single states only. */
+enum wqc_dense_mode { WQC_DENSE_TO_DENSE_STATE = 0, WQC_DENSE_STATEVECTOR = 1 };
+WQC_API wqc_status wqc_mps_to_dense(wqc_mps* mps, int32_t mode, double* out);
 
 /* Right bond of every site (out has qubit_count entries). */
 WQC_API wqc_status wqc_mps_bond_dims(wqc_mps* mps, uint32_t* out);
 
 /* Read / write one site tensor [l][2][r] as re,im pairs (used for
  * to_dense_state, overlap and tests; mps.rs:742-780, 1421-1474).  With
- * buf == NULL only the shape is returned. */
+ * buf == NULL only the shape is returned.  Uploads are taken one site at a
+ * time; the next call that computes on the state first checks that the
+ * chain closes (each left bond equals the left neighbour's right bond, the
+ * first left and last right bonds are 1) and fails with WQC_ERR_INVALID
+ * ("uploaded sites do not chain") otherwise. */
 WQC_API wqc_status wqc_mps_download_site(wqc_mps* mps, uint32_t site, uint32_t* l, uint32_t* r, double* buf);
 WQC_API wqc_status wqc_mps_upload_site(wqc_mps* mps, uint32_t site, uint32_t l, uint32_t r, const double* buf);
 
@@ -239,19 +272,25 @@ WQC_API wqc_status wqc_mps_expectation_pauli(wqc_mps* mps, const char* labels, c
  * qubit_count * site_stride complex128 values (re,im pairs); site q starts at
  * complex element q * site_stride and is [l][2][r] row-major, r =
  * bond_dims[q] and l = bond_dims[q - 1] (1 for q = 0), the layout that
- * wqc_mps_download_site returns.  bond_dims, labels, coeffs and out are host
- * memory.  stream: a cudaStream_t of the current device (NULL = the legacy
- * default stream); the call returns once its work on it has finished.
+ * wqc_mps_download_site returns.  The chain must be closed: the last right
+ * bond, bond_dims[qubit_count - 1], is 1 (else WQC_ERR_INVALID).  bond_dims,
+ * labels, coeffs and out are host memory; labels holds nterms *
+ * qubit_count characters and coeffs 2 * nterms doubles.  stream: a
+ * cudaStream_t of the current device (NULL = the legacy default stream).
+ *
+ * The call is synchronous: it returns once its work on `stream` has
+ * finished and the result is in `out`.  It must not be called while
+ * `stream` is being captured into a CUDA graph (it then returns
+ * WQC_ERR_INVALID without enqueuing anything).
  *
  * Working memory is one array of 16 MiB + 128 KiB that the library holds in
  * every GPU where this code is loaded, until the process exits.  Limits:
  * bond dimensions 1..256 and at most 1024 qubits; larger sizes are rejected
  * with WQC_ERR_INVALID or WQC_ERR_INVALID_QUBIT_COUNT and a message naming
  * the limit.  The first call on a device looks up that device's address of
- * the array (and may load this code onto the GPU); make that first call
- * before any stream capture.  All calls on a device share the array, which
- * keeps the last call's contents; calls that overlap on the GPU (from two
- * host threads at once) race on it, so serialise them. */
+ * the array (and may load this code onto the GPU).  All calls on a device
+ * share the array, which keeps the last call's contents; calls that overlap
+ * on the GPU (from two host threads at once) race on it, so serialise them. */
 WQC_API wqc_status wqc_expectation_pauli_noalloc(const double* sites, uint64_t site_stride, const uint32_t* bond_dims,
                                                  uint32_t qubit_count, const char* labels, const double* coeffs,
                                                  uint32_t nterms, void* stream, double out[2]);

@@ -132,3 +132,45 @@ def test_generators_have_the_stated_shapes():
     assert len(params) == 512 and int(np.sum(pidx >= 0)) == 512
     labels, coeffs = C.zz_x_observable(32)
     assert len(labels) == 63 and all(len(x) == 32 for x in labels)
+
+
+def test_cuda_request_without_device_fails():
+    """A `cuda` request without a device is reported as unavailable and no
+    state is built: there is no CPU fallback (engine_status.rs:40-84)."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    st = W.probe_tn_engine_status("cuda")
+    assert st["active"] == "unavailable" and "CUDA device not found" in st["note"]
+    with pytest.raises(W.WqcCudaError) as e:
+        W.CudaMps(4, 8)
+    assert e.value.code == W.ERR_NO_DEVICE
+
+
+def test_oom_byte_counts_start_at_zero():
+    """wqc_cuda_last_oom is exported and reports (0, 0) before any OOM on
+    this thread."""
+    import threading
+
+    out = []
+    t = threading.Thread(target=lambda: out.append(W.last_oom()))
+    t.start()
+    t.join()
+    assert out == [(0, 0)]
+
+
+def test_pauli_labels_are_checked_before_the_c_abi():
+    """The C ABI reads nterms * width label bytes and 2 * nterms doubles; the
+    binding refuses short labels and short coefficient arrays first."""
+    fake = W.CudaMps.__new__(W.CudaMps)
+    fake._h = None
+    fake.n = 4
+    with pytest.raises(ValueError, match="characters"):
+        fake.expectation(["ZZZ"], [1.0])
+    with pytest.raises(ValueError, match="coefficients"):
+        fake.expectation(["ZZZZ", "XXXX"], [1.0])
+    with pytest.raises(ValueError, match="characters"):
+        W.expectation_pauli_noalloc(0, 8, [2, 2, 1], ["ZZ"], [1.0])
+    with pytest.raises(ValueError, match="coefficients"):
+        W.expectation_pauli_noalloc(0, 8, [2, 2, 1], ["ZZZ"], [])

@@ -52,6 +52,24 @@ def test_state_beyond_device_memory_is_refused(cuda_ctx):
     with pytest.raises(W.WqcCudaError) as e:
         W.CudaMps(n, 256, ctx=cuda_ctx)
     assert e.value.code == W.ERR_OOM and "Insufficient memory" in str(e.value)
+    # EngineError::InsufficientMemory { required, available } gets both counts
+    # through wqc_cuda_last_oom.
+    assert e.value.required >= W.workspace_bytes(n, 256) > e.value.available > 0
+    assert W.last_oom() == (e.value.required, e.value.available)
     m = W.CudaMps(4, 4, ctx=cuda_ctx)  # the context is still usable
     m.apply_gates(C.gates_array([C.g1(C.H, 0)]))
     assert abs(m.amplitude_zero() - 2 ** -0.5) < 1e-12
+
+
+def test_uploaded_sites_that_do_not_chain_are_refused(cuda_ctx):
+    """An upload whose bonds disagree with its neighbours' is refused by the
+    next call that computes on the state, instead of giving wrong results."""
+    m = W.CudaMps(4, 8, ctx=cuda_ctx)
+    rng = np.random.default_rng(3)
+    m.set_site(1, rng.normal(size=(1, 2, 4)) + 0j)  # site 2 still has left bond 1
+    with pytest.raises(W.WqcCudaError) as e:
+        m.apply_gates(C.gates_array([C.g2(C.CNOT, 0, 1)]))
+    assert e.value.code == W.ERR_INVALID and "do not chain" in str(e.value)
+    m.set_site(2, rng.normal(size=(4, 2, 1)) + 0j)  # now 1 x 2 x 4 | 4 x 2 x 1 closes the chain
+    m.apply_gates(C.gates_array([C.g2(C.CNOT, 0, 1)]))
+    assert np.isfinite(m.amplitude_zero())

@@ -32,17 +32,34 @@ def amp_err(a: complex, b: complex, n: int) -> float:
     return abs(a - b) / max(abs(b), 2.0 ** (-n / 2.0))
 
 
-def assert_records_match(got, ref):
+def oracle_drift(n, chi, gates, rule=0):
+    """Per-split |discarded weight| difference between two oracle runs of the
+    same circuit, one with its Golub-Kahan SVD (the reference's primary) and
+    one with its Jacobi SVD as primary: how far two FP64 SVDs of the same
+    matrices drift apart once truncation carries their rounding on."""
+    runs = []
+    for primary in (0, 1):
+        O.set_primary_svd(primary)
+        try:
+            runs.append(O.run(n, chi, gates, rule=rule).records())
+        finally:
+            O.set_primary_svd(0)
+    assert all(np.array_equal(runs[0][k], runs[1][k]) for k in ("rows", "cols", "path", "chi"))
+    return np.abs(runs[0]["discarded_weight"] - runs[1]["discarded_weight"])
+
+
+def assert_records_match(got, ref, drift=None):
+    """Shapes, paths and kept chi bit-exact; discarded weights within
+    DISC_ATOL (times the weight's size), plus, for long truncating runs, ten
+    times the oracle's own drift between two SVDs up to that split."""
     assert len(got) == len(ref), f"split count {len(got)} != {len(ref)}"
     for k in ("left_site", "rows", "cols", "ell", "path", "chi"):
         bad = np.nonzero(got[k] != ref[k])[0]
         assert bad.size == 0, f"{k} differs at splits {bad[:10]}: got {got[k][bad[:10]]} ref {ref[k][bad[:10]]}"
     d = np.abs(got["discarded_weight"] - ref["discarded_weight"])
-    # Rounding differences accumulate through the truncating splits: the
-    # bound is DISC_ATOL over the 150 splits of the 16-qubit chi 32 circuit
-    # and grows linearly with the split index beyond that.
-    growth = np.maximum(1.0, np.arange(len(ref)) / 150.0)
-    tol = DISC_ATOL * np.maximum(1.0, np.abs(ref["discarded_weight"])) * growth
+    tol = DISC_ATOL * np.maximum(1.0, np.abs(ref["discarded_weight"]))
+    if drift is not None:
+        tol = tol + 10.0 * np.maximum.accumulate(drift)
     bad = np.nonzero(d > tol)[0]
     assert bad.size == 0, (f"discarded weight differs at splits {bad[:5]}: got {got['discarded_weight'][bad[:5]]} "
                            f"ref {ref['discarded_weight'][bad[:5]]}")
@@ -351,7 +368,7 @@ def test_exact_rule_circuit_parity_at_chi_96(cuda_ctx):
     g = C.gates_array(C.random_layers(18, 12, seed=7))
     m = W.run(18, 96, g, ctx=cuda_ctx, rule=W.SPLIT_RULE_EXACT)
     o = O.run(18, 96, g, rule=1)
-    assert_records_match(m.split_records(), o.records())
+    assert_records_match(m.split_records(), o.records(), drift=oracle_drift(18, 96, g, rule=1))
     a, b = m.amplitude_at_compact_zero(), o.amplitude_zero()
     assert rel_err(a, b) < AMP_RTOL, (a, b)
 
@@ -421,12 +438,13 @@ def test_batch_of_uneven_slices_matches_single_runs_and_oracle(cuda_ctx):
     bits differ) in split shapes, paths and kept chi exactly and in the
     amplitude within AMP_RTOL, and match its own oracle run: amplitude
     within AMP_RTOL, split shapes, paths and kept chi bit-exact over the
-    whole run, discarded weights within the per-split tolerance over the
-    first 500 splits.  The deepest slices (about 1000 truncating splits at
-    chi 32) drift from the oracle beyond that, exponentially, to a few 1e-9
-    relative in their last weights; the single-state path drifts the same
-    way, so that is rounding amplified by repeated truncation, not
-    batching."""
+    whole run, and discarded weights over every split within 1e-12 plus ten
+    times the oracle's own drift between its two SVDs.  The deepest slices
+    (about 1000 truncating splits at chi 32) carry rounding differences into
+    later truncations: the oracle's Golub-Kahan and Jacobi runs of the same
+    slice drift apart to ~5e-9 in the last weights, the size of the drift
+    between device and oracle (test_oracle_drift_under_a_change_of_svd pins
+    that on the CPU)."""
     slices = C.config2_slices(12, seed=99)
     for s in slices:  # keep the oracle side short
         s.chi = min(s.chi, 32)
@@ -453,4 +471,4 @@ def test_batch_of_uneven_slices_matches_single_runs_and_oracle(cuda_ctx):
         assert amp_err(amps[i], o.amplitude_zero(), s.n) < AMP_RTOL, (i, amps[i], o.amplitude_zero())
         for k in ("left_site", "rows", "cols", "ell", "path", "chi"):
             assert np.array_equal(recs[i][k], ref[k]), (i, k)
-        assert_records_match(recs[i][:500], ref[:500])
+        assert_records_match(recs[i], ref, drift=oracle_drift(s.n, s.chi, s.gates))

@@ -341,3 +341,31 @@ def test_call_sequence_folds_rotations_and_batches_layers():
     a = O.run(n, 16, g).amplitude_zero()
     b = O.run(n, 16, g, call_sequence=True).amplitude_zero()
     assert abs(a - b) < 1e-12
+
+
+def test_oracle_drift_under_a_change_of_svd():
+    """Two FP64 SVDs of the same matrices -- the oracle's Golub-Kahan (the
+    reference's primary, nalgebra's family) and its svd_guard.rs Jacobi as
+    primary -- agree to rounding on one split, but a long truncating run
+    carries the difference into every later cut.  On the deepest slice of the
+    batching test (43 qubits, 1008 splits at chi 32) the kept chi and paths
+    stay identical while the per-split discarded weights drift apart far
+    beyond 1e-12: the drift the device's Jacobi shows against the oracle on
+    such runs is rounding of this kind, and the GPU tests bound it by this
+    drift measured on the oracle itself."""
+    s = C.config2_slices(12, seed=99)[1]
+    chi = min(s.chi, 32)
+    runs = []
+    for primary in (0, 1):
+        O.set_primary_svd(primary)
+        try:
+            runs.append(O.run(s.n, chi, s.gates).records())
+        finally:
+            O.set_primary_svd(0)
+    a, b = runs
+    assert len(a) == len(b) > 1000
+    for k in ("left_site", "rows", "cols", "path", "chi"):
+        assert np.array_equal(a[k], b[k]), k
+    d = np.abs(a["discarded_weight"] - b["discarded_weight"])
+    assert d[:150].max() <= 1e-12  # early splits agree to the per-split tolerance
+    assert 1e-11 < d.max() < 1e-6  # the tail drifts, by rounding amplified through the cuts

@@ -8,10 +8,15 @@ working memory from one fixed array inside the library instead.
 
 The GPU test runs the state through the allocating path, copies its sites
 into a buffer that torch owns, and checks that the allocation-free entry
-point, called twice in a row through the C ABI (a larger state first, then
-a smaller one with other terms, so that anything left in the shared array
-by the first call would show), gives what wqc_mps_expectation_pauli gives,
-within the amplitude tolerance of the parity tests.
+point, called three times in a row through the C ABI, gives what
+wqc_mps_expectation_pauli gives, within the amplitude tolerance of the
+parity tests.  The first call is at bond 256 with six terms, more than the
+four that one launch holds at that bond, so the second launch of that call
+reuses the environment slots of the first; the later calls use smaller
+states and other terms.  Every launch clears the per-term results before it
+runs and each transfer-matrix step writes the environment entries it then
+reads, so what the calls check is the results clearing, the chunking and the
+size bookkeeping, not a full wipe of the array.
 
 The file name sorts last so that a run stopping at its first failure has run
 every other test before this one.
@@ -51,6 +56,9 @@ def test_noalloc_expectation_matches_allocating_entry_point_on_two_calls(cuda_ct
 
     stream = torch.cuda.current_stream().cuda_stream
     cases = []
+    gates = C.gates_array(C.ry_rz_brickwork(18, 18, seed=10))  # bonds up to 256
+    labels, coeffs = random_terms(18, 6, seed=9)  # two launches: 4 terms per launch at bond 256
+    cases.append((18, 256, gates, labels, coeffs, 256 * 2 * 256))
     gates = C.gates_array(C.random_layers(14, 10, seed=11))  # bonds up to 64
     labels, coeffs = C.zz_x_observable(14)
     labels, coeffs = labels + ["I" * 14], np.concatenate([coeffs, [1.0]])
@@ -72,7 +80,7 @@ def test_noalloc_expectation_matches_allocating_entry_point_on_two_calls(cuda_ct
         got = W.expectation_pauli_noalloc(buf.data_ptr(), stride, dims, labels, coeffs, stream=stream)
         assert abs(got - want) <= RTOL * max(1.0, abs(want)), (n, chi, got, want)
         assert abs(want) > 1e-3  # the comparison is not between two zeros
-    assert bonds[0] > bonds[1]  # the second call reads less of the array than the first wrote
+    assert bonds[0] == 256 and bonds[0] > bonds[1] > bonds[2]  # each call reads less than the one before wrote
 
 
 def test_noalloc_expectation_rejects_sizes_beyond_its_limits():
@@ -86,3 +94,11 @@ def test_noalloc_expectation_rejects_sizes_beyond_its_limits():
     with pytest.raises(W.WqcCudaError) as e:
         W.expectation_pauli_noalloc(0, 4, [2, 2, 1], ["ZZZ"], [1.0])  # site 1 is 2x2x2 = 8 > 4
     assert e.value.code == W.ERR_INVALID and "stride" in str(e.value)
+
+
+def test_noalloc_expectation_rejects_an_open_chain():
+    # The recursion's result is the expectation only when the last right bond
+    # is 1; a trailing bond above 1 is refused before any device work.
+    with pytest.raises(W.WqcCudaError) as e:
+        W.expectation_pauli_noalloc(0, 8, [2, 2, 2], ["ZZZ"], [1.0])
+    assert e.value.code == W.ERR_INVALID and "closed chain" in str(e.value)

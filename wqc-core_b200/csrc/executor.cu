@@ -27,10 +27,20 @@ using namespace wqc;
 namespace {
 
 thread_local std::string g_err;
+// Byte counts of the last WQC_ERR_OOM on this thread, for
+// EngineError::InsufficientMemory { required, available } (src/engine.rs:72).
+thread_local uint64_t g_oom_required = 0, g_oom_available = 0;
 
 wqc_status fail(wqc_status code, const std::string& msg) {
     g_err = msg;
     return code;
+}
+
+wqc_status fail_oom(uint64_t required, uint64_t available) {
+    g_oom_required = required;
+    g_oom_available = available;
+    return fail(WQC_ERR_OOM, "Insufficient memory: need " + std::to_string(required) + " bytes, only " +
+                                 std::to_string(available) + " bytes free on the device");
 }
 
 #define CUDA_TRY(expr)                                                                                    \
@@ -40,6 +50,7 @@ wqc_status fail(wqc_status code, const std::string& msg) {
     } while (0)
 
 constexpr int kMaxSweeps = 60;
+constexpr int kDenseMaxQubits = 28;  // 2^28 complex128 = 4 GiB on the host
 constexpr size_t kSmemLimit = 232448 - 1024;  // 227 KB opt-in per block, minus static shared memory
 
 struct Mat2 {
@@ -222,6 +233,21 @@ struct wqc_mps {
     std::vector<int> slice_last_wave;
     std::vector<cudaEvent_t> wave_done;
     cudaEvent_t call_start = nullptr;
+    // Cached environments of the trace feeders (single states): L_0..L_lvalid
+    // and R_rvalid..R_{n-1} are current; an operation on sites [a, b] leaves
+    // lvalid <= a and rvalid >= b.
+    double2* d_envL = nullptr;
+    double2* d_envR = nullptr;
+    int* d_targets = nullptr;     // targets of one wqc_mps_site_amplitudes_many call
+    double2* d_env_out = nullptr; // its (a0, a1) pairs
+    int lvalid = 0, rvalid = 0;
+    void touch(int a, int b) {
+        lvalid = std::min(lvalid, a);
+        rvalid = std::max(rvalid, b);
+    }
+    // Set by wqc_mps_upload_site: the bonds of the chain are checked once
+    // before the next call that computes on it.
+    bool uploaded = false;
     // accounting
     uint64_t bytes_now = 0, bytes_peak = 0;
     bool profiling = false;
@@ -241,8 +267,7 @@ wqc_status dmalloc(wqc_mps* m, void** p, size_t bytes) {
         cudaGetLastError();
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
-        return fail(WQC_ERR_OOM, "Insufficient memory: need " + std::to_string(bytes) + " bytes, only " +
-                                     std::to_string(fr) + " bytes free on the device");
+        return fail_oom(bytes, fr);
     }
     m->bytes_now += bytes;
     m->bytes_peak = std::max(m->bytes_peak, m->bytes_now);
@@ -273,8 +298,6 @@ void set_kernel_attributes() {
     }
     if (g_attr_err == cudaSuccess)
         g_attr_err = cudaFuncSetAttribute(amplitude_zero_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-    if (g_attr_err == cudaSuccess)
-        g_attr_err = cudaFuncSetAttribute(site_amplitudes_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
 }
 
 int round_up(int x, int q) { return ((x + q - 1) / q) * q; }
@@ -524,6 +547,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
     plan.first_seq = seq;
     for (size_t oi = 0; oi < ops.size(); ++oi) {
         const Op& o = ops[oi];
+        m->touch(o.site, o.two ? o.site + 1 : o.site);
         if (!o.two) {
             LevelBuild& lb = level(level_of[oi]);
             if (lb.oq_index.empty()) lb.oq_index.assign(m->n, -1);
@@ -783,8 +807,10 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
             count_launch(m, 1);
         }
         auto jacobi = [&](int mode, cudaStream_t on) -> wqc_status {
+            bool any = false;
             for (const Group& gr : w.groups) {
                 if (gr.mode != mode) continue;
+                any = true;
                 if (gr.C < 1)
                     return fail(WQC_ERR_INVALID, "two-site matrix too large for the cluster-resident Jacobi SVD");
                 Timed t(m, 0, on);
@@ -807,6 +833,12 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                     CUDA_TRY(launch_jacobi(m->fp32, gr.reg, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off, mode,
                                            kMaxSweeps, m->d_status, m->d_counters));
                 count_launch(m, 0);
+            }
+            if (any) {
+                Timed t(m, 4, on);
+                svd_probe_kernel<<<dim3(nj, 2), 256, 0, on>>>(d_jobs, m->d_state, m->d_slots, mode, m->fp32 ? 1 : 0,
+                                                               m->d_status);
+                count_launch(m, 4);
             }
             return WQC_OK;
         };
@@ -915,8 +947,36 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
     return WQC_OK;
 }
 
+// After uploads: every site's left bond must equal its left neighbour's right
+// bond, and each slice must start and end on a bond of 1.  An upload is one
+// site at a time, so the chain can only be checked once the caller computes
+// on it; a broken chain is refused instead of giving wrong results.
+wqc_status check_uploaded_chain(wqc_mps* m) {
+    if (!m->uploaded) return WQC_OK;
+    CUDA_TRY(cudaStreamSynchronize(m->stream));
+    std::vector<int> dl(m->n), dr(m->n);
+    CUDA_TRY(cudaMemcpy(dl.data(), m->d_dl, m->n * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(dr.data(), m->d_dr, m->n * sizeof(int), cudaMemcpyDeviceToHost));
+    for (size_t sl = 0; sl < m->seg_first.size(); ++sl) {
+        const int first = m->seg_first[sl], last = first + m->seg_n[sl] - 1;
+        for (int q = first; q <= last; ++q) {
+            const int want = q == first ? 1 : dr[q - 1];
+            if (dl[q] != want)
+                return fail(WQC_ERR_INVALID, "uploaded sites do not chain: site " + std::to_string(q - first) +
+                                                 " has left bond " + std::to_string(dl[q]) + ", expected " +
+                                                 std::to_string(want));
+        }
+        if (dr[last] != 1)
+            return fail(WQC_ERR_INVALID, "uploaded sites do not chain: the last site's right bond is " +
+                                             std::to_string(dr[last]) + ", expected 1");
+    }
+    m->uploaded = false;
+    return WQC_OK;
+}
+
 wqc_status run_ops(wqc_mps* m, const std::vector<Op>& ops) {
     if (*m->h_cancel) return fail(WQC_ERR_CANCELLED, "computation cancelled: the client has gone");
+    if (wqc_status s = check_uploaded_chain(m)) return s;
     Plan plan;
     build_plan(m, ops, plan);
     return launch_plan(m, plan);
@@ -970,6 +1030,11 @@ wqc_status record_error(wqc_status code, const std::string& msg) { return fail(c
 extern "C" {
 
 const char* wqc_cuda_last_error(void) { return g_err.c_str(); }
+
+void wqc_cuda_last_oom(uint64_t* required, uint64_t* available) {
+    if (required) *required = g_oom_required;
+    if (available) *available = g_oom_available;
+}
 
 wqc_status wqc_cuda_open(int device, wqc_cuda_ctx** out) {
     if (!out) return fail(WQC_ERR_INVALID, "null output pointer");
@@ -1098,9 +1163,7 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     const uint64_t need = site_bytes + uint64_t(m->nslots) * slot_bytes;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "cudaMemGetInfo"));
-    if (need > fr)
-        return bail(fail(WQC_ERR_OOM, "Insufficient memory: need " + std::to_string(need) + " bytes, only " +
-                                          std::to_string(fr) + " bytes free on the device"));
+    if (need > fr) return bail(fail_oom(need, fr));
     void* p = nullptr;
     if (wqc_status st = dmalloc(m, &p, site_bytes)) return bail(st);
     m->site_pool = static_cast<double2*>(p);
@@ -1123,6 +1186,17 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     m->d_small = static_cast<double2*>(p);
     m->d_counters = reinterpret_cast<unsigned long long*>(m->d_small + small - 4);
     if (cudaMemset(m->d_small, 0, small * sizeof(double2)) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "memset"));
+    if (ns.size() == 1) {  // the trace feeders' environment cache (single states)
+        const size_t env_bytes = 2 * size_t(n) * chi_cap * sizeof(double2) + size_t(n) * 2 * sizeof(double2) +
+                                 size_t(n) * sizeof(int);
+        if (wqc_status st = dmalloc(m, &p, env_bytes)) return bail(st);
+        m->d_envL = static_cast<double2*>(p);
+        m->d_envR = m->d_envL + size_t(n) * chi_cap;
+        m->d_env_out = m->d_envR + size_t(n) * chi_cap;
+        m->d_targets = reinterpret_cast<int*>(m->d_env_out + size_t(n) * 2);
+    }
+    m->lvalid = 0;
+    m->rvalid = n - 1;
     int* hc = nullptr;
     if (cudaHostAlloc(reinterpret_cast<void**>(&hc), sizeof(int), cudaHostAllocMapped) != cudaSuccess)
         return bail(fail(WQC_ERR_CUDA, "cudaHostAlloc"));
@@ -1204,6 +1278,8 @@ wqc_status wqc_mps_reset(wqc_mps* m) {
     if (wqc_status st = reset_sites(m)) return st;
     std::fill(m->ub.begin(), m->ub.end(), 1);
     m->rec_count = 0;
+    m->lvalid = 0;
+    m->rvalid = m->n - 1;
     return WQC_OK;
 }
 
@@ -1219,6 +1295,7 @@ void wqc_mps_destroy(wqc_mps* m) {
     dfree(m, m->d_small, 0);
     dfree(m, m->d_records, 0);
     dfree(m, m->d_seg, 0);
+    dfree(m, m->d_envL, 0);
     for (auto e : m->wave_done) cudaEventDestroy(e);
     if (m->call_start) cudaEventDestroy(m->call_start);
     dfree(m, m->d_stage.d, 0);
@@ -1295,6 +1372,7 @@ wqc_status wqc_batch_apply_gates(wqc_mps* m, const wqc_gate* gates, const uint32
 
 wqc_status wqc_batch_amplitudes(wqc_mps* m, double* out) {
     if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
+    if (wqc_status st = check_uploaded_chain(m)) return st;
     const int nseg = int(m->seg_first.size());
     amplitude_zero_kernel<<<nseg, 512, 2 * m->chi * sizeof(double2), m->stream>>>(m->dev, m->d_seg, m->d_small);
     count_launch(m, -1);
@@ -1460,6 +1538,7 @@ void wqc_mps_cancel(wqc_mps* m) {
 
 wqc_status wqc_mps_amplitude_zero(wqc_mps* m, double out[2]) {
     if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
+    if (wqc_status st = check_uploaded_chain(m)) return st;
     amplitude_zero_kernel<<<1, 512, 2 * m->chi * sizeof(double2), m->stream>>>(m->dev, m->d_seg, m->d_small);
     count_launch(m, -1);
     CUDA_TRY(cudaGetLastError());
@@ -1472,20 +1551,97 @@ wqc_status wqc_mps_amplitude_zero(wqc_mps* m, double out[2]) {
     return WQC_OK;
 }
 
+wqc_status wqc_mps_site_amplitudes_many(wqc_mps* m, const uint32_t* targets, uint32_t count, double* out) {
+    if (!m || (count && (!targets || !out))) return fail(WQC_ERR_INVALID, "null argument");
+    if (!m->d_envL) return fail(WQC_ERR_INVALID, "site amplitudes take a single state, not a batch");
+    if (count == 0) return WQC_OK;
+    if (count > uint32_t(m->n)) return fail(WQC_ERR_INVALID, "more targets than sites");
+    std::vector<int> t(count);
+    int lo = m->n, hi = -1;
+    for (uint32_t k = 0; k < count; ++k) {
+        if (targets[k] >= uint32_t(m->n)) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "target out of range");
+        t[k] = int(targets[k]);
+        lo = std::min(lo, t[k]);
+        hi = std::max(hi, t[k]);
+    }
+    if (wqc_status st = check_uploaded_chain(m)) return st;
+    const int lfrom = m->lvalid, lto = std::max(m->lvalid, hi);
+    const int rfrom = m->rvalid, rto = std::min(m->rvalid, lo);
+    CUDA_TRY(cudaMemcpyAsync(m->d_targets, t.data(), count * sizeof(int), cudaMemcpyHostToDevice, m->stream));
+    m->stats.h2d_bytes += count * sizeof(int);
+    site_envs_kernel<<<1, 512, 0, m->stream>>>(m->dev, m->d_envL, m->d_envR, lfrom, lto, rfrom, rto, m->d_targets,
+                                               int(count), m->d_env_out);
+    count_launch(m, -1);
+    CUDA_TRY(cudaGetLastError());
+    std::vector<double2> h(2 * size_t(count));
+    CUDA_TRY(cudaMemcpyAsync(h.data(), m->d_env_out, h.size() * sizeof(double2), cudaMemcpyDeviceToHost, m->stream));
+    m->stats.d2h_bytes += h.size() * sizeof(double2);
+    if (wqc_status s = sync_status(m)) return s;
+    m->lvalid = lto;
+    m->rvalid = rto;
+    for (size_t k = 0; k < h.size(); ++k) {
+        out[2 * k] = h[k].x;
+        out[2 * k + 1] = h[k].y;
+    }
+    return WQC_OK;
+}
+
 wqc_status wqc_mps_site_amplitudes(wqc_mps* m, uint32_t target, double out[4]) {
     if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
     if (target >= uint32_t(m->n)) return fail(WQC_ERR_QUBIT_OUT_OF_RANGE, "target out of range");
-    site_amplitudes_kernel<<<1, 512, 4 * m->chi * sizeof(double2), m->stream>>>(m->dev, int(target), m->d_small);
-    count_launch(m, -1);
-    CUDA_TRY(cudaGetLastError());
-    double2 h[2];
-    CUDA_TRY(cudaMemcpyAsync(h, m->d_small, 2 * sizeof(double2), cudaMemcpyDeviceToHost, m->stream));
+    return wqc_mps_site_amplitudes_many(m, &target, 1, out);
+}
+
+wqc_status wqc_mps_to_dense(wqc_mps* m, int32_t mode, double* out) {
+    if (!m || !out) return fail(WQC_ERR_INVALID, "null argument");
+    if (m->seg_first.size() != 1) return fail(WQC_ERR_INVALID, "the dense state takes a single state, not a batch");
+    if (mode != WQC_DENSE_TO_DENSE_STATE && mode != WQC_DENSE_STATEVECTOR)
+        return fail(WQC_ERR_INVALID, "unknown dense mode");
+    const int n = m->n;
+    if (mode == WQC_DENSE_STATEVECTOR && n > 20)  // mps.rs:217-221
+        return fail(WQC_ERR_INVALID, "full statevector projection requires qubit_count <= 20");
+    if (n > kDenseMaxQubits)
+        return fail(WQC_ERR_INVALID_QUBIT_COUNT, "the dense state is limited to " + std::to_string(kDenseMaxQubits) +
+                                                     " qubits");
+    if (wqc_status st = check_uploaded_chain(m)) return st;
     if (wqc_status s = sync_status(m)) return s;
-    out[0] = h[0].x;
-    out[1] = h[0].y;
-    out[2] = h[1].x;
-    out[3] = h[1].y;
-    return WQC_OK;
+    std::vector<int> dl(n), dr(n);
+    CUDA_TRY(cudaMemcpy(dl.data(), m->d_dl, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(dr.data(), m->d_dr, n * sizeof(int), cudaMemcpyDeviceToHost));
+    size_t most = 1;
+    for (int q = 0; q < n; ++q) {
+        if (dl[q] != (q ? dr[q - 1] : 1))  // mps.rs:229-234
+            return fail(WQC_ERR_INVALID, "MPS bond layout mismatch during statevector projection");
+        most = std::max(most, (size_t(2) << q) * size_t(dr[q]));
+    }
+    if (dr[n - 1] != 1) return fail(WQC_ERR_INVALID, "MPS bond layout mismatch during statevector projection");
+    void *d_a = nullptr, *d_b = nullptr;
+    if (wqc_status st = dmalloc(m, &d_a, most * sizeof(double2))) return st;
+    if (wqc_status st = dmalloc(m, &d_b, most * sizeof(double2))) {
+        dfree(m, d_a, most * sizeof(double2));
+        return st;
+    }
+    double2* cur = static_cast<double2*>(d_a);
+    double2* nxt = static_cast<double2*>(d_b);
+    const double2 one = cmake(1.0, 0.0);
+    cudaError_t e = cudaMemcpyAsync(cur, &one, sizeof(double2), cudaMemcpyHostToDevice, m->stream);
+    const int prune = mode == WQC_DENSE_TO_DENSE_STATE ? 1 : 0;
+    for (int q = 0; q < n && e == cudaSuccess; ++q) {
+        const long prefix = 1L << q;
+        const long total = 2 * prefix * dr[q];
+        const int grid = int(std::min<long>((total + 255) / 256, 8L * m->ctx->sm_count));
+        dense_step_kernel<<<grid, 256, 0, m->stream>>>(cur, m->site_ptr[q], dl[q], dr[q], prefix, prune, nxt);
+        count_launch(m, -1);
+        e = cudaGetLastError();
+        std::swap(cur, nxt);
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, cur, (size_t(1) << n) * sizeof(double2), cudaMemcpyDeviceToHost, m->stream);
+    m->stats.d2h_bytes += (size_t(1) << n) * sizeof(double2);
+    wqc_status rc = e == cudaSuccess ? sync_status(m) : fail(WQC_ERR_CUDA, cudaGetErrorString(e));
+    dfree(m, d_a, most * sizeof(double2));
+    dfree(m, d_b, most * sizeof(double2));
+    return rc;
 }
 
 wqc_status wqc_mps_bond_dims(wqc_mps* m, uint32_t* out) {
@@ -1525,6 +1681,8 @@ wqc_status wqc_mps_upload_site(wqc_mps* m, uint32_t site, uint32_t l, uint32_t r
     CUDA_TRY(cudaMemcpy(m->d_dr + site, &ir, sizeof(int), cudaMemcpyHostToDevice));
     if (site > 0) m->ub[site - 1] = std::max(m->ub[site - 1], il);
     if (int(site) + 1 < m->n) m->ub[site] = std::max(m->ub[site], ir);
+    m->uploaded = true;
+    m->touch(int(site), int(site));
     return WQC_OK;
 }
 
@@ -1613,6 +1771,7 @@ wqc_status wqc_mps_sample(wqc_mps* m, const uint32_t* qubits, uint32_t count, ui
         bitpos[qubits[j]] = int(j);
     }
     if (shots == 0) return WQC_OK;
+    if (wqc_status s = check_uploaded_chain(m)) return s;
     if (wqc_status s = sync_status(m)) return s;
     const int n = m->n;
     std::vector<int> dl(n), dr(n);
@@ -1692,6 +1851,7 @@ wqc_status wqc_mps_expectation_pauli(wqc_mps* m, const char* labels, const doubl
         out[0] = out[1] = 0;
         return WQC_OK;
     }
+    if (wqc_status st = check_uploaded_chain(m)) return st;
     const size_t E = size_t(m->chi) * m->chi;
     const size_t scratch = size_t(nterms) * 4 * E * sizeof(double2);
     void* d_lab = nullptr;

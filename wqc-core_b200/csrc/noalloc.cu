@@ -162,6 +162,12 @@ extern "C" wqc_status wqc_expectation_pauli_noalloc(const double* sites, uint64_
                                                      std::to_string(site_stride));
         env_cap = std::max(env_cap, int(r));
     }
+    // The transfer-matrix recursion ends on the right environment's (0, 0)
+    // entry, which is the expectation only for a closed chain.
+    if (bond_dims[qubit_count - 1] != 1)
+        return record_error(WQC_ERR_INVALID, "the last site's right bond is " +
+                                                 std::to_string(bond_dims[qubit_count - 1]) +
+                                                 "; the allocation-free expectation needs a closed chain (1)");
     for (size_t i = 0; i < size_t(nterms) * qubit_count; ++i) {
         const char ch = labels[i];
         if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z')
@@ -188,6 +194,14 @@ extern "C" wqc_status wqc_expectation_pauli_noalloc(const double* sites, uint64_
     if (wqc_status s = scratch_address(device, &scratch)) return s;
 
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Every call waits for its results on the host (cudaStreamSynchronize
+    // below), which a stream under capture does not allow.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return cuda_fail("cudaStreamIsCapturing", e);
+    if (cap != cudaStreamCaptureStatusNone)
+        return record_error(WQC_ERR_INVALID, "the allocation-free expectation is synchronous and cannot be called "
+                                             "while its stream is being captured");
     const size_t per_term = 4 * size_t(env_cap) * env_cap * sizeof(double2);
     const int chunk = int(std::min<size_t>(kNaMaxTermsPerLaunch, kNaEnvBytes / per_term));
     int dims[kNaMaxQubits];

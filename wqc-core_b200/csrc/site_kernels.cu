@@ -73,83 +73,117 @@ __global__ void __launch_bounds__(512) amplitude_zero_kernel(DeviceMps mps, cons
     if (threadIdx.x == 0) out[blockIdx.x] = len > 0 ? v[0] : cmake(0, 0);
 }
 
-// Trace feeders (mps.rs:679-740): environments with the all-ones physical
-// vector on both sides of `target`, then (a0, a1).
-__global__ void __launch_bounds__(512) site_amplitudes_kernel(DeviceMps mps, int target, double2* out) {
-    extern __shared__ double2 buf[];  // 4 * chi_max
-    double2* le = buf;
-    double2* tmp = buf + mps.chi_max;
-    double2* re = buf + 2 * mps.chi_max;
-    double2* tmp2 = buf + 3 * mps.chi_max;
+// Trace feeders (mps.rs:679-740), incremental and batched.  The left
+// environment of site i, L_i (length dl[i]), and the right environment,
+// R_i (length dr[i]), contract every site left (right) of i with the
+// all-ones physical vector; they stay cached in envL / envR (chi_max
+// entries per site) between calls.  The host knows which sites its
+// operations touched since the last call, so it passes the ranges still to
+// compute: L_{lfrom+1} .. L_{lto} from L_{lfrom} (L_0 = [1] is written when
+// lfrom == 0) and R_{rfrom-1} .. R_{rto} from R_{rfrom} (R_{n-1} = [1] when
+// rfrom == n-1).  Then, for every target t, a_s = sum_{a,b} L_t[a]
+// site_t[a, s, b] R_t[b] (out[2k], out[2k+1] for targets[k]).  One CTA: each
+// environment step needs the previous one.
+__global__ void __launch_bounds__(512) site_envs_kernel(DeviceMps mps, double2* envL, double2* envR, int lfrom,
+                                                        int lto, int rfrom, int rto, const int* targets, int count,
+                                                        double2* out) {
+    const int cap = mps.chi_max;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     __shared__ double2 red[2][512 / 32];
-    int llen = 1, rlen = 1;
-    if (threadIdx.x == 0) {
-        le[0] = cmake(1.0, 0.0);
-        re[0] = cmake(1.0, 0.0);
-    }
+    if (lfrom == 0 && tid == 0) envL[0] = cmake(1.0, 0.0);
+    if (rfrom == mps.n - 1 && tid == 0) envR[size_t(mps.n - 1) * cap] = cmake(1.0, 0.0);
     __syncthreads();
-    for (int i = 0; i < target; ++i) {
+    for (int i = lfrom; i < lto; ++i) {
         const int l = mps.dl[i], r = mps.dr[i];
-        const double2* s = mps.site[i];
-        const int la = min(l, llen);
-        for (int b = threadIdx.x; b < r; b += blockDim.x) {
+        const int len = i == 0 ? 1 : mps.dr[i - 1];
+        const double2* site = mps.site[i];
+        const double2* cur = envL + size_t(i) * cap;
+        double2* nxt = envL + size_t(i + 1) * cap;
+        const int la = min(l, len);
+        for (int b = tid; b < r; b += blockDim.x) {
             double2 acc = cmake(0, 0);
             for (int a = 0; a < la; ++a)
-                for (int p = 0; p < 2; ++p) cfma(acc, le[a], s[(size_t(a) * 2 + p) * r + b]);
-            tmp[b] = acc;
+                for (int p = 0; p < 2; ++p) cfma(acc, cur[a], site[(size_t(a) * 2 + p) * r + b]);
+            nxt[b] = acc;
         }
         __syncthreads();
-        for (int b = threadIdx.x; b < r; b += blockDim.x) le[b] = tmp[b];
-        __syncthreads();
-        llen = r;
     }
-    if (target + 1 < mps.n) {
-        for (int i = mps.n - 1; i > target; --i) {
-            const int l = mps.dl[i], r = mps.dr[i];
-            const double2* s = mps.site[i];
-            const int rb = min(r, rlen);
-            for (int a = threadIdx.x; a < l; a += blockDim.x) {
-                double2 acc = cmake(0, 0);
-                for (int b = 0; b < rb; ++b)
-                    for (int p = 0; p < 2; ++p) cfma(acc, re[b], s[(size_t(a) * 2 + p) * r + b]);
-                tmp2[a] = acc;
+    for (int i = rfrom; i > rto; --i) {
+        const int l = mps.dl[i], r = mps.dr[i];
+        const int len = i == mps.n - 1 ? 1 : mps.dl[i + 1];
+        const double2* site = mps.site[i];
+        const double2* cur = envR + size_t(i) * cap;
+        double2* nxt = envR + size_t(i - 1) * cap;
+        const int rb = min(r, len);
+        for (int a = tid; a < l; a += blockDim.x) {
+            double2 acc = cmake(0, 0);
+            for (int b = 0; b < rb; ++b)
+                for (int p = 0; p < 2; ++p) cfma(acc, cur[b], site[(size_t(a) * 2 + p) * r + b]);
+            nxt[a] = acc;
+        }
+        __syncthreads();
+    }
+    for (int k = 0; k < count; ++k) {
+        const int t = targets[k];
+        const int l = mps.dl[t], r = mps.dr[t];
+        const int llen = t == 0 ? 1 : mps.dr[t - 1];
+        const int rlen = t == mps.n - 1 ? 1 : mps.dl[t + 1];
+        const double2* site = mps.site[t];
+        const double2* le = envL + size_t(t) * cap;
+        const double2* re = envR + size_t(t) * cap;
+        double2 a0 = cmake(0, 0), a1 = cmake(0, 0);
+        for (long e = tid; e < long(llen) * r; e += blockDim.x) {
+            const int a = int(e / r), b = int(e % r);
+            if (a >= l) continue;
+            const double2 rv = b < rlen ? re[b] : cmake(1.0, 0.0);
+            cfma(a0, le[a], cmul(site[(size_t(a) * 2) * r + b], rv));
+            cfma(a1, le[a], cmul(site[(size_t(a) * 2 + 1) * r + b], rv));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            a0.x += __shfl_xor_sync(0xffffffffu, a0.x, o);
+            a0.y += __shfl_xor_sync(0xffffffffu, a0.y, o);
+            a1.x += __shfl_xor_sync(0xffffffffu, a1.x, o);
+            a1.y += __shfl_xor_sync(0xffffffffu, a1.y, o);
+        }
+        if (lane == 0) {
+            red[0][wid] = a0;
+            red[1][wid] = a1;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double2 s0 = cmake(0, 0), s1 = cmake(0, 0);
+            for (int w = 0; w < nw; ++w) {
+                s0 = cadd(s0, red[0][w]);
+                s1 = cadd(s1, red[1][w]);
             }
-            __syncthreads();
-            for (int a = threadIdx.x; a < l; a += blockDim.x) re[a] = tmp2[a];
-            __syncthreads();
-            rlen = l;
+            out[2 * k] = s0;
+            out[2 * k + 1] = s1;
         }
+        __syncthreads();
     }
-    const int l = mps.dl[target], r = mps.dr[target];
-    const double2* s = mps.site[target];
-    double2 a0 = cmake(0, 0), a1 = cmake(0, 0);
-    for (long e = threadIdx.x; e < long(llen) * r; e += blockDim.x) {
-        const int a = int(e / r), b = int(e % r);
-        if (a >= l) continue;
-        const double2 rv = b < rlen ? re[b] : cmake(1.0, 0.0);
-        cfma(a0, le[a], cmul(s[(size_t(a) * 2) * r + b], rv));
-        cfma(a1, le[a], cmul(s[(size_t(a) * 2 + 1) * r + b], rv));
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        a0.x += __shfl_xor_sync(0xffffffffu, a0.x, o);
-        a0.y += __shfl_xor_sync(0xffffffffu, a0.y, o);
-        a1.x += __shfl_xor_sync(0xffffffffu, a1.x, o);
-        a1.y += __shfl_xor_sync(0xffffffffu, a1.y, o);
-    }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) {
-        red[0][wid] = a0;
-        red[1][wid] = a1;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double2 s0 = cmake(0, 0), s1 = cmake(0, 0);
-        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
-            s0 = cadd(s0, red[0][w]);
-            s1 = cadd(s1, red[1][w]);
+}
+
+// The dense state (mps.rs:742-780 to_dense_state, 215-260
+// contract_to_statevector), one site per launch: cur holds the contraction of
+// sites 0..q-1 as [prefix][a] (prefix < 2^q, a < l); nxt gets
+// [s 2^q + prefix][b] = sum_a cur[prefix][a] site[a, s, b].  Basis bit q is
+// qubit q.  With prune, site entries with |x|^2 < 1e-30 count as zero, as
+// to_dense_state's recursion skips them.
+__global__ void __launch_bounds__(256) dense_step_kernel(const double2* cur, const double2* site, int l, int r,
+                                                         long prefix, int prune, double2* nxt) {
+    const long total = 2 * prefix * r;
+    for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += long(gridDim.x) * blockDim.x) {
+        const long basis = e / r;
+        const int b = int(e % r);
+        const int s = int(basis / prefix);
+        const long pre = basis % prefix;
+        double2 acc = cmake(0, 0);
+        for (int a = 0; a < l; ++a) {
+            const double2 x = site[(size_t(a) * 2 + s) * r + b];
+            if (prune && cnorm2(x) < 1e-30) continue;
+            cfma(acc, cur[pre * l + a], x);
         }
-        out[0] = s0;
-        out[1] = s1;
+        nxt[e] = acc;
     }
 }
 

@@ -1342,6 +1342,105 @@ __global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(con
 }
 
 // ---------------------------------------------------------------------------
+// The probe-vector half of the reference's factorisation check
+// (svd_reproduces, svd_guard.rs:256-283): U Sigma V^H x must reproduce X x
+// for the two fixed probes x_j = (sin t, cos t), t = (j + 1) (0.754877666 +
+// p 0.56984029), to 1e-9 ||X||_F ||x|| + 1e-14.  The Jacobi keeps W = X V =
+// U Sigma and no V, and U Sigma V^H x = U U^H X x over the columns with
+// sigma > 0, so with y = X x the rebuilt vector is W diag(1/sigma^2) W^H y:
+// it equals y only when W's columns are orthogonal and span X's range.
+// Columns at the storage's rounding level (the Jacobi's noise floor) are
+// left out: their direction is noise and they carry less than the tolerance.
+// One CTA per (job, probe); a failure sets the same status as the Frobenius
+// check ("failed its check").
+// ---------------------------------------------------------------------------
+constexpr int kProbeMax = 512;
+
+__global__ void __launch_bounds__(256) svd_probe_kernel(const SplitJob* jobs, const SplitState* st,
+                                                        const SlotBuffers* slots, int mode, int fp32, int* status) {
+    const int j = blockIdx.x;
+    const int probe = blockIdx.y;
+    const SplitState S = st[j];
+    if (!jacobi_active(S, mode)) return;
+    const SplitJob& J = jobs[j];
+    const SlotBuffers Bf = slots[J.slot];
+    const double2* src;
+    int sr, sc, ld, rows_of_src;
+    jacobi_task(J, S, Bf, mode, src, sr, sc, ld, rows_of_src);
+    const int M = rows_of_src ? sc : sr;
+    const int N = rows_of_src ? sr : sc;
+    if (M > kProbeMax || N > kProbeMax) {
+        if (threadIdx.x == 0) atomicOr(status, kStatusBadShape);
+        return;
+    }
+    __shared__ double2 xs[kProbeMax], ys[kProbeMax], zs[kProbeMax];
+    __shared__ double red[8];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    const double step = 0.754877666 + double(probe) * 0.56984029;
+    double fro2_part = 0;
+    for (int c = tid; c < N; c += blockDim.x) {
+        double sn, cs;
+        sincos(double(c + 1) * step, &sn, &cs);
+        xs[c] = cmake(sn, cs);
+        const double sg = Bf.sigma[c];
+        fro2_part += sg * sg;
+    }
+    for (int o = 16; o > 0; o >>= 1) fro2_part += __shfl_xor_sync(0xffffffffu, fro2_part, o);
+    if (lane == 0) red[wid] = fro2_part;
+    __syncthreads();
+    double fro2 = 0;
+    for (int w = 0; w < nw; ++w) fro2 += red[w];
+    const double floor2 = (fp32 ? 1e-12 : 1e-30) * fro2;
+    // y = X x, one warp per row.
+    for (int i = wid; i < M; i += nw) {
+        double2 acc = cmake(0, 0);
+        for (int c = lane; c < N; c += 32) {
+            const double2 a = rows_of_src ? cconj(src[size_t(c) * ld + i]) : src[size_t(i) * ld + c];
+            cfma(acc, a, xs[c]);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        }
+        if (lane == 0) ys[i] = acc;
+    }
+    __syncthreads();
+    // z = diag(1/sigma^2) W^H y, one warp per column.
+    for (int c = wid; c < N; c += nw) {
+        const double sg = Bf.sigma[c];
+        double2 acc = cmake(0, 0);
+        if (sg * sg > floor2) {
+            const double2* wc = Bf.w + size_t(c) * M;
+            for (int i = lane; i < M; i += 32) cfma_conj(acc, wc[i], ys[i]);
+            for (int o = 16; o > 0; o >>= 1) {
+                acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+                acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+            }
+            acc = cscale(acc, 1.0 / (sg * sg));
+        }
+        if (lane == 0) zs[c] = acc;
+    }
+    __syncthreads();
+    // |y - W z|^2, one thread per row.
+    double err2 = 0;
+    for (int i = tid; i < M; i += blockDim.x) {
+        double2 r = cmake(0, 0);
+        for (int c = 0; c < N; ++c) cfma(r, Bf.w[size_t(c) * M + i], zs[c]);
+        err2 += cnorm2(csub(ys[i], r));
+    }
+    for (int o = 16; o > 0; o >>= 1) err2 += __shfl_xor_sync(0xffffffffu, err2, o);
+    __syncthreads();
+    if (lane == 0) red[wid] = err2;
+    __syncthreads();
+    if (tid == 0) {
+        double e2 = 0;
+        for (int w = 0; w < nw; ++w) e2 += red[w];
+        const double tol = fp32 ? 1e-4 : 1e-9;  // the Frobenius check's tolerance of each form
+        if (!(sqrt(e2) <= tol * sqrt(fro2) * sqrt(double(N)) + 1e-14)) atomicOr(status, kStatusSvdCheck);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // finalize: stable descending sort, truncation rule, ambiguity test,
 // discarded weight and the split record.
 // ---------------------------------------------------------------------------

@@ -77,6 +77,9 @@ inline int jacobi_staged_b(int M, int N, size_t elem, size_t smem_limit, size_t*
 }
 // Elements (double2) of the `gs` workspace for two-site matrices up to R x R.
 inline size_t jacobi_staged_elems(int R) { return size_t(R + 32) * size_t(R); }
+// Probe-vector factorisation check of every active Jacobi task (grid: jobs x 2).
+__global__ void svd_probe_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots, int mode,
+                                 int fp32, int* status);
 // noise_rel: singular values below noise_rel * (largest) count as zero (0 in
 // the plain form; the precision form's FP32 rounding level).
 __global__ void finalize_kernel(const SplitJob* jobs, SplitState* st, const SlotBuffers* slots, int mode,
@@ -96,7 +99,10 @@ struct OneQubitOp {
 __global__ void apply_1q_kernel(const OneQubitOp* ops, const double2* mats, DeviceMps mps);
 __global__ void amplitude_zero_kernel(DeviceMps mps, const int* seg, double2* out);
 __global__ void reset_sites_kernel(DeviceMps mps);
-__global__ void site_amplitudes_kernel(DeviceMps mps, int target, double2* out);
+__global__ void site_envs_kernel(DeviceMps mps, double2* envL, double2* envR, int lfrom, int lto, int rfrom, int rto,
+                                 const int* targets, int count, double2* out);
+__global__ void dense_step_kernel(const double2* cur, const double2* site, int l, int r, long prefix, int prune,
+                                  double2* nxt);
 __global__ void pauli_expectation_kernel(DeviceMps mps, const char* labels, int nterms, double2* scratch,
                                          int env_cap, double2* out);
 __global__ void overlap_half_kernel(const double2* env, int kl, int bl, const double2* ket, int kr, double2* tmp);

@@ -49,16 +49,21 @@ EXPORTS = (
     "wqc_mps_reset_stats", "wqc_mps_stream", "wqc_schedule_gates", "wqc_mps_reset", "wqc_mps_debug_workspace",
     "wqc_batch_create", "wqc_batch_apply_gates", "wqc_batch_amplitudes", "wqc_batch_slice_times",
     "wqc_expectation_pauli_noalloc", "wqc_batch_expectation_pauli", "wqc_mps_sample",
-    "wqc_mps_overlap",
+    "wqc_mps_overlap", "wqc_cuda_last_oom", "wqc_mps_site_amplitudes_many", "wqc_mps_to_dense",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
 
 
 class WqcCudaError(RuntimeError):
-    def __init__(self, code: int, message: str):
+    """A failing C ABI call.  For WQC_ERR_OOM, ``required`` and ``available``
+    carry the byte counts of EngineError::InsufficientMemory (src/engine.rs:72)."""
+
+    def __init__(self, code: int, message: str, required: int = 0, available: int = 0):
         super().__init__(f"[{code}] {message}")
         self.code = code
+        self.required = required
+        self.available = available
 
 
 class KernelStats(ctypes.Structure):
@@ -90,6 +95,8 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         P, I, U32, U8, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint8, ctypes.POINTER(ctypes.c_double)
         L.wqc_cuda_last_error.restype = ctypes.c_char_p
+        L.wqc_cuda_last_oom.argtypes = [ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+        L.wqc_cuda_last_oom.restype = None
         L.wqc_cuda_open.argtypes = [I, ctypes.POINTER(P)]
         L.wqc_cuda_close.argtypes = [P]
         L.wqc_cuda_device_info.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
@@ -111,6 +118,8 @@ def lib():
         L.wqc_mps_cancel.restype = None
         L.wqc_mps_amplitude_zero.argtypes = [P, D]
         L.wqc_mps_site_amplitudes.argtypes = [P, U32, D]
+        L.wqc_mps_site_amplitudes_many.argtypes = [P, ctypes.POINTER(U32), U32, D]
+        L.wqc_mps_to_dense.argtypes = [P, ctypes.c_int32, D]
         L.wqc_mps_bond_dims.argtypes = [P, ctypes.POINTER(U32)]
         L.wqc_mps_download_site.argtypes = [P, U32, ctypes.POINTER(U32), ctypes.POINTER(U32), D]
         L.wqc_mps_upload_site.argtypes = [P, U32, U32, U32, D]
@@ -146,9 +155,19 @@ def lib():
     return _LIB
 
 
+def last_oom():
+    """(required, available) bytes of the last WQC_ERR_OOM on this thread."""
+    req, avail = ctypes.c_uint64(), ctypes.c_uint64()
+    lib().wqc_cuda_last_oom(ctypes.byref(req), ctypes.byref(avail))
+    return req.value, avail.value
+
+
 def _check(rc: int) -> None:
     if rc != OK:
-        raise WqcCudaError(rc, lib().wqc_cuda_last_error().decode())
+        msg = lib().wqc_cuda_last_error().decode()
+        if rc == ERR_OOM:
+            raise WqcCudaError(rc, msg, *last_oom())
+        raise WqcCudaError(rc, msg)
 
 
 def _dp(a: np.ndarray):
@@ -157,6 +176,21 @@ def _dp(a: np.ndarray):
 
 def _c128(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def _pauli_args(labels, coeffs, width: int):
+    """Labels joined for the C ABI and coefficients as complex128, after the
+    checks the C side cannot make: it reads nterms * width label bytes and
+    2 * nterms doubles, so a short label or a short coefficient array would
+    be read past its end."""
+    labels = list(labels)
+    c = _c128(coeffs).reshape(-1)
+    if len(c) != len(labels):
+        raise ValueError(f"{len(labels)} Pauli labels but {len(c)} coefficients")
+    for i, lab in enumerate(labels):
+        if len(lab) != width:
+            raise ValueError(f"Pauli label {i} has {len(lab)} characters; the register has {width} qubits")
+    return "".join(labels).encode(), c
 
 
 class Context:
@@ -179,6 +213,19 @@ class Context:
         tot, fr, sm = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int32()
         _check(lib().wqc_cuda_device_info(self._h, ctypes.byref(tot), ctypes.byref(fr), ctypes.byref(sm)))
         return {"total_bytes": tot.value, "free_bytes": fr.value, "sm_count": sm.value}
+
+
+def probe_tn_engine_status(requested: str = "cuda") -> dict:
+    """The backend probe of src/tn/engine_status.rs:40-84 for a `cuda`
+    request: active "cuda" when a context opens, else "unavailable" with the
+    reason.  There is no CPU fallback, so a state cannot be built then."""
+    if requested != "cuda":
+        return {"requested": requested, "active": requested, "note": None}
+    try:
+        Context.shared()
+    except WqcCudaError as e:
+        return {"requested": "cuda", "active": "unavailable", "note": f"CUDA device not found: {e}"}
+    return {"requested": "cuda", "active": "cuda", "note": None}
 
 
 def schedule(n: int, gates: np.ndarray):
@@ -255,7 +302,10 @@ class CudaMps:
 
     # sweep-tree hooks (mps.rs:621-655)
     def apply_unary_at(self, site: int, gate) -> None:
-        self.apply_gate((gate[0], site, 0, 0, gate[-1] if len(gate) > 2 else 0.0))
+        """gate: (kind, angle) or a C.g1 tuple (kind, qubit, 0, 0, angle); the
+        qubit is replaced by `site` (the tree's wire-to-site mapping)."""
+        angle = gate[1] if len(gate) == 2 else (gate[-1] if len(gate) > 2 else 0.0)
+        self.apply_gate((gate[0], site, 0, 0, float(angle)))
 
     def apply_tdg_at(self, site: int) -> None:
         r = 0.70710678118654752440
@@ -293,6 +343,14 @@ class CudaMps:
         _check(lib().wqc_mps_site_amplitudes(self._h, target, _dp(out)))
         return complex(out[0], out[1]), complex(out[2], out[3])
 
+    def site_amplitudes_many(self, targets) -> np.ndarray:
+        """(a0, a1) of every target in one call: shape (len(targets), 2)."""
+        t = np.ascontiguousarray(targets, dtype=np.uint32)
+        out = np.zeros((len(t), 2), dtype=np.complex128)
+        _check(lib().wqc_mps_site_amplitudes_many(self._h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                                  len(t), _dp(out.view(np.float64))))
+        return out
+
     def control_probability(self, control: int) -> float:
         _, a1 = self.site_amplitudes(control)
         return a1.real * a1.real + a1.imag * a1.imag
@@ -314,18 +372,20 @@ class CudaMps:
         _check(lib().wqc_mps_upload_site(self._h, i, t.shape[0], t.shape[2], _dp(t.view(np.float64))))
 
     def to_dense_state(self) -> np.ndarray:
-        """Dense 2^N vector from the downloaded sites (mps.rs:742-780 layout:
-        qubit q is bit q); for tests and small registers."""
-        state = np.ones((1, 1), dtype=np.complex128)  # [basis, bond]
-        for q in range(self.n):
-            s = self.site(q)
-            nxt = np.einsum("xa,asb->sxb", state, s)  # basis bit q is the new slowest index
-            state = nxt.reshape(-1, s.shape[2])
-        return state[:, 0]
+        """to_dense_state (mps.rs:742-780) on the device: the 2^N vector,
+        qubit q is bit q, site entries with |x|^2 < 1e-30 skipped."""
+        out = np.zeros(1 << self.n, dtype=np.complex128)
+        _check(lib().wqc_mps_to_dense(self._h, 0, _dp(out.view(np.float64))))
+        return out
+
+    def contract_to_statevector(self) -> np.ndarray:
+        """contract_to_statevector (mps.rs:215-260) on the device (N <= 20)."""
+        out = np.zeros(1 << min(self.n, 20), dtype=np.complex128)
+        _check(lib().wqc_mps_to_dense(self._h, 1, _dp(out.view(np.float64))))
+        return out
 
     def expectation(self, labels, coeffs) -> complex:
-        joined = "".join(labels).encode()
-        c = _c128(coeffs)
+        joined, c = _pauli_args(labels, coeffs, self.n)
         out = np.zeros(2)
         _check(lib().wqc_mps_expectation_pauli(self._h, joined, _dp(c.view(np.float64)), len(labels), _dp(out)))
         return complex(out[0], out[1])
@@ -422,8 +482,7 @@ def expectation_pauli_noalloc(sites_ptr: int, site_stride: int, bond_dims, label
     len(bond_dims) sites of site_stride complex128 values each, site q laid
     out [l][2][r]; stream is a cudaStream_t handle (0 = legacy default)."""
     dims = np.ascontiguousarray(bond_dims, dtype=np.uint32)
-    joined = "".join(labels).encode()
-    c = _c128(coeffs)
+    joined, c = _pauli_args(labels, coeffs, len(dims))
     out = np.zeros(2)
     _check(lib().wqc_expectation_pauli_noalloc(sites_ptr or None, site_stride,
                                                dims.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(dims),
@@ -468,8 +527,7 @@ class CudaBatch(CudaMps):
 
     def expectations(self, labels, coeffs) -> np.ndarray:
         """The Pauli sum on every slice (wqc_batch_expectation_pauli)."""
-        joined = "".join(labels).encode()
-        c = _c128(coeffs)
+        joined, c = _pauli_args(labels, coeffs, int(self.qubits[0]) if len(self.qubits) else 0)
         out = np.zeros(len(self.qubits), dtype=np.complex128)
         _check(lib().wqc_batch_expectation_pauli(self._h, joined, _dp(c.view(np.float64)), len(labels),
                                                  _dp(out.view(np.float64))))
