@@ -295,6 +295,38 @@ WQC_API wqc_status wqc_expectation_pauli_noalloc(const double* sites, uint64_t s
                                                  uint32_t qubit_count, const char* labels, const double* coeffs,
                                                  uint32_t nterms, void* stream, double out[2]);
 
+/* Differentiation form: the adjoint (reverse-mode) gradient of a Pauli-sum
+ * observable f = sum_t Re(c_t) <psi|P_t|psi> (compute_expectations,
+ * src/expectation.rs:98-200) with respect to the angle of every RX/RY/RZ
+ * gate, through the reference's truncated forward path: one-qubit gates,
+ * SWAP-routed two-site applies and the truncated SVD split with sqrt(S)
+ * absorbed on both sides (mps.rs:333-429, 1124-1171).  The reference has no
+ * reverse mode; this pair is the forward/backward op a Rust caller binds.
+ *
+ * wqc_adjoint_forward resets `mps` to |0...0>, runs `gates` on it and keeps
+ * a checkpoint of the sites at each gate index in `checkpoints` (for
+ * instance the first gate of every second layer) and at the end; the state
+ * then holds the circuit's output.  Every split takes the exact SVD (the
+ * range finder's rank-48 test matrix has no meaningful derivative); single
+ * states in the plain FP64 form only.
+ *
+ * wqc_adjoint_backward: value[0] = f, value[1] = sum_t Im(c_t) <P_t>;
+ * grad[i] = d f / d angle of gate i (0 for gates without an angle).  The
+ * sweep restores each segment from its checkpoint, recomputes it and runs
+ * it in reverse: a split's reverse is the complex SVD's reverse mode with
+ * the cotangents of the dropped singular vectors zero (the truncation term)
+ * and 1/(s_j^2 - s_i^2) Lorentzian-broadened for near-degenerate values.
+ * This is the derivative of the truncated map, which differs from a
+ * parameter-shift estimate by the truncation's own effect.  `adj` can be
+ * swept again with other observables; the state holds the forward's output
+ * afterwards. */
+typedef struct wqc_adjoint wqc_adjoint;
+WQC_API wqc_status wqc_adjoint_forward(wqc_mps* mps, const wqc_gate* gates, uint32_t count,
+                                       const uint32_t* checkpoints, uint32_t ncheckpoints, wqc_adjoint** out);
+WQC_API wqc_status wqc_adjoint_backward(wqc_adjoint* adj, const char* labels, const double* coeffs, uint32_t nterms,
+                                        double value[2], double* grad);
+WQC_API void wqc_adjoint_destroy(wqc_adjoint* adj);
+
 /* Diagnostics: copy one split-workspace buffer of `slot` (the last wave's
  * job in that slot) to host memory, at most `bytes`.  which: 0 theta
  * (rows x cols, row-major), 1 Omega, 2 A*Omega, 3 A^H*(A*Omega), 4 Y then

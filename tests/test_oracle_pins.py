@@ -369,3 +369,23 @@ def test_oracle_drift_under_a_change_of_svd():
     d = np.abs(a["discarded_weight"] - b["discarded_weight"])
     assert d[:150].max() <= 1e-12  # early splits agree to the per-split tolerance
     assert 1e-11 < d.max() < 1e-6  # the tail drifts, by rounding amplified through the cuts
+
+
+def test_numpy_adjoint_matches_central_differences():
+    """oracle/adjoint.py, the checker of the device adjoint: its forward is
+    the oracle's (same value) and its reverse sweep through truncating
+    splits matches central differences of its own forward to 1e-8."""
+    import adjoint as A
+
+    for n, layers, chi in ((6, 3, 3), (8, 2, 64)):
+        gates, pidx, _ = C.hea_ansatz(n, layers, seed=5)
+        labels, coeffs = C.zz_x_observable(n)
+        f, g = A.gradient(n, chi, gates, labels, coeffs)
+        assert abs(f - O.run(n, chi, gates).expectation(labels, coeffs).real) <= 1e-12
+        h = 1e-5
+        for i in np.nonzero(pidx >= 0)[0][::5]:
+            gp, gm = gates.copy(), gates.copy()
+            gp["angle"][i] += h
+            gm["angle"][i] -= h
+            fd = (A.value(n, chi, gp, labels, coeffs) - A.value(n, chi, gm, labels, coeffs)) / (2 * h)
+            assert abs(g[i] - fd) <= 1e-8

@@ -150,6 +150,7 @@ struct Op {
     bool two;
     int site;        // 1q: site; 2q: left site (global site index)
     int slice = 0;   // batch slice the operation belongs to
+    int gate = -1;   // index of the gate (in the caller's list) this operation comes from
     Mat2 m2;
     double2 ueff[16];
 };
@@ -395,17 +396,20 @@ void count_launch(wqc_mps* m, int kind) {
 // ---------------------------------------------------------------------------
 struct Expander {
     std::vector<Op> ops;
+    int cur = -1;  // gate being expanded
     void one(int q, const Mat2& u) {
         Op o{};
         o.two = false;
         o.site = q;
         o.m2 = u;
+        o.gate = cur;
         ops.push_back(o);
     }
     void two_at(int p, const Mat4& u, bool cf) {
         Op o{};
         o.two = true;
         o.site = p;
+        o.gate = cur;
         effective(u, cf, o.ueff);
         ops.push_back(o);
     }
@@ -470,6 +474,7 @@ wqc_status check_gate(int n, const wqc_gate& g) {
 wqc_status expand(int n, const wqc_gate* gates, uint32_t count, bool adjoint, Expander& ex) {
     for (uint32_t i = 0; i < count; ++i) {
         const wqc_gate& g = gates[adjoint ? count - 1 - i : i];
+        ex.cur = int(adjoint ? count - 1 - i : i);
         if (wqc_status s = check_gate(n, g)) return s;
         switch (g.kind) {
             case WQC_GATE_CNOT:
@@ -1977,5 +1982,430 @@ void wqc_mps_reset_stats(wqc_mps* m) {
 }
 
 void* wqc_mps_stream(wqc_mps* m) { return m ? static_cast<void*>(m->stream) : nullptr; }
+
+}  // extern "C"
+
+// ===========================================================================
+// Differentiation form: the adjoint (reverse-mode) gradient of a Pauli-sum
+// observable with respect to the rotation angles of the gate list.
+//
+// Forward: the gate list runs on the state from |0...0> in segments; the
+// sites (and bonds) at the start of every segment but the first, and at the
+// end, are copied to checkpoints.  Backward: the site cotangents of the end
+// state come from the observable's environments; then, segment by segment
+// from the last, the segment's state is restored from its checkpoint and its
+// operations are recomputed one at a time, the inputs each needs in reverse
+// (the site before a one-qubit gate; the sites, theta and the Jacobi's W,
+// singular values and order of a split) copied to a tape, and the tape is
+// swept in reverse (adjoint_kernels.cu).  The split rule is the exact one on
+// every split (a range finder seeded by a rank-48 test matrix has no
+// meaningful derivative), and the plain FP64 form is required.
+// ===========================================================================
+struct wqc_adjoint {
+    wqc_mps* m = nullptr;
+    std::vector<wqc_gate> gates;
+    std::vector<uint32_t> starts;  // segment starts; segment s is [starts[s], starts[s + 1] or count)
+    size_t pool_bytes = 0;         // the state's site pool
+    // checkpoint c (1 .. nseg - 1: segment starts; nseg: the end state):
+    // site pool, then dl and dr
+    std::vector<char*> cp;
+    std::vector<std::vector<int>> cp_ub;
+    uint32_t end_records = 0;
+    bool forward_done = false;
+};
+
+namespace {
+
+// d u / d angle of the rotations of gates.rs:10-66.
+bool rotation_derivative(const wqc_gate& g, double2* du) {
+    const double s = 0.5 * std::sin(g.angle / 2.0), c = 0.5 * std::cos(g.angle / 2.0);
+    switch (g.kind) {
+        case WQC_GATE_RX:
+            du[0] = C(-s); du[1] = C(0, -c); du[2] = C(0, -c); du[3] = C(-s);
+            return true;
+        case WQC_GATE_RY:
+            du[0] = C(-s); du[1] = C(-c); du[2] = C(c); du[3] = C(-s);
+            return true;
+        case WQC_GATE_RZ:
+            du[0] = C(-s, -c); du[1] = C(0); du[2] = C(0); du[3] = C(-s, c);
+            return true;
+        default:
+            return false;
+    }
+}
+
+size_t adj_pool_bytes(const wqc_mps* m) { return size_t(m->n) * m->chi * 2 * m->chi * sizeof(double2); }
+
+wqc_status adj_save(wqc_adjoint* a, size_t c) {
+    wqc_mps* m = a->m;
+    const size_t bytes = a->pool_bytes + 2 * size_t(m->n) * sizeof(int);
+    if (!a->cp[c]) {
+        void* p = nullptr;
+        if (wqc_status st = dmalloc(m, &p, bytes)) return st;
+        a->cp[c] = static_cast<char*>(p);
+    }
+    CUDA_TRY(cudaMemcpyAsync(a->cp[c], m->site_pool, a->pool_bytes, cudaMemcpyDeviceToDevice, m->stream));
+    CUDA_TRY(cudaMemcpyAsync(a->cp[c] + a->pool_bytes, m->d_dl, size_t(m->n) * sizeof(int), cudaMemcpyDeviceToDevice,
+                             m->stream));
+    CUDA_TRY(cudaMemcpyAsync(a->cp[c] + a->pool_bytes + size_t(m->n) * sizeof(int), m->d_dr,
+                             size_t(m->n) * sizeof(int), cudaMemcpyDeviceToDevice, m->stream));
+    a->cp_ub[c] = m->ub;
+    return WQC_OK;
+}
+
+wqc_status adj_restore(wqc_adjoint* a, size_t c) {
+    wqc_mps* m = a->m;
+    if (c == 0) {
+        reset_sites_kernel<<<(m->n + 255) / 256, 256, 0, m->stream>>>(m->dev);
+        CUDA_TRY(cudaGetLastError());
+        std::fill(m->ub.begin(), m->ub.end(), 1);
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(m->site_pool, a->cp[c], a->pool_bytes, cudaMemcpyDeviceToDevice, m->stream));
+        CUDA_TRY(cudaMemcpyAsync(m->d_dl, a->cp[c] + a->pool_bytes, size_t(m->n) * sizeof(int),
+                                 cudaMemcpyDeviceToDevice, m->stream));
+        CUDA_TRY(cudaMemcpyAsync(m->d_dr, a->cp[c] + a->pool_bytes + size_t(m->n) * sizeof(int),
+                                 size_t(m->n) * sizeof(int), cudaMemcpyDeviceToDevice, m->stream));
+        m->ub = a->cp_ub[c];
+    }
+    m->lvalid = 0;
+    m->rvalid = m->n - 1;
+    return WQC_OK;
+}
+
+// Device buffers of one backward pass, freed together.
+struct AdjBuffers {
+    wqc_mps* m;
+    std::vector<std::pair<void*, size_t>> owned;
+    explicit AdjBuffers(wqc_mps* mm) : m(mm) {}
+    ~AdjBuffers() {
+        if (m->stream) cudaStreamSynchronize(m->stream);
+        for (auto& p : owned) dfree(m, p.first, p.second);
+    }
+    template <class T>
+    wqc_status get(T** out, size_t count) {
+        void* p = nullptr;
+        const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+        if (wqc_status st = dmalloc(m, &p, bytes)) return st;
+        owned.push_back({p, bytes});
+        *out = static_cast<T*>(p);
+        return WQC_OK;
+    }
+    void release(void* p) {
+        for (size_t i = 0; i < owned.size(); ++i)
+            if (owned[i].first == p) {
+                cudaStreamSynchronize(m->stream);
+                dfree(m, p, owned[i].second);
+                owned.erase(owned.begin() + long(i));
+                return;
+            }
+    }
+};
+
+// One recomputed operation on the tape.
+struct TapeEntry {
+    bool two;
+    int site;
+    int gate;
+    double2 u[16];
+    size_t off;  // byte offset of its data in the tape arena
+};
+
+}  // namespace
+
+extern "C" {
+
+wqc_status wqc_adjoint_forward(wqc_mps* m, const wqc_gate* gates, uint32_t count, const uint32_t* checkpoints,
+                               uint32_t ncheckpoints, wqc_adjoint** out) {
+    if (!m || !out || (!gates && count) || (ncheckpoints && !checkpoints)) return fail(WQC_ERR_INVALID, "null argument");
+    if (m->seg_first.size() != 1) return fail(WQC_ERR_INVALID, "the adjoint takes a single state, not a batch");
+    if (m->fp32) return fail(WQC_ERR_INVALID, "the adjoint differentiates the plain FP64 form");
+    Expander check;
+    if (wqc_status st = expand(m->n, gates, count, false, check)) return st;
+    auto* a = new wqc_adjoint();
+    a->m = m;
+    a->gates.assign(gates, gates + count);
+    a->starts.push_back(0);
+    std::vector<uint32_t> cps(checkpoints, checkpoints + ncheckpoints);
+    std::sort(cps.begin(), cps.end());
+    for (uint32_t c : cps)
+        if (c > a->starts.back() && c < count) a->starts.push_back(c);
+    a->pool_bytes = adj_pool_bytes(m);
+    a->cp.assign(a->starts.size() + 1, nullptr);
+    a->cp_ub.resize(a->starts.size() + 1);
+    const bool rule = m->exact_only;
+    m->exact_only = true;
+    wqc_status st = wqc_mps_reset(m);
+    for (size_t sgi = 0; sgi < a->starts.size() && st == WQC_OK; ++sgi) {
+        if (sgi > 0) st = adj_save(a, sgi);
+        const uint32_t g0 = a->starts[sgi], g1 = sgi + 1 < a->starts.size() ? a->starts[sgi + 1] : count;
+        if (st == WQC_OK && g1 > g0) {
+            Expander ex;
+            st = expand(m->n, a->gates.data() + g0, g1 - g0, false, ex);
+            if (st == WQC_OK) st = run_ops(m, ex.ops);
+        }
+    }
+    if (st == WQC_OK) st = adj_save(a, a->starts.size());
+    if (st == WQC_OK) st = sync_status(m);
+    m->exact_only = rule;
+    a->end_records = m->rec_count;
+    if (st != WQC_OK) {
+        wqc_adjoint_destroy(a);
+        return st;
+    }
+    a->forward_done = true;
+    *out = a;
+    return WQC_OK;
+}
+
+wqc_status wqc_adjoint_backward(wqc_adjoint* a, const char* labels, const double* coeffs, uint32_t nterms,
+                                double value[2], double* grad) {
+    if (!a || !a->forward_done || !labels || !coeffs || !value || (!grad && !a->gates.empty()))
+        return fail(WQC_ERR_INVALID, "null argument");
+    wqc_mps* m = a->m;
+    const int n = m->n, chi = m->chi, R = 2 * chi;
+    for (size_t i = 0; i < size_t(nterms) * n; ++i) {
+        const char ch = labels[i];
+        if (ch != 'I' && ch != 'X' && ch != 'Y' && ch != 'Z')
+            return fail(WQC_ERR_INVALID, std::string("invalid pauli character in label"));
+    }
+    if (nterms == 0) return fail(WQC_ERR_INVALID, "the adjoint needs at least one Pauli term");
+    CUDA_TRY(cudaSetDevice(m->ctx->device));
+    const bool rule = m->exact_only;
+    m->exact_only = true;
+    struct RuleGuard {
+        wqc_mps* m;
+        bool rule;
+        ~RuleGuard() { m->exact_only = rule; }
+    } guard{m, rule};
+    AdjBuffers buf(m);
+    const size_t site_cap = size_t(chi) * 2 * chi;
+    // Cotangent sites, one per site at the state's capacity, and their pointers.
+    double2* bar_pool = nullptr;
+    double2** d_bars = nullptr;
+    if (wqc_status st = buf.get(&bar_pool, site_cap * n)) return st;
+    if (wqc_status st = buf.get(&d_bars, n)) return st;
+    std::vector<double2*> bars(n);
+    for (int q = 0; q < n; ++q) bars[q] = bar_pool + site_cap * q;
+    CUDA_TRY(cudaMemcpyAsync(d_bars, bars.data(), n * sizeof(double2*), cudaMemcpyHostToDevice, m->stream));
+    // The end state and the observable's environments, values and cotangents.
+    if (wqc_status st = adj_restore(a, a->starts.size())) return st;
+    {
+        const size_t E = size_t(chi) * chi;
+        char* d_lab = nullptr;
+        double* d_cre = nullptr;
+        double2 *envs = nullptr, *tmp = nullptr, *vals = nullptr;
+        if (wqc_status st = buf.get(&d_lab, size_t(nterms) * n + 16)) return st;
+        if (wqc_status st = buf.get(&d_cre, nterms)) return st;
+        if (wqc_status st = buf.get(&envs, size_t(nterms) * (2 * n + 1) * E)) return st;
+        if (wqc_status st = buf.get(&tmp, size_t(nterms) * 2 * E)) return st;
+        if (wqc_status st = buf.get(&vals, nterms)) return st;
+        std::vector<double> cre(nterms);
+        for (uint32_t t = 0; t < nterms; ++t) cre[t] = coeffs[2 * t];
+        CUDA_TRY(cudaMemcpyAsync(d_lab, labels, size_t(nterms) * n, cudaMemcpyHostToDevice, m->stream));
+        CUDA_TRY(cudaMemcpyAsync(d_cre, cre.data(), nterms * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+        adj_pauli_envs_kernel<<<nterms, 256, 0, m->stream>>>(m->dev, d_lab, int(nterms), chi, envs, tmp, vals);
+        count_launch(m, -1);
+        // Holes in chunks of terms, accumulated in term order.
+        const size_t per_term = 2 * size_t(n) * site_cap * sizeof(double2);
+        const int chunk = int(std::max<size_t>(1, std::min<size_t>(16, (size_t(1) << 30) / per_term)));
+        double2 *holes = nullptr, *htmp = nullptr;
+        if (wqc_status st = buf.get(&holes, size_t(chunk) * n * site_cap)) return st;
+        if (wqc_status st = buf.get(&htmp, size_t(chunk) * n * site_cap)) return st;
+        const int agrid = int(std::max<size_t>(1, std::min<size_t>((site_cap + 255) / 256, 64)));
+        for (uint32_t t0 = 0; t0 < nterms; t0 += uint32_t(chunk)) {
+            const int cnt = int(std::min<uint32_t>(uint32_t(chunk), nterms - t0));
+            adj_pauli_holes_kernel<<<dim3(n, cnt), 256, 0, m->stream>>>(m->dev, d_lab, int(t0), chi, envs, htmp, holes);
+            adj_pauli_accumulate_kernel<<<dim3(agrid, n), 256, 0, m->stream>>>(m->dev, d_bars, holes, d_cre, int(t0),
+                                                                             cnt, chi, t0 == 0 ? 1 : 0);
+            count_launch(m, -1);
+            count_launch(m, -1);
+        }
+        CUDA_TRY(cudaGetLastError());
+        std::vector<double2> hv(nterms);
+        CUDA_TRY(cudaMemcpyAsync(hv.data(), vals, nterms * sizeof(double2), cudaMemcpyDeviceToHost, m->stream));
+        CUDA_TRY(cudaStreamSynchronize(m->stream));
+        double re = 0, im = 0;
+        for (uint32_t t = 0; t < nterms; ++t) {  // coeff * Re<P> (expectation.rs:177-185), term order
+            re += coeffs[2 * t] * hv[t].x;
+            im += coeffs[2 * t + 1] * hv[t].x;
+        }
+        value[0] = re;
+        value[1] = im;
+        buf.release(envs);
+        buf.release(tmp);
+        buf.release(holes);
+        buf.release(htmp);
+    }
+    // Gradient slots: one per one-qubit operation of the whole list.
+    Expander all;
+    if (wqc_status st = expand(n, a->gates.data(), uint32_t(a->gates.size()), false, all)) return st;
+    size_t n1q = 0;
+    for (const Op& o : all.ops) n1q += o.two ? 0 : 1;
+    double* d_grad = nullptr;
+    if (wqc_status st = buf.get(&d_grad, n1q + 1)) return st;
+    CUDA_TRY(cudaMemsetAsync(d_grad, 0, (n1q + 1) * sizeof(double), m->stream));
+    std::vector<int> slot_gate;  // gate of each gradient slot
+    // Split workspace (column-major R x R matrices) and the slot-0 buffers.
+    double2* ws = nullptr;
+    double* wsd = nullptr;
+    if (wqc_status st = buf.get(&ws, 10 * size_t(R) * R)) return st;
+    if (wqc_status st = buf.get(&wsd, 2 * size_t(R))) return st;
+    SlotBuffers slot0;
+    CUDA_TRY(cudaMemcpy(&slot0, m->d_slots, sizeof(slot0), cudaMemcpyDeviceToHost));
+    // Tape layout of one operation (bytes, 256-aligned parts).
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t site_b = al(site_cap * sizeof(double2));
+    const size_t mat_b = al(size_t(R) * R * sizeof(double2));
+    const size_t one_b = site_b + al(2 * sizeof(int));
+    const size_t two_b = 2 * site_b + 2 * mat_b + al(R * sizeof(double)) + al(R * sizeof(int)) + al(sizeof(SplitState));
+    char* tape = nullptr;
+    size_t tape_cap = 0;
+    // First gradient slot of each segment (one-qubit operations in program order).
+    std::vector<size_t> seg_slot0(a->starts.size());
+    {
+        size_t acc = 0;
+        for (size_t sgi = 0; sgi < a->starts.size(); ++sgi) {
+            seg_slot0[sgi] = acc;
+            const uint32_t g1 = sgi + 1 < a->starts.size() ? a->starts[sgi + 1] : uint32_t(a->gates.size());
+            for (const Op& o : all.ops)
+                if (!o.two && o.gate >= int(a->starts[sgi]) && o.gate < int(g1)) ++acc;
+        }
+        for (const Op& o : all.ops)
+            if (!o.two) slot_gate.push_back(o.gate);
+    }
+    const int eg = int(std::min<long>((long(R) * R + 255) / 256, 4L * m->ctx->sm_count));
+    const dim3 gg((R + 31) / 32, (R + 31) / 32);
+    for (size_t sgi = a->starts.size(); sgi-- > 0;) {
+        const uint32_t g0 = a->starts[sgi];
+        const uint32_t g1 = sgi + 1 < a->starts.size() ? a->starts[sgi + 1] : uint32_t(a->gates.size());
+        if (g1 <= g0) continue;
+        Expander ex;
+        if (wqc_status st = expand(n, a->gates.data() + g0, g1 - g0, false, ex)) return st;
+        std::vector<TapeEntry> ents;
+        size_t need = 0;
+        for (const Op& o : ex.ops) {
+            TapeEntry t{};
+            t.two = o.two;
+            t.site = o.site;
+            t.gate = o.gate + int(g0);
+            if (o.two)
+                std::memcpy(t.u, o.ueff, sizeof(t.u));
+            else
+                std::memcpy(t.u, o.m2.u, sizeof(o.m2.u));
+            t.off = need;
+            need += o.two ? two_b : one_b;
+            ents.push_back(t);
+        }
+        if (need > tape_cap) {
+            if (tape) buf.release(tape);
+            tape = nullptr;
+            if (wqc_status st = buf.get(&tape, need)) return st;
+            tape_cap = need;
+        }
+        // Recompute the segment one operation at a time, taping each one's inputs.
+        if (wqc_status st = adj_restore(a, sgi)) return st;
+        for (size_t k = 0; k < ex.ops.size(); ++k) {
+            const Op& o = ex.ops[k];
+            char* base = tape + ents[k].off;
+            if (!o.two) {
+                CUDA_TRY(cudaMemcpyAsync(base, m->site_ptr[o.site], site_cap * sizeof(double2),
+                                         cudaMemcpyDeviceToDevice, m->stream));
+                CUDA_TRY(cudaMemcpyAsync(base + site_b, m->d_dl + o.site, sizeof(int), cudaMemcpyDeviceToDevice,
+                                         m->stream));
+                CUDA_TRY(cudaMemcpyAsync(base + site_b + sizeof(int), m->d_dr + o.site, sizeof(int),
+                                         cudaMemcpyDeviceToDevice, m->stream));
+            } else {
+                CUDA_TRY(cudaMemcpyAsync(base, m->site_ptr[o.site], site_cap * sizeof(double2),
+                                         cudaMemcpyDeviceToDevice, m->stream));
+                CUDA_TRY(cudaMemcpyAsync(base + site_b, m->site_ptr[o.site + 1], site_cap * sizeof(double2),
+                                         cudaMemcpyDeviceToDevice, m->stream));
+            }
+            std::vector<Op> one{o};
+            if (wqc_status st = run_ops(m, one)) return st;
+            if (o.two) {
+                char* p = base + 2 * site_b;
+                CUDA_TRY(cudaMemcpyAsync(p, slot0.theta, size_t(R) * R * sizeof(double2), cudaMemcpyDeviceToDevice,
+                                         m->stream));
+                CUDA_TRY(cudaMemcpyAsync(p + mat_b, slot0.w, size_t(R) * R * sizeof(double2),
+                                         cudaMemcpyDeviceToDevice, m->stream));
+                CUDA_TRY(cudaMemcpyAsync(p + 2 * mat_b, slot0.sigma, R * sizeof(double), cudaMemcpyDeviceToDevice,
+                                         m->stream));
+                CUDA_TRY(cudaMemcpyAsync(p + 2 * mat_b + al(R * sizeof(double)), slot0.perm, R * sizeof(int),
+                                         cudaMemcpyDeviceToDevice, m->stream));
+                CUDA_TRY(cudaMemcpyAsync(p + 2 * mat_b + al(R * sizeof(double)) + al(R * sizeof(int)), m->d_state,
+                                         sizeof(SplitState), cudaMemcpyDeviceToDevice, m->stream));
+            }
+        }
+        // Reverse sweep over the segment.
+        size_t slot = seg_slot0[sgi];
+        for (const TapeEntry& t : ents) slot += t.two ? 0 : 1;
+        for (size_t k = ents.size(); k-- > 0;) {
+            const TapeEntry& t = ents[k];
+            const char* base = tape + t.off;
+            if (!t.two) {
+                --slot;
+                Adj1q g{};
+                std::memcpy(g.u, t.u, sizeof(g.u));
+                g.has_du = rotation_derivative(a->gates[t.gate], g.du) ? 1 : 0;
+                g.slot = int(slot);
+                adj_one_qubit_kernel<<<1, 256, 0, m->stream>>>(bars[t.site], reinterpret_cast<const double2*>(base),
+                                                               reinterpret_cast<const int*>(base + site_b), g, d_grad);
+                count_launch(m, -1);
+                continue;
+            }
+            AdjSplit A{};
+            const char* p = base + 2 * site_b;
+            A.site_l = reinterpret_cast<const double2*>(base);
+            A.site_r = reinterpret_cast<const double2*>(base + site_b);
+            A.theta = reinterpret_cast<const double2*>(p);
+            A.w = reinterpret_cast<const double2*>(p + mat_b);
+            A.sigma = reinterpret_cast<const double*>(p + 2 * mat_b);
+            A.perm = reinterpret_cast<const int*>(p + 2 * mat_b + al(R * sizeof(double)));
+            A.st = reinterpret_cast<const SplitState*>(p + 2 * mat_b + al(R * sizeof(double)) + al(R * sizeof(int)));
+            A.bar_l = bars[t.site];
+            A.bar_r = bars[t.site + 1];
+            std::memcpy(A.u, t.u, sizeof(A.u));
+            double2* w = ws;
+            const size_t RR = size_t(R) * R;
+            A.U = w; A.V = w + RR; A.Ub = w + 2 * RR; A.Vb = w + 3 * RR; A.M = w + 4 * RR; A.Nm = w + 5 * RR;
+            A.Z = w + 6 * RR; A.T1 = w + 7 * RR; A.tb = w + 8 * RR; A.tb0 = w + 9 * RR;
+            A.inv = wsd;
+            A.sq = wsd + R;
+            A.R = R;
+            adj_split_prep_kernel<<<eg, 256, 0, m->stream>>>(A);
+            adj_split_gemm_kernel<<<gg, 256, 0, m->stream>>>(A, kAdjStageOther);
+            adj_split_gemm_kernel<<<gg, 256, 0, m->stream>>>(A, kAdjStageM);
+            adj_split_gemm_kernel<<<gg, 256, 0, m->stream>>>(A, kAdjStageN);
+            adj_split_assemble_kernel<<<eg, 256, 0, m->stream>>>(A);
+            adj_split_gemm_kernel<<<gg, 256, 0, m->stream>>>(A, kAdjStageT1);
+            adj_split_gemm_kernel<<<gg, 256, 0, m->stream>>>(A, kAdjStageTb);
+            adj_split_gemm_kernel<<<gg, 256, 0, m->stream>>>(A, kAdjStageTb2);
+            adj_split_gate_kernel<<<eg, 256, 0, m->stream>>>(A);
+            adj_split_gemm_kernel<<<gg, 256, 0, m->stream>>>(A, kAdjStageBarL);
+            adj_split_gemm_kernel<<<gg, 256, 0, m->stream>>>(A, kAdjStageBarR);
+            for (int c = 0; c < 11; ++c) count_launch(m, -1);
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+    std::vector<double> hg(n1q + 1);
+    CUDA_TRY(cudaMemcpyAsync(hg.data(), d_grad, (n1q + 1) * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    if (wqc_status st = sync_status(m)) return st;
+    for (size_t i = 0; i < a->gates.size(); ++i) grad[i] = 0.0;
+    for (size_t sl = 0; sl < n1q; ++sl) grad[slot_gate[sl]] += hg[sl];
+    // The state holds the end state again; its records are the forward's.
+    if (wqc_status st = adj_restore(a, a->starts.size())) return st;
+    m->rec_count = a->end_records;
+    return sync_status(m);
+}
+
+void wqc_adjoint_destroy(wqc_adjoint* a) {
+    if (!a) return;
+    if (a->m) {
+        if (a->m->stream) cudaStreamSynchronize(a->m->stream);
+        const size_t bytes = a->pool_bytes + 2 * size_t(a->m->n) * sizeof(int);
+        for (char* p : a->cp) dfree(a->m, p, bytes);
+    }
+    delete a;
+}
 
 }  // extern "C"

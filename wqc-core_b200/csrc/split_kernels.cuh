@@ -112,6 +112,45 @@ __global__ void sample_env_kernel(const double2* site, int l, int r, const doubl
 __global__ void sample_shots_kernel(DeviceMps mps, const double2* envs, const unsigned long long* env_off,
                                     const int* bitpos, unsigned long long seed, int shots, unsigned long long* out);
 
+// Adjoint kernels (adjoint_kernels.cu).
+struct Adj1q {
+    double2 u[4];   // the gate, row-major
+    double2 du[4];  // d u / d angle (rotations)
+    int has_du;
+    int slot;       // gradient slot of this gate instance
+};
+// One split of the reverse sweep: the tape's copies of its forward inputs
+// and outputs, the cotangent sites it updates, and the workspace matrices
+// (column-major, leading dimension R = 2 chi_max).
+struct AdjSplit {
+    const SplitState* st;
+    const double2* theta;   // rows x cols, row-major
+    const double2* w;       // Jacobi W, M x N column-major
+    const double* sigma;    // N
+    const int* perm;        // N: sorted position -> column
+    const double2* site_l;  // site p before the split: [dl][2][k]
+    const double2* site_r;  // site p+1 before the split: [k][2][dr]
+    double2* bar_l;         // cotangent of site p
+    double2* bar_r;         // cotangent of site p+1
+    double2 u[16];          // effective 4x4 of the gate on theta
+    double2 *U, *V, *Ub, *Vb, *M, *Nm, *Z, *T1, *tb, *tb0;
+    double *inv, *sq;
+    int R;
+};
+enum { kAdjStageOther = 0, kAdjStageM, kAdjStageN, kAdjStageT1, kAdjStageTb, kAdjStageTb2, kAdjStageBarL,
+       kAdjStageBarR };
+__global__ void adj_pauli_envs_kernel(DeviceMps mps, const char* labels, int nterms, int cap, double2* envs,
+                                      double2* tmp_all, double2* vals);
+__global__ void adj_pauli_holes_kernel(DeviceMps mps, const char* labels, int t0, int cap, const double2* envs,
+                                       double2* tmp_all, double2* holes);
+__global__ void adj_pauli_accumulate_kernel(DeviceMps mps, double2* const* bars, const double2* holes,
+                                            const double* coef_re, int t0, int count, int cap, int first);
+__global__ void adj_one_qubit_kernel(double2* bar, const double2* before, const int* dims, Adj1q g, double* grad);
+__global__ void adj_split_prep_kernel(AdjSplit A);
+__global__ void adj_split_gemm_kernel(AdjSplit A, int stage);
+__global__ void adj_split_assemble_kernel(AdjSplit A);
+__global__ void adj_split_gate_kernel(AdjSplit A);
+
 // Jacobi shared-memory footprint for a working matrix of M rows and N columns
 // on a cluster of C CTAs, `elem` bytes per complex entry.
 inline size_t jacobi_smem_bytes(int M, int N, int C, size_t elem = sizeof(double2)) {

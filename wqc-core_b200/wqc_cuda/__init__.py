@@ -50,6 +50,7 @@ EXPORTS = (
     "wqc_batch_create", "wqc_batch_apply_gates", "wqc_batch_amplitudes", "wqc_batch_slice_times",
     "wqc_expectation_pauli_noalloc", "wqc_batch_expectation_pauli", "wqc_mps_sample",
     "wqc_mps_overlap", "wqc_cuda_last_oom", "wqc_mps_site_amplitudes_many", "wqc_mps_to_dense",
+    "wqc_adjoint_forward", "wqc_adjoint_backward", "wqc_adjoint_destroy",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
@@ -120,6 +121,10 @@ def lib():
         L.wqc_mps_site_amplitudes.argtypes = [P, U32, D]
         L.wqc_mps_site_amplitudes_many.argtypes = [P, ctypes.POINTER(U32), U32, D]
         L.wqc_mps_to_dense.argtypes = [P, ctypes.c_int32, D]
+        L.wqc_adjoint_forward.argtypes = [P, P, U32, ctypes.POINTER(U32), U32, ctypes.POINTER(P)]
+        L.wqc_adjoint_backward.argtypes = [P, ctypes.c_char_p, D, U32, D, D]
+        L.wqc_adjoint_destroy.argtypes = [P]
+        L.wqc_adjoint_destroy.restype = None
         L.wqc_mps_bond_dims.argtypes = [P, ctypes.POINTER(U32)]
         L.wqc_mps_download_site.argtypes = [P, U32, ctypes.POINTER(U32), ctypes.POINTER(U32), D]
         L.wqc_mps_upload_site.argtypes = [P, U32, U32, U32, D]
@@ -491,6 +496,59 @@ def expectation_pauli_noalloc(sites_ptr: int, site_stride: int, bond_dims, label
     return complex(out[0], out[1])
 
 
+class Adjoint:
+    """The differentiation form's forward/backward op pair
+    (wqc_adjoint_forward / wqc_adjoint_backward) on a single state: the
+    forward runs `gates` from |0...0> keeping checkpoints at the gate
+    indices `checkpoints`; backward(labels, coeffs) returns (f, df/dangle
+    per gate) by the reverse sweep."""
+
+    def __init__(self, mps: "CudaMps", gates: np.ndarray, checkpoints=()):
+        self.mps = mps
+        self.gates = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        cps = np.ascontiguousarray(checkpoints, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        _check(lib().wqc_adjoint_forward(mps._h, self.gates.ctypes.data, len(self.gates),
+                                         cps.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), len(cps),
+                                         ctypes.byref(h)))
+        self._h = h
+
+    def backward(self, labels, coeffs):
+        joined, c = _pauli_args(labels, coeffs, self.mps.n)
+        value = np.zeros(2)
+        grad = np.zeros(max(len(self.gates), 1))
+        _check(lib().wqc_adjoint_backward(self._h, joined, _dp(c.view(np.float64)), len(labels), _dp(value),
+                                          _dp(grad)))
+        return float(value[0]), grad[: len(self.gates)]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().wqc_adjoint_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def adjoint_gradient(n: int, chi: int, gates: np.ndarray, pidx: np.ndarray, labels, coeffs, checkpoints=(),
+                     ctx: Context | None = None):
+    """(f, df/dparams) by the adjoint: per-gate derivatives summed over the
+    gate instances of each parameter (pidx[i] = parameter of gate i, or -1)."""
+    m = CudaMps(n, chi, ctx=ctx)
+    adj = Adjoint(m, gates, checkpoints)
+    try:
+        f, g = adj.backward(labels, coeffs)
+    finally:
+        adj.close()
+        m.close()
+    pidx = np.asarray(pidx)
+    grad = np.zeros(int(pidx.max()) + 1 if pidx.size and pidx.max() >= 0 else 0)
+    for i, p in enumerate(pidx):
+        if p >= 0:
+            grad[p] += g[i]
+    return f, grad
+
+
 class CudaBatch(CudaMps):
     """Many independent slices in one device state (wqc_batch_create): their
     splits share waves; each slice keeps its own MpsState semantics."""
@@ -635,5 +693,5 @@ def split_flops(rec) -> float:
     return f
 
 
-__all__ = ["CudaMps", "CudaBatch", "Context", "WqcCudaError", "lib", "build", "run", "workspace_bytes", "split_flops",
+__all__ = ["CudaMps", "CudaBatch", "Context", "Adjoint", "adjoint_gradient", "WqcCudaError", "lib", "build", "run", "workspace_bytes", "split_flops",
            "svd_flops", "CNOT4", "CZ4", "SWAP4", "EXPORTS", "KERNEL_KINDS", "math"]

@@ -170,6 +170,13 @@ def hea_ansatz(n: int = 32, layers: int = 8, seed: int = 20261206):
     return gates_array(gates), np.array(pidx, dtype=np.int64), params
 
 
+def hea_checkpoints(n: int, layers: int, every: int = 2) -> np.ndarray:
+    """Gate indices of the first gate of every `every`-th layer of
+    hea_ansatz(n, layers) after the first (the adjoint's checkpoints)."""
+    per_layer = 2 * n + (n - 1)
+    return np.array([L * per_layer for L in range(every, layers, every)], dtype=np.uint32)
+
+
 def zz_x_observable(n: int):
     """sum_i Z_i Z_{i+1} + 0.5 sum_i X_i as (labels, coefficients); label
     character n-1-q acts on qubit q."""
