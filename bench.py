@@ -169,16 +169,20 @@ def oracle_batch_sample(slices, budget_s: float, threads: int):
 
 
 def precision_leg(W, torch, ctx, w, rule, steps: int, flush, fp64_value: float) -> dict:
-    """The precision form (WQC_PRECISION_FP32: complex64 Jacobi columns, FP64
-    rotation parameters, tests and norms) on the same circuit and steps, and
-    its amplitude error on the 16-qubit chi 32 brickwork against the plain
-    FP64 form (itself within 1e-12 of the FP64 oracle there)."""
+    """The precision form (WQC_PRECISION_FP32: complex64 Jacobi sweeps with
+    the accumulated V as each SVD's first phase, V made orthonormal in FP64,
+    X V in FP64, FP64 sweeps to finish) on the whole headline circuit, and
+    its error against FP64: on the 16-qubit chi 32 brickwork against the
+    plain form (itself within 1e-12 of the FP64 oracle there), and on the
+    headline circuit under the exact rule against the oracle's fixture."""
     m = W.CudaMps(w.n, w.chi, ctx=ctx, precision=W.PRECISION_FP32)
     m.set_split_rule(rule)
     stream = torch.cuda.ExternalStream(m.stream())
     total_ms, splits = 0.0, 0
     for k in range(steps + 1):
         m.reset()
+        if k == 1:
+            m.reset_stats()
         flush.fill_(float(np.random.random()))
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -190,6 +194,7 @@ def precision_leg(W, torch, ctx, w, rule, steps: int, flush, fp64_value: float) 
         if k > 0:  # the first pass is a warm-up
             total_ms += e0.elapsed_time(e1)
             splits += m.split_count()
+    st = m.kernel_stats()
     m.close()
     value = splits / (total_ms * 1e-3)
     w0 = C.config0()
@@ -199,17 +204,40 @@ def precision_leg(W, torch, ctx, w, rule, steps: int, flush, fp64_value: float) 
         m0.apply_gates(w0.gates)
         amps.append(m0.amplitude_at_compact_zero())
         m0.close()
-    return {
-        "form": "complex64 Jacobi columns (FP32 dot products and rotation updates), FP64 rotation parameters, "
-                "tolerance and convergence tests, column norms, sort and cut; sites, merge and range finder FP64",
+    out = {
+        "form": "each SVD: complex64 Jacobi sweeps (FP32 dot products and updates, FP64 rotation parameters and "
+                "tests) carrying X V and V, then V orthonormalised (one Newton-Schulz step), X V formed and FP64 "
+                "sweeps to finish; sites, merge, range finder, sort and cut FP64",
         "value": value,
         "unit": UNIT,
         "steps": steps,
+        "workload": "whole circuit from |0...0>, same as whole_circuit of the plain form",
         "speedup_vs_fp64": value / fp64_value,
+        "sweeps_per_svd_first_phase": st["jacobi_sweeps_first"] / st["jacobi_tasks"] if st["jacobi_tasks"] else None,
+        "sweeps_per_svd_fp64_finish": st["jacobi_sweeps"] / st["jacobi_tasks"] if st["jacobi_tasks"] else None,
         "amp_rel_err_vs_fp64": abs(amps[1] - amps[0]) / abs(amps[0]),
-        "error_workload": f"{w0.name}: {w0.n} qubits, chi_max {w0.chi} (the 50-qubit circuit's amplitude, ~1e-25, "
-                          f"is not stable under any change of rounding and is not used)",
+        "error_workload": f"{w0.name}: {w0.n} qubits, chi_max {w0.chi}",
     }
+    fx = os.path.join(ROOT, "tests", "golden", "config1_exact.npz")
+    if os.path.exists(fx) and w.n == 50:
+        ref = np.load(fx)
+        m1 = W.CudaMps(w.n, w.chi, ctx=ctx, precision=W.PRECISION_FP32)
+        m1.set_split_rule(W.SPLIT_RULE_EXACT)
+        m1.apply_gates(w.gates)
+        rec = m1.split_records()
+        norm2 = m1.expectation(["I" * w.n], [1.0]).real
+        m1.close()
+        rr = ref["records"]
+        out["exact_rule_vs_oracle"] = {
+            "chi_path_shape_bit_exact": bool(len(rr) == len(rec) and all(
+                np.array_equal(rr[k], rec[k]) for k in ("left_site", "rows", "cols", "path", "chi"))),
+            "max_weight_diff": float(np.max(np.abs(rr["discarded_weight"] - rec["discarded_weight"])))
+            if len(rr) == len(rec) else None,
+            "norm2_rel_err": abs(norm2 - float(ref["norm2"])) / float(ref["norm2"]),
+            "note": "the 50-qubit state's norm^2 (1.2e-30 after 2804 truncating splits) against the FP64 oracle; "
+                    "the oracle drifts against itself under a change of FP64 SVD by tests/golden/config1_drift.npz",
+        }
+    return out
 
 
 def oracle_gradient_sample(n, chi, lists, labels, coeffs, budget_s: float, threads: int):
@@ -247,8 +275,12 @@ def differentiation_leg(W, torch, ctx, flush, cpu_budget: float) -> dict:
     """Config 3's workload: the 32-qubit hardware-efficient ansatz (8 layers
     of RY, RZ on every qubit and a CZ ladder; 512 parameters), observable
     sum Z_i Z_i+1 + 0.5 sum X_i, chi_max 64.  One full gradient by the
-    parameter-shift rule: 1025 circuits (unshifted + two per parameter) as
-    slices of one batch, the observable evaluated on every slice."""
+    adjoint (forward with checkpoints every 2 layers, reverse sweep with SVD
+    backward through the truncated splits), and one by the parameter-shift
+    rule: 1025 circuits (unshifted + two per parameter) as slices of one
+    batch, the observable evaluated on every slice.  Through truncating
+    splits the two are different quantities (the adjoint is the derivative
+    of the truncated map); their distance is reported."""
     from wqc_cuda import gradients as G
 
     n, chi = 32, 64
@@ -271,10 +303,35 @@ def differentiation_leg(W, torch, ctx, flush, cpu_budget: float) -> dict:
     splits = b.split_count()
     b.close()
     grad = 0.5 * (vals[1::2] - vals[2::2])
+    # The adjoint: forward with checkpoints, then the reverse sweep (wall clock
+    # of the two C ABI calls, which synchronise the state's stream).
+    adj_runs = []
+    for _ in range(2):  # the first is a warm-up
+        m = W.CudaMps(n, chi, ctx=ctx)
+        flush.fill_(float(np.random.random()))
+        torch.cuda.synchronize()
+        ta = time.perf_counter()
+        adj = W.Adjoint(m, gates, C.hea_checkpoints(n, 8, 2))
+        tb = time.perf_counter()
+        fa, ga = adj.backward(labels, coeffs)
+        tc = time.perf_counter()
+        adj.close()
+        m.close()
+        adj_runs.append((tb - ta, tc - tb, fa, ga))
+    fwd_s, bwd_s, fa, ga = adj_runs[-1]
+    adj_grad = np.zeros(len(grad))
+    for i, p in enumerate(pidx):
+        if p >= 0:
+            adj_grad[p] += ga[i]
     out = {
         "workload": "hea32_l8_chi64: 32 qubits, 8 layers RY/RZ + CZ ladder, 512 parameters, "
                     "sum Z_i Z_i+1 + 0.5 sum X_i (63 terms), chi_max 64, FP64",
-        "method": "parameter shift on the batching form (the adjoint is not built)",
+        "method": "adjoint (checkpoints every 2 layers) and parameter shift on the batching form",
+        "adjoint_seconds": fwd_s + bwd_s,
+        "adjoint_forward_seconds": fwd_s,
+        "adjoint_backward_seconds": bwd_s,
+        "adjoint_value": fa,
+        "adjoint_vs_shift_max_abs_diff": float(np.abs(adj_grad - grad).max()),
         "circuits": len(lists),
         "gradient_seconds": dev_s,
         "gradient_seconds_e2e": wall,

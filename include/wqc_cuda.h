@@ -50,13 +50,15 @@ enum wqc_status_code {
 /* Arithmetic of the split path. */
 enum wqc_precision {
     WQC_PRECISION_FP64 = 0, /* plain form: complex128 throughout */
-    WQC_PRECISION_FP32 = 1  /* precision form: the Jacobi SVD works on complex64 columns
-                               (FP32 dot products and rotation updates; FP64 rotation
-                               parameters, tolerance tests, convergence test and column
-                               norms); sites, merges, range finder, sort and cut stay
-                               FP64.  Results carry FP32-level error against the plain
-                               form; split decisions made on near-tied singular values
-                               may differ from it. */
+    WQC_PRECISION_FP32 = 1  /* precision form: each Jacobi SVD runs in two phases.  The
+                               first sweeps complex64 columns (FP32 dot products and
+                               rotation updates, FP64 rotation parameters, tolerance and
+                               convergence tests) that carry X V and the accumulated V;
+                               V is then made orthonormal to FP64 rounding (one
+                               Newton-Schulz step) and X V formed in FP64, and FP64
+                               sweeps finish from there (quadratic convergence: a few
+                               sweeps).  Sites, merges, range finder, sort and cut stay
+                               FP64, so results carry FP64-level error. */
 };
 
 typedef struct wqc_cuda_ctx wqc_cuda_ctx;
@@ -356,7 +358,8 @@ typedef struct wqc_kernel_stats {
     uint64_t h2d_bytes;      /* host-to-device bytes copied by the calls (gate plans, sites) */
     uint64_t d2h_bytes;      /* device-to-host bytes of results (amplitudes, ...) */
     uint64_t jacobi_tasks;   /* SVDs run by the Jacobi kernel */
-    uint64_t jacobi_sweeps;  /* sweeps those SVDs took in total */
+    uint64_t jacobi_sweeps;  /* FP64 sweeps those SVDs took in total */
+    uint64_t jacobi_sweeps_first; /* precision form: sweeps of the complex64 first phase */
 } wqc_kernel_stats;
 WQC_API wqc_status wqc_mps_set_profiling(wqc_mps* mps, int32_t on);
 WQC_API wqc_status wqc_mps_kernel_stats(wqc_mps* mps, wqc_kernel_stats* out);

@@ -86,6 +86,7 @@ struct SplitState {
     int w_rows_of_src;   // exact Jacobi: 1 when W = theta^H (rows < cols)
     int skip;            // cancelled before this wave: nothing is computed or written
     double discarded;
+    double fro2;         // ||X||_F^2 seen by the precision form's first Jacobi phase
 };
 
 // Per-slot workspace pointers (device memory carved from one arena).

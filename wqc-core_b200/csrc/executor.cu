@@ -155,13 +155,22 @@ struct Op {
     double2 ueff[16];
 };
 
-struct Group {
-    int mode, C, idx_off, count;
-    size_t smem;
-    int threads;          // one warp per column pair of a block, at most kJacobiThreads
+// Launch shape of one Jacobi phase for a group of jobs.
+struct PhaseCfg {
+    int C = 0;            // cluster size
+    size_t smem = 0;
+    int threads = 0;      // one warp per column pair of a block, at most kJacobiThreads
     bool staged = false;  // jacobi_staged_kernel with blocks of b columns
     bool reg = false;     // cluster Jacobi variant with register-resident top columns
     int b = 0;
+};
+
+// Jobs of one wave whose SVDs share launch shapes: one phase in the plain
+// form; the complex64 first phase and the FP64 finish in the precision form.
+struct Group {
+    int mode, idx_off, count;
+    int nph = 1;
+    PhaseCfg ph[2];
 };
 
 struct Wave {
@@ -325,23 +334,25 @@ int round_up(int x, int q) { return ((x + q - 1) / q) * q; }
 // the other slices of its batch.
 bool jacobi_reg_variant(int M, int b) { return M <= kJacobiRegMaxRows && b <= kJacobiRegThreads / 32; }
 
-int choose_cluster(int M, int N, int max_c, int njobs, int sm_count, size_t elem, bool throughput) {
+// len: rows stored per column (M, or M + N when the precision form's first
+// phase carries V).
+int choose_cluster(int M, int N, int max_c, int njobs, int sm_count, size_t elem, bool throughput, int len = 0) {
+    if (len <= 0) len = M;
     int best = -1;
     double best_cost = 1e300;
     for (int Cc = 1; Cc <= max_c; ++Cc) {
-        if (jacobi_smem_bytes(M, N, Cc, elem) > kSmemLimit) continue;
+        if (jacobi_smem_bytes(len, N, Cc, elem) > kSmemLimit) continue;
         const int Np = round_up(N, 4 * Cc), b = Np / (2 * Cc);
         const int max_b = throughput ? kJacobiThreads / 32 : jacobi_max_warps(M);
         if (b > max_b && Cc < max_c) continue;  // more pairs than warps
         double cost;
         if (throughput) {
             const bool reg = jacobi_reg_variant(M, b);
-            const double traffic = (reg ? 3.0 : 6.0) * double(elem) * b * M / 128.0;
+            const double traffic = (reg ? 3.0 : 6.0) * double(elem) * b * len / 128.0;
             const double round = std::max(reg ? 1900.0 : 1300.0, traffic);
             const double cycles = Np * round + (Cc > 1 ? (2 * Cc - 1) * 4600.0 : 0.0);
             cost = cycles / 1900.0 * Cc;  // SM-microseconds at ~1.9 GHz
         } else {
-            const double len = M;
             const double step = std::max(0.3, b * (8.0 * M + 12.0 * len) / 64.0 / 1900.0);
             const double exch = Cc > 1 ? 2.0 + 2.0 * b * len * 16.0 / 1.0e5 : 0.0;
             cost = (Np - 1) * step + (2 * Cc - 1) * exch;
@@ -604,24 +615,52 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 w.oq_count = int(lb.oq.size());
                 first = false;
             }
-            const size_t j1 = std::min(lb.jobs.size(), j0 + size_t(m->nslots));
-            w.jobs_off = int(plan.jobs.size());
-            w.njobs = int(j1 - j0);
-            // cluster groups: key (mode, C)
-            std::vector<std::pair<std::pair<int, int>, std::vector<int>>> groups;
-            auto add = [&](int mode, int Cc, int local) {
+            // Jacobi groups: key (mode, shape of phase 1, shape of phase 2);
+            // a shape is a cluster size, or -b for the staged kernel with
+            // blocks of b columns.
+            struct GKey {
+                int mode, k1, k2;
+            };
+            std::vector<std::pair<GKey, std::vector<int>>> groups;
+            auto add = [&](int mode, int k1, int k2, int local) {
                 for (auto& g : groups)
-                    if (g.first.first == mode && g.first.second == Cc) {
+                    if (g.first.mode == mode && g.first.k1 == k1 && g.first.k2 == k2) {
                         g.second.push_back(local);
                         return;
                     }
-                groups.push_back({{mode, Cc}, {local}});
+                groups.push_back({{mode, k1, k2}, {local}});
             };
             auto shape = [&](size_t k, int& rows, int& cols, int& ell) {
                 rows = 2 * lb.bounds[k].first;
                 cols = 2 * lb.bounds[k].second;
                 ell = std::min(std::min(lb.jobs[k].chi_max + kRsvdOversample, rows), cols);
             };
+            // Working matrix of a job in a mode: M x N, M >= N.
+            auto dims = [&](size_t k, int mode, int& M, int& N) {
+                int rows, cols, ell;
+                shape(k, rows, cols, ell);
+                M = mode != kJacobiRsvd ? std::max(rows, cols) : cols;
+                N = mode != kJacobiRsvd ? std::min(rows, cols) : ell;
+            };
+            const int nj_wave = int(std::min(lb.jobs.size(), j0 + size_t(m->nslots)) - j0);
+            // A shape beyond every cluster's shared memory goes to the staged
+            // kernel (0: no kernel takes it).
+            auto cluster_or_staged = [&](int M, int N, size_t elem, int len) {
+                const int c = choose_cluster(M, N, m->ctx->max_cluster, nj_wave, m->ctx->sm_count, elem, m->batch, len);
+                return c >= 1 ? c : -jacobi_staged_b(len, N, elem, kSmemLimit, nullptr);
+            };
+            auto keys = [&](int M, int N, int& k1, int& k2) {
+                if (m->fp32) {
+                    k1 = cluster_or_staged(M, N, sizeof(float2), M + N);
+                    k2 = cluster_or_staged(M, N, sizeof(double2), M);
+                } else {
+                    k1 = cluster_or_staged(M, N, sizeof(double2), M);
+                    k2 = 0;
+                }
+            };
+            const size_t j1 = j0 + size_t(nj_wave);
+            w.jobs_off = int(plan.jobs.size());
+            w.njobs = nj_wave;
             for (size_t k = j0; k < j1; ++k) {
                 SplitJob J = lb.jobs[k];
                 const int local = int(k - j0);
@@ -638,72 +677,61 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 w.max_rows = std::max(w.max_rows, rows);
                 w.max_cols = std::max(w.max_cols, cols);
                 w.max_ell = std::max(w.max_ell, ell);
-                const int nj_wave = int(j1 - j0);
-                const size_t elem = m->fp32 ? sizeof(float2) : sizeof(double2);
-                // A shape beyond every cluster's shared memory goes to the
-                // staged kernel: group key -b (0: no kernel takes it).
-                auto cluster_or_staged = [&](int M, int N) {
-                    const int c =
-                        choose_cluster(M, N, m->ctx->max_cluster, nj_wave, m->ctx->sm_count, elem, m->batch);
-                    return c >= 1 ? c : -jacobi_staged_b(M, N, elem, kSmemLimit, nullptr);
-                };
-                const int c_exact = cluster_or_staged(std::max(rows, cols), std::min(rows, cols));
-                add(kJacobiExact, c_exact, local);
+                int M, N, k1, k2;
+                dims(k, kJacobiExact, M, N);
+                keys(M, N, k1, k2);
+                add(kJacobiExact, k1, k2, local);
                 if (rs) {
                     w.any_rsvd = true;
-                    add(kJacobiFallback, c_exact, local);
-                    add(kJacobiRsvd, cluster_or_staged(cols, ell), local);
+                    add(kJacobiFallback, k1, k2, local);
+                    dims(k, kJacobiRsvd, M, N);
+                    keys(M, N, k1, k2);
+                    add(kJacobiRsvd, k1, k2, local);
                 }
             }
+            // Launch shape of one phase for the jobs of a group.
+            auto fill = [&](PhaseCfg& pc, int key, int mode, const std::vector<int>& locals, size_t elem, bool with_v) {
+                size_t sm = 0;
+                int bmax = 1, mmax = 1;
+                if (key < 0) {
+                    pc.staged = true;
+                    pc.b = -key;
+                    pc.C = m->ctx->max_cluster;
+                    for (int local : locals) {
+                        int M, N;
+                        dims(j0 + local, mode, M, N);
+                        sm = std::max(sm, size_t(2) * pc.b * size_t(with_v ? M + N : M) * elem);
+                    }
+                    pc.smem = sm;
+                    pc.threads = 32 * std::min(kJacobiStagedThreads / 32, std::max(4, pc.b));
+                    return;
+                }
+                pc.C = key;
+                for (int local : locals) {
+                    int M, N;
+                    dims(j0 + local, mode, M, N);
+                    sm = std::max(sm, jacobi_smem_bytes(with_v ? M + N : M, N, std::max(pc.C, 1), elem));
+                    bmax = std::max(bmax, round_up(N, 4 * std::max(pc.C, 1)) / (2 * std::max(pc.C, 1)));
+                    mmax = std::max(mmax, M);
+                }
+                pc.smem = sm;
+                // Register-resident variant when every job of the group fits it.
+                pc.reg = jacobi_reg_variant(mmax, bmax);
+                pc.threads = 32 * std::min((pc.reg ? kJacobiRegThreads : kJacobiThreads) / 32, std::max(2, bmax));
+            };
             for (auto& g : groups) {
                 Group gr;
-                gr.mode = g.first.first;
-                gr.C = g.first.second;
+                gr.mode = g.first.mode;
                 gr.idx_off = int(plan.idx.size());
                 gr.count = int(g.second.size());
-                const size_t elem = m->fp32 ? sizeof(float2) : sizeof(double2);
-                if (gr.C < 0) {
-                    gr.staged = true;
-                    gr.b = -gr.C;
-                    gr.C = m->ctx->max_cluster;
-                    size_t sm = 0;
-                    for (int local : g.second) {
-                        int rows, cols, ell;
-                        shape(j0 + local, rows, cols, ell);
-                        const int M = gr.mode != kJacobiRsvd ? std::max(rows, cols) : cols;
-                        sm = std::max(sm, size_t(2) * gr.b * size_t(M) * elem);
-                    }
-                    gr.smem = sm;
-                    gr.threads = 32 * std::min(kJacobiStagedThreads / 32, std::max(4, gr.b));
-                    for (int local : g.second) plan.idx.push_back(local);
-                    w.groups.push_back(gr);
-                    continue;
+                if (m->fp32) {
+                    gr.nph = 2;
+                    fill(gr.ph[0], g.first.k1, gr.mode, g.second, sizeof(float2), true);
+                    fill(gr.ph[1], g.first.k2, gr.mode, g.second, sizeof(double2), false);
+                } else {
+                    gr.nph = 1;
+                    fill(gr.ph[0], g.first.k1, gr.mode, g.second, sizeof(double2), false);
                 }
-                // shared memory for the largest job of the group
-                size_t sm = 0;
-                for (int local : g.second) {
-                    int rows, cols, ell;
-                    shape(j0 + local, rows, cols, ell);
-                    const size_t sz = gr.mode != kJacobiRsvd
-                                          ? jacobi_smem_bytes(std::max(rows, cols), std::min(rows, cols), std::max(gr.C, 1),
-                                                              m->fp32 ? sizeof(float2) : sizeof(double2))
-                                          : jacobi_smem_bytes(cols, ell, std::max(gr.C, 1),
-                                                              m->fp32 ? sizeof(float2) : sizeof(double2));
-                    sm = std::max(sm, sz);
-                }
-                gr.smem = sm;
-                int bmax = 1, mmax = 1;
-                for (int local : g.second) {
-                    int rows, cols, ell;
-                    shape(j0 + local, rows, cols, ell);
-                    const int N = gr.mode != kJacobiRsvd ? std::min(rows, cols) : ell;
-                    const int Cc = std::max(gr.C, 1);
-                    bmax = std::max(bmax, round_up(N, 4 * Cc) / (2 * Cc));
-                    mmax = std::max(mmax, gr.mode != kJacobiRsvd ? std::max(rows, cols) : cols);
-                }
-                // Register-resident variant when every job of the group fits it.
-                gr.reg = jacobi_reg_variant(mmax, bmax);
-                gr.threads = 32 * std::min((gr.reg ? kJacobiRegThreads : kJacobiThreads) / 32, std::max(2, bmax));
                 for (int local : g.second) plan.idx.push_back(local);
                 w.groups.push_back(gr);
             }
@@ -799,10 +827,8 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
         }
         const SplitJob* d_jobs = d_jobs_all + w.jobs_off;
         const int nj = w.njobs;
-        // Precision form: singular values under 1e-5 of the largest are the
-        // complex64 Jacobi's rounding noise (zero columns come out at ~1e-6
-        // of the norm), far above the 1e-12 cut, so they count as zero.
-        const double noise_rel = m->fp32 ? 1e-5 : 0.0;
+        // Both forms end on FP64 columns: no singular value is FP32 noise.
+        const double noise_rel = 0.0;
         {
             Timed t(m, 1);
             prepare_kernel<<<(nj + 127) / 128, 128, 0, m->stream>>>(d_jobs, m->d_state, nj, m->dev);
@@ -811,38 +837,59 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
             merge_gate_kernel<<<g, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);
             count_launch(m, 1);
         }
+        auto launch_phase = [&](const Group& gr, const PhaseCfg& pc, int mode, int phase, bool fp32,
+                                cudaStream_t on) -> wqc_status {
+            if (pc.C < 1) return fail(WQC_ERR_INVALID, "two-site matrix too large for the cluster-resident Jacobi SVD");
+            Timed t(m, 0, on);
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(gr.count * pc.C);
+            cfg.blockDim = dim3(pc.threads);
+            cfg.dynamicSmemBytes = pc.smem;
+            cfg.stream = on;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = pc.C;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            if (pc.staged)
+                CUDA_TRY(launch_jacobi_staged(fp32, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off, mode, phase,
+                                              kMaxSweeps, pc.b, m->d_status, m->d_counters));
+            else
+                CUDA_TRY(launch_jacobi(fp32, pc.reg, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off, mode,
+                                       phase, kMaxSweeps, m->d_status, m->d_counters));
+            count_launch(m, 0);
+            return WQC_OK;
+        };
         auto jacobi = [&](int mode, cudaStream_t on) -> wqc_status {
             bool any = false;
             for (const Group& gr : w.groups) {
                 if (gr.mode != mode) continue;
                 any = true;
-                if (gr.C < 1)
-                    return fail(WQC_ERR_INVALID, "two-site matrix too large for the cluster-resident Jacobi SVD");
-                Timed t(m, 0, on);
-                cudaLaunchConfig_t cfg = {};
-                cfg.gridDim = dim3(gr.count * gr.C);
-                cfg.blockDim = dim3(gr.threads);
-                cfg.dynamicSmemBytes = gr.smem;
-                cfg.stream = on;
-                cudaLaunchAttribute attr[1];
-                attr[0].id = cudaLaunchAttributeClusterDimension;
-                attr[0].val.clusterDim.x = gr.C;
-                attr[0].val.clusterDim.y = 1;
-                attr[0].val.clusterDim.z = 1;
-                cfg.attrs = attr;
-                cfg.numAttrs = 1;
-                if (gr.staged)
-                    CUDA_TRY(launch_jacobi_staged(m->fp32, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off,
-                                                  mode, kMaxSweeps, gr.b, m->d_status, m->d_counters));
-                else
-                    CUDA_TRY(launch_jacobi(m->fp32, gr.reg, cfg, d_jobs, m->d_state, m->d_slots, d_idx + gr.idx_off, mode,
-                                           kMaxSweeps, m->d_status, m->d_counters));
-                count_launch(m, 0);
+                if (gr.nph == 1) {
+                    if (wqc_status s = launch_phase(gr, gr.ph[0], mode, kPhasePlain, false, on)) return s;
+                } else if (wqc_status s = launch_phase(gr, gr.ph[0], mode, kPhaseFp32V, true, on)) {
+                    return s;
+                }
             }
-            if (any) {
+            if (!any) return WQC_OK;
+            if (m->fp32) {
+                // G = V^H V, V' = V (3 I - G) / 2, X V' for every job of the mode, then the FP64 finish.
+                Timed t(m, 0, on);
+                const int side = std::max(w.max_rows, w.max_cols);
+                const dim3 g((side + 31) / 32, (side + 31) / 32, nj);
+                for (int stage = 0; stage < 3; ++stage) {
+                    precond_gemm_kernel<<<g, 256, 0, on>>>(d_jobs, m->d_state, m->d_slots, mode, stage);
+                    count_launch(m, 0);
+                }
+            }
+            for (const Group& gr : w.groups)
+                if (gr.mode == mode && gr.nph == 2)
+                    if (wqc_status s = launch_phase(gr, gr.ph[1], mode, kPhaseFinish, false, on)) return s;
+            {
                 Timed t(m, 4, on);
-                svd_probe_kernel<<<dim3(nj, 2), 256, 0, on>>>(d_jobs, m->d_state, m->d_slots, mode, m->fp32 ? 1 : 0,
-                                                               m->d_status);
+                svd_probe_kernel<<<dim3(nj, 2), 256, 0, on>>>(d_jobs, m->d_state, m->d_slots, mode, 0, m->d_status);
                 count_launch(m, 4);
             }
             return WQC_OK;
@@ -1157,9 +1204,15 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     const int R = 2 * chi_cap, E = std::min(chi_cap + kRsvdOversample, R);
     // theta, w, z + range finder + tau (+ the staged Jacobi's workspace when a
     // two-site matrix can exceed a cluster's shared memory)
-    const size_t el = precision == WQC_PRECISION_FP32 ? sizeof(float2) : sizeof(double2);
-    const bool staged = choose_cluster(R, R, ctx->max_cluster, 1, ctx->sm_count, el, false) < 1 ||
-                        choose_cluster(R, E, ctx->max_cluster, 1, ctx->sm_count, el, false) < 1;
+    // The staged Jacobi's workspace holds (R + 32) x R complex128 values: the
+    // padded FP64 columns, or the precision form's complex64 columns with V
+    // under them ((R + 32) x 2R complex64 values, the same bytes).
+    const bool fp32 = precision == WQC_PRECISION_FP32;
+    auto no_cluster = [&](int M, int N) {
+        return choose_cluster(M, N, ctx->max_cluster, 1, ctx->sm_count, sizeof(double2), false) < 1 ||
+               (fp32 && choose_cluster(M, N, ctx->max_cluster, 1, ctx->sm_count, sizeof(float2), false, M + N) < 1);
+    };
+    const bool staged = no_cluster(R, R) || no_cluster(R, E);
     const size_t gs_c = staged ? jacobi_staged_elems(R) : 0;
     const size_t slot_c = size_t(R) * R * 3 + size_t(R) * E * 6 + E + gs_c;
     const size_t slot_bytes = ((slot_c * sizeof(double2) + size_t(R) * (sizeof(double) + sizeof(int)) + 4095) / 4096) * 4096;
@@ -1961,10 +2014,11 @@ wqc_status wqc_mps_kernel_stats(wqc_mps* m, wqc_kernel_stats* out) {
         m->event_pool.push_back(e.second.second);
     }
     m->events.clear();
-    unsigned long long c[2] = {0, 0};
+    unsigned long long c[3] = {0, 0, 0};
     CUDA_TRY(cudaMemcpy(c, m->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
     m->stats.jacobi_tasks = c[0];
     m->stats.jacobi_sweeps = c[1];
+    m->stats.jacobi_sweeps_first = c[2];
     *out = m->stats;
     return WQC_OK;
 }
@@ -1978,7 +2032,7 @@ void wqc_mps_reset_stats(wqc_mps* m) {
     }
     m->events.clear();
     m->stats = wqc_kernel_stats{};
-    cudaMemset(m->d_counters, 0, 2 * sizeof(unsigned long long));
+    cudaMemset(m->d_counters, 0, 3 * sizeof(unsigned long long));
 }
 
 void* wqc_mps_stream(wqc_mps* m) { return m ? static_cast<void*>(m->stream) : nullptr; }

@@ -721,8 +721,9 @@ __device__ __forceinline__ int jacobi_rotate(T* __restrict__ xp, T* __restrict__
 constexpr int kJacobiRegRows = 8;
 
 template <typename T>
-__device__ __forceinline__ int jacobi_rotate_reg(T (&u)[kJacobiRegRows], T* __restrict__ xq, int M, double tol,
-                                                 double noise_floor, int lane, double& relmax) {
+__device__ __forceinline__ int jacobi_rotate_reg(T (&u)[kJacobiRegRows], T* __restrict__ xq, int M, int len,
+                                                 T* __restrict__ xp_tail, double tol, double noise_floor, int lane,
+                                                 double& relmax) {
     using R = typename JacobiReal<T>::R;
     T v[kJacobiRegRows];
 #pragma unroll
@@ -772,6 +773,18 @@ __device__ __forceinline__ int jacobi_rotate_reg(T (&u)[kJacobiRegRows], T* __re
             u[k] = p;
             xq[r] = q;
         }
+    }
+    // Rows M .. len-1 (the right rotations accumulated in the precision
+    // form's first phase) stay in shared memory for both columns.
+    for (int r = M + lane; r < len; r += 32) {
+        const T x = xp_tail[r], y = xq[r];
+        T p, q;
+        p.x = fma(cr, x.x, -fma(wr, y.x, wi * y.y));
+        p.y = fma(cr, x.y, -fma(wr, y.y, -wi * y.x));
+        q.x = fma(wr, x.x, fma(-wi, x.y, cr * y.x));
+        q.y = fma(wr, x.y, fma(wi, x.x, cr * y.y));
+        xp_tail[r] = p;
+        xq[r] = q;
     }
     return 1;
 }
@@ -833,10 +846,8 @@ __device__ __forceinline__ double2 to_f64(float2 x) { return make_double2(x.x, x
 
 template <typename T, bool kReg>
 __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jacobi_cluster_kernel(
-    const SplitJob* jobs, const SplitState* st,
-                                                                          const SlotBuffers* slots, const int* idx,
-                                                                          int mode, int max_sweeps, int* status,
-                                                                          unsigned long long* counters) {
+    const SplitJob* jobs, SplitState* st, const SlotBuffers* slots, const int* idx, int mode, int phase,
+    int max_sweeps, int* status, unsigned long long* counters) {
     constexpr bool kF64 = sizeof(T) == sizeof(double2);
     cg::cluster_group cluster = cg::this_cluster();
     const int C = int(cluster.num_blocks());
@@ -854,7 +865,11 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
     const int quantum = 4 * C;
     const int Np = ((N + quantum - 1) / quantum) * quantum;
     const int b = Np / (2 * C);
-    const int len = M;  // W only: the other side's vectors are recovered from W after the SVD
+    // W only, the other side's vectors are recovered from W after the SVD;
+    // the precision form's first phase also carries V (N rows under W).
+    const int vrows = phase == kPhaseFp32V ? N : 0;
+    const int len = M + vrows;
+    const bool colmajor = rows_of_src || phase == kPhaseFinish;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
@@ -877,7 +892,11 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
     auto bot_buf_of = [&](int r, int k) { return r == 0 ? 1 : (4 - k % 3) % 3; };
     auto spare_buf_of = [&](int k) { return (5 - k % 3) % 3; };
     // Frobenius norm over the columns this CTA loads, then over the cluster.
+    // The precision form's finishing phase starts from X V (column-major in
+    // the slot's W buffer), formed from the dust-zeroed X.
+    const double2* wsrc = Bf.w;
     auto src_at = [&](int i, int col) -> double2 {
+        if (phase == kPhaseFinish) return wsrc[size_t(col) * M + i];
         return rows_of_src ? cconj(src[size_t(col) * ld + i]) : src[size_t(i) * ld + col];
     };
     double part = 0;
@@ -885,7 +904,7 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
         const int id = half == 0 ? rank : 2 * C - 1 - rank;
         for (int e = tid; e < b * M; e += nthreads) {
             int c, i;
-            if (rows_of_src) { c = e / M; i = e % M; } else { i = e / b; c = e % b; }
+            if (colmajor) { c = e / M; i = e % M; } else { i = e / b; c = e % b; }
             const int col = id * b + c;
             if (col < N) part += cnorm2(src_at(i, col));
         }
@@ -912,12 +931,16 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
         T* base = buf(half);
         for (int e = tid; e < b * M; e += nthreads) {
             int c, i;
-            if (rows_of_src) { c = e / M; i = e % M; } else { i = e / b; c = e % b; }
+            if (colmajor) { c = e / M; i = e % M; } else { i = e / b; c = e % b; }
             const int col = id * b + c;
             double2 x = col < N ? src_at(i, col) : cmake(0, 0);
-            if (cnorm2(x) < dust2) x = cmake(0, 0);
+            if (phase != kPhaseFinish && cnorm2(x) < dust2) x = cmake(0, 0);
             chk_in += cnorm2(x);
             base[size_t(c) * len + i] = to_store<T>(x);
+        }
+        for (int e = tid; e < b * vrows; e += nthreads) {  // V = I (padding columns: zero)
+            const int c = e / vrows, i = e % vrows;
+            base[size_t(c) * len + M + i] = to_store<T>(cmake(id * b + c == i ? 1.0 : 0.0, 0.0));
         }
     }
     __syncthreads();
@@ -978,8 +1001,8 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
                 }
                 for (int k = 0; k < b; ++k) {
                     if (wid < b)
-                        my_rot += jacobi_rotate_reg(u, bb + size_t((wid + k) % b) * len, M, tol, noise_floor, lane,
-                                                    my_rel);
+                        my_rot += jacobi_rotate_reg(u, bb + size_t((wid + k) % b) * len, M, len, col, tol,
+                                                    noise_floor, lane, my_rel);
                     __syncthreads();
                 }
                 if (wid < b) {
@@ -1071,8 +1094,24 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
                 status[4] = int(bits & 0xffffffffull);
             }
         }
-        atomicAdd(counters + 0, 1ull);
-        atomicAdd(counters + 1, (unsigned long long)(converged ? sweep + 1 : sweep));
+        if (phase != kPhaseFp32V) atomicAdd(counters + 0, 1ull);
+        atomicAdd(counters + (phase == kPhaseFp32V ? 2 : 1), (unsigned long long)(converged ? sweep + 1 : sweep));
+    }
+    if (phase == kPhaseFp32V) {
+        // The accumulated V (FP64) for the finishing phase, and ||X||_F^2
+        // for its dust zeroing of X.
+        for (int half = 0; half < 2; ++half) {
+            const int id = circle_at(half == 0 ? rank : 2 * C - 1 - rank, xk, 2 * C);
+            const T* base = buf(half == 0 ? top_buf_of(rank, xk) : bot_buf_of(rank, xk));
+            for (int c = wid; c < b; c += nwarps) {
+                const int col = id * b + c;
+                if (col >= N) continue;
+                for (int r = lane; r < N; r += 32) Bf.z[size_t(col) * N + r] = to_f64(base[size_t(c) * len + M + r]);
+            }
+        }
+        if (rank == 0 && tid == 0) st[j].fro2 = fro2;
+        cluster.sync();  // no CTA leaves while another may still read its shared memory
+        return;
     }
     // Write back: W columns and column norms.
     for (int half = 0; half < 2; ++half) {
@@ -1135,10 +1174,10 @@ __global__ void __launch_bounds__(kReg ? kJacobiRegThreads : kJacobiThreads) jac
 // outputs are those of jacobi_cluster_kernel.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(const SplitJob* jobs, const SplitState* st,
+__global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(const SplitJob* jobs, SplitState* st,
                                                                          const SlotBuffers* slots, const int* idx,
-                                                                         int mode, int max_sweeps, int b, int* status,
-                                                                         unsigned long long* counters) {
+                                                                         int mode, int phase, int max_sweeps, int b,
+                                                                         int* status, unsigned long long* counters) {
     constexpr bool kF64 = sizeof(T) == sizeof(double2);
     cg::cluster_group cluster = cg::this_cluster();
     const int C = int(cluster.num_blocks());
@@ -1156,7 +1195,8 @@ __global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(con
     const int K = (N + 2 * b - 1) / (2 * b);
     const int nblk = 2 * K;
     const int Np = nblk * b;
-    const int len = M;  // W only, as in jacobi_cluster_kernel
+    const int vrows = phase == kPhaseFp32V ? N : 0;  // as in jacobi_cluster_kernel
+    const int len = M + vrows;
     const size_t blk = size_t(b) * len;
     T* G = reinterpret_cast<T*>(Bf.gs);
     if (G == nullptr) {  // a state sized without the workspace (uniform over the cluster)
@@ -1172,7 +1212,9 @@ __global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(con
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int nthreads = blockDim.x;
     const int nwarps = nthreads / 32;
+    const double2* wsrc = Bf.w;
     auto src_at = [&](int i, int col) -> double2 {
+        if (phase == kPhaseFinish) return wsrc[size_t(col) * M + i];
         return rows_of_src ? cconj(src[size_t(col) * ld + i]) : src[size_t(i) * ld + col];
     };
     if (tid == 0) ctl.rot = 0;
@@ -1197,12 +1239,13 @@ __global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(con
     double chk_in = 0, chk_out = 0;
     for (int col = rank; col < Np; col += C) {
         T* x = G + size_t(col) * len;
-        for (int i = tid; i < len; i += nthreads) {
+        for (int i = tid; i < M; i += nthreads) {
             double2 v = col < N ? src_at(i, col) : cmake(0, 0);
-            if (cnorm2(v) < dust2) v = cmake(0, 0);
+            if (phase != kPhaseFinish && cnorm2(v) < dust2) v = cmake(0, 0);
             chk_in += cnorm2(v);
             x[i] = to_store<T>(v);
         }
+        for (int i = tid; i < vrows; i += nthreads) x[M + i] = to_store<T>(cmake(col == i ? 1.0 : 0.0, 0.0));
     }
     __threadfence();
     cluster.sync();
@@ -1299,8 +1342,15 @@ __global__ void __launch_bounds__(kJacobiStagedThreads) jacobi_staged_kernel(con
                 status[4] = int(bits & 0xffffffffull);
             }
         }
-        atomicAdd(counters + 0, 1ull);
-        atomicAdd(counters + 1, (unsigned long long)(converged ? sweep + 1 : sweep));
+        if (phase != kPhaseFp32V) atomicAdd(counters + 0, 1ull);
+        atomicAdd(counters + (phase == kPhaseFp32V ? 2 : 1), (unsigned long long)(converged ? sweep + 1 : sweep));
+    }
+    if (phase == kPhaseFp32V) {  // V (FP64) and ||X||_F^2 for the finishing phase
+        for (int col = rank + C * wid; col < N; col += C * nwarps)
+            for (int r = lane; r < N; r += 32) Bf.z[size_t(col) * N + r] = to_f64(__ldcg(G + size_t(col) * len + M + r));
+        if (rank == 0 && tid == 0) st[j].fro2 = fro2;
+        cluster.sync();
+        return;
     }
     // Write back W and the column norms; CTA r takes columns r, r+C, ...,
     // one warp per column.
@@ -1438,6 +1488,79 @@ __global__ void __launch_bounds__(256) svd_probe_kernel(const SplitJob* jobs, co
         const double tol = fp32 ? 1e-4 : 1e-9;  // the Frobenius check's tolerance of each form
         if (!(sqrt(e2) <= tol * sqrt(fro2) * sqrt(double(N)) + 1e-14)) atomicOr(status, kStatusSvdCheck);
     }
+}
+
+// ---------------------------------------------------------------------------
+// The precision form's FP64 products between its Jacobi phases (see
+// split_kernels.cuh): 32 x 32 tiles, batched over the wave's jobs.  G lives
+// in the slot's omega and y0 buffers and V' in zr and y (each pair holds
+// 2 R ell >= R^2 entries); none of them is in use while an SVD of the job
+// runs.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) precond_gemm_kernel(const SplitJob* jobs, const SplitState* st,
+                                                           const SlotBuffers* slots, int mode, int stage) {
+    const int j = blockIdx.z;
+    const SplitState S = st[j];
+    if (!jacobi_active(S, mode)) return;
+    const SplitJob& J = jobs[j];
+    const SlotBuffers B = slots[J.slot];
+    const double2* src;
+    int sr, sc, ld, rows_of_src;
+    jacobi_task(J, S, B, mode, src, sr, sc, ld, rows_of_src);
+    const int M = rows_of_src ? sc : sr, N = rows_of_src ? sr : sc;
+    const int m = stage == 2 ? M : N, n = N, k = N;
+    const int i0 = blockIdx.y * kGemmT, n0 = blockIdx.x * kGemmT;
+    if (i0 >= m || n0 >= n) return;
+    const double2* V = B.z;
+    double2* G = B.omega;
+    double2* V2 = B.zr;
+    const double dust2 = kDustRel * kDustRel * S.fro2;
+    auto a_at = [&](int i, int kk) -> double2 {
+        if (stage == 0) return cconj(V[size_t(i) * N + kk]);  // V^H
+        if (stage == 1) return V[size_t(kk) * N + i];
+        const double2 x = rows_of_src ? cconj(src[size_t(kk) * ld + i]) : src[size_t(i) * ld + kk];
+        return cnorm2(x) < dust2 ? cmake(0, 0) : x;  // X, dust-zeroed as the first phase loaded it
+    };
+    auto b_at = [&](int kk, int jj) -> double2 {
+        if (stage == 0) return V[size_t(jj) * N + kk];
+        if (stage == 1) {
+            const double2 g = G[size_t(jj) * N + kk];
+            return cmake((kk == jj ? 1.5 : 0.0) - 0.5 * g.x, -0.5 * g.y);
+        }
+        return V2[size_t(jj) * N + kk];
+    };
+    __shared__ double2 As[kGemmT][kGemmK + 1];
+    __shared__ double2 Bs[kGemmK][kGemmT + 1];
+    const int tid = threadIdx.x, tr = tid / 16, tc = tid % 16;
+    double2 acc[2][2] = {{cmake(0, 0), cmake(0, 0)}, {cmake(0, 0), cmake(0, 0)}};
+    for (int k0 = 0; k0 < k; k0 += kGemmK) {
+        for (int e = tid; e < kGemmT * kGemmK; e += 256) {
+            const int r = e / kGemmK, c = e % kGemmK;
+            As[r][c] = (i0 + r < m && k0 + c < k) ? a_at(i0 + r, k0 + c) : cmake(0, 0);
+        }
+        for (int e = tid; e < kGemmK * kGemmT; e += 256) {
+            const int r = e / kGemmT, c = e % kGemmT;
+            Bs[r][c] = (k0 + r < k && n0 + c < n) ? b_at(k0 + r, n0 + c) : cmake(0, 0);
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int c = 0; c < kGemmK; ++c) {
+            const double2 a0 = As[tr][c], a1 = As[tr + 16][c];
+            const double2 b0 = Bs[c][tc], b1 = Bs[c][tc + 16];
+            cfma(acc[0][0], a0, b0);
+            cfma(acc[0][1], a0, b1);
+            cfma(acc[1][0], a1, b0);
+            cfma(acc[1][1], a1, b1);
+        }
+        __syncthreads();
+    }
+    double2* C = stage == 0 ? G : stage == 1 ? V2 : B.w;
+    const int ldc = stage == 2 ? M : N;
+    for (int x = 0; x < 2; ++x)
+        for (int y = 0; y < 2; ++y) {
+            const int i = i0 + tr + 16 * x, jj = n0 + tc + 16 * y;
+            if (i < m && jj < n) C[size_t(jj) * ldc + i] = acc[x][y];
+        }
 }
 
 // ---------------------------------------------------------------------------
@@ -1688,29 +1811,29 @@ const void* jacobi_staged(bool fp32) {
                 : reinterpret_cast<const void*>(jacobi_staged_kernel<double2>);
 }
 
-cudaError_t launch_jacobi_staged(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
-                                 const SplitState* st, const SlotBuffers* slots, const int* idx, int mode,
-                                 int max_sweeps, int b, int* status, unsigned long long* counters) {
+cudaError_t launch_jacobi_staged(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, SplitState* st,
+                                 const SlotBuffers* slots, const int* idx, int mode, int phase, int max_sweeps, int b,
+                                 int* status, unsigned long long* counters) {
     if (fp32)
-        return cudaLaunchKernelEx(&cfg, jacobi_staged_kernel<float2>, jobs, st, slots, idx, mode, max_sweeps, b,
+        return cudaLaunchKernelEx(&cfg, jacobi_staged_kernel<float2>, jobs, st, slots, idx, mode, phase, max_sweeps, b,
                                   status, counters);
-    return cudaLaunchKernelEx(&cfg, jacobi_staged_kernel<double2>, jobs, st, slots, idx, mode, max_sweeps, b, status,
-                              counters);
+    return cudaLaunchKernelEx(&cfg, jacobi_staged_kernel<double2>, jobs, st, slots, idx, mode, phase, max_sweeps, b,
+                              status, counters);
 }
 
-cudaError_t launch_jacobi(bool fp32, bool reg, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
-                          const SplitState* st, const SlotBuffers* slots, const int* idx, int mode, int max_sweeps,
-                          int* status, unsigned long long* counters) {
+cudaError_t launch_jacobi(bool fp32, bool reg, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, SplitState* st,
+                          const SlotBuffers* slots, const int* idx, int mode, int phase, int max_sweeps, int* status,
+                          unsigned long long* counters) {
     if (fp32 && reg)
-        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<float2, true>, jobs, st, slots, idx, mode, max_sweeps,
-                                  status, counters);
+        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<float2, true>, jobs, st, slots, idx, mode, phase,
+                                  max_sweeps, status, counters);
     if (fp32)
-        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<float2, false>, jobs, st, slots, idx, mode, max_sweeps,
-                                  status, counters);
+        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<float2, false>, jobs, st, slots, idx, mode, phase,
+                                  max_sweeps, status, counters);
     if (reg)
-        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<double2, true>, jobs, st, slots, idx, mode, max_sweeps,
-                                  status, counters);
-    return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<double2, false>, jobs, st, slots, idx, mode, max_sweeps,
-                              status, counters);
+        return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<double2, true>, jobs, st, slots, idx, mode, phase,
+                                  max_sweeps, status, counters);
+    return cudaLaunchKernelEx(&cfg, jacobi_cluster_kernel<double2, false>, jobs, st, slots, idx, mode, phase,
+                              max_sweeps, status, counters);
 }
 }  // namespace wqc

@@ -42,15 +42,26 @@ inline size_t qr_cluster_smem_bytes(int m, int n, int C, bool global_cols = fals
 // in the plain form, complex64 in the precision form), reached from other
 // files through these host functions.
 const void* jacobi_kernel(bool fp32, bool reg);
-cudaError_t launch_jacobi(bool fp32, bool reg, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
-                          const SplitState* st, const SlotBuffers* slots, const int* idx, int mode, int max_sweeps,
-                          int* status, unsigned long long* counters);
+// Phases of a Jacobi SVD: the plain one; the precision form's first phase
+// (complex64 columns carrying W = X V and the accumulated V, written out as
+// FP64 for the finish); and its finishing phase (FP64 sweeps that start from
+// X V, formed in FP64 by precond_gemm_kernel).
+enum { kPhasePlain = 0, kPhaseFp32V = 1, kPhaseFinish = 2 };
+cudaError_t launch_jacobi(bool fp32, bool reg, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, SplitState* st,
+                          const SlotBuffers* slots, const int* idx, int mode, int phase, int max_sweeps, int* status,
+                          unsigned long long* counters);
 // The staged variant for working matrices beyond a cluster's shared memory:
 // columns in the slot's `gs` workspace, blocks of b columns (b even).
 const void* jacobi_staged(bool fp32);
-cudaError_t launch_jacobi_staged(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs,
-                                 const SplitState* st, const SlotBuffers* slots, const int* idx, int mode,
-                                 int max_sweeps, int b, int* status, unsigned long long* counters);
+cudaError_t launch_jacobi_staged(bool fp32, const cudaLaunchConfig_t& cfg, const SplitJob* jobs, SplitState* st,
+                                 const SlotBuffers* slots, const int* idx, int mode, int phase, int max_sweeps, int b,
+                                 int* status, unsigned long long* counters);
+// The precision form's FP64 products between its two Jacobi phases, for the
+// jobs active in `mode`: stage 0, G = V^H V; stage 1, V' = V (3 I - G) / 2
+// (one Newton-Schulz step: orthonormal to FP64 rounding); stage 2, X V'
+// into the slot's W buffer, X dust-zeroed as the first phase loaded it.
+__global__ void precond_gemm_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots, int mode,
+                                    int stage);
 // Shape of the staged Jacobi for an M x N working matrix on a cluster of C
 // CTAs: the block width b <= 16 whose two blocks fit `smem_limit` and whose
 // sweep is shortest, counted in dependent rotation rounds: (2K-1) steps of

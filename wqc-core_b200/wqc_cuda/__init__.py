@@ -76,6 +76,7 @@ class KernelStats(ctypes.Structure):
         ("d2h_bytes", ctypes.c_uint64),
         ("jacobi_tasks", ctypes.c_uint64),
         ("jacobi_sweeps", ctypes.c_uint64),
+        ("jacobi_sweeps_first", ctypes.c_uint64),
     ]
 
 
@@ -465,6 +466,7 @@ class CudaMps:
             "d2h_bytes": int(st.d2h_bytes),
             "jacobi_tasks": int(st.jacobi_tasks),
             "jacobi_sweeps": int(st.jacobi_sweeps),
+            "jacobi_sweeps_first": int(st.jacobi_sweeps_first),
         }
 
     def reset_stats(self) -> None:
