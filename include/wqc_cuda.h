@@ -80,6 +80,21 @@ WQC_API void wqc_cuda_last_oom(uint64_t* required, uint64_t* available);
 WQC_API wqc_status wqc_cuda_open(int device, wqc_cuda_ctx** out);
 WQC_API void wqc_cuda_close(wqc_cuda_ctx* ctx);
 
+/* Measure the Jacobi SVD's cluster size for the saturated shapes of chi_max
+ * 16, 32, 64 and 128 (plain form and the precision form's first phase; one
+ * latency-bound split and a 32-split batch), or load the measurement from
+ * `cache_path` (NULL: $WQC_TUNE_PATH, else $XDG_CACHE_HOME or ~/.cache,
+ * /wqc/jacobi-clusters) when its first line matches this machine's
+ * fingerprint (device name, SM count, compute capability, driver and
+ * runtime versions).  A fresh measurement is written back there.  States
+ * created on `ctx` afterwards use the measured sizes for those shapes and
+ * the cost model for the rest.  The calibration-plus-cache pattern of the
+ * reference's GEMM side (src/tn/gpu/gemm.rs:495-543, 649-702); budget_seconds
+ * > 0 stops measuring once spent.  *entries (nullable) receives the number
+ * of tuned shapes. */
+WQC_API wqc_status wqc_cuda_autotune(wqc_cuda_ctx* ctx, const char* cache_path, double budget_seconds,
+                                     uint32_t* entries);
+
 /* Device memory for /sysinfo's vram_budget_bytes (engine_status.rs:105-117)
  * and the SM count.  Any out pointer may be NULL. */
 WQC_API wqc_status wqc_cuda_device_info(wqc_cuda_ctx* ctx, uint64_t* total_bytes, uint64_t* free_bytes, int32_t* sm_count);

@@ -8,8 +8,11 @@
 // the host only tracks upper bounds to size launches.
 #include <cuda_runtime.h>
 
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -51,6 +54,7 @@ wqc_status fail_oom(uint64_t required, uint64_t available) {
 
 constexpr int kMaxSweeps = 60;
 constexpr int kDenseMaxQubits = 28;  // 2^28 complex128 = 4 GiB on the host
+constexpr size_t kSlotBudget = size_t(2) << 30;  // split workspace per chi_max bucket
 constexpr size_t kSmemLimit = 232448 - 1024;  // 227 KB opt-in per block, minus static shared memory
 
 struct Mat2 {
@@ -193,6 +197,14 @@ struct wqc_cuda_ctx {
     int sm_count = 0;
     int max_cluster = 8;
     std::mutex mu;
+    // Jacobi cluster sizes measured by wqc_cuda_autotune, by working-matrix
+    // shape (M x N, rows stored per column, bytes per complex entry) and by
+    // kind of wave (one latency-bound split, or a throughput-bound batch).
+    struct Tuned {
+        int M, N, len, elem, throughput, C;
+    };
+    std::vector<Tuned> tuned;
+    int force_C = 0;  // set by the tuner while it measures one cluster size
 };
 
 struct wqc_mps {
@@ -219,6 +231,15 @@ struct wqc_mps {
     int* d_cancel = nullptr;
     // split workspace
     int nslots = 0;
+    // Slots come in buckets, one per distinct chi_max of the slices, each
+    // slot sized for its bucket's largest two-site matrix (R = 2 chi_max).
+    std::vector<int> bucket_chi, bucket_base, bucket_cap;
+    std::vector<int> slot_R, slot_E;
+    int bucket_of(int chi) const {
+        for (size_t b = 0; b < bucket_chi.size(); ++b)
+            if (bucket_chi[b] == chi) return int(b);
+        return 0;
+    }
     char* slot_pool = nullptr;
     SlotBuffers* d_slots = nullptr;
     SplitState* d_state = nullptr;
@@ -336,8 +357,17 @@ bool jacobi_reg_variant(int M, int b) { return M <= kJacobiRegMaxRows && b <= kJ
 
 // len: rows stored per column (M, or M + N when the precision form's first
 // phase carries V).
-int choose_cluster(int M, int N, int max_c, int njobs, int sm_count, size_t elem, bool throughput, int len = 0) {
+int choose_cluster(const wqc_cuda_ctx* ctx, int M, int N, int max_c, int njobs, int sm_count, size_t elem,
+                   bool throughput, int len = 0) {
     if (len <= 0) len = M;
+    if (ctx) {
+        auto fits = [&](int Cc) { return Cc >= 1 && Cc <= max_c && jacobi_smem_bytes(len, N, Cc, elem) <= kSmemLimit; };
+        if (ctx->force_C > 0 && fits(ctx->force_C)) return ctx->force_C;
+        for (const auto& t : ctx->tuned)
+            if (t.M == M && t.N == N && t.len == len && t.elem == int(elem) && t.throughput == int(throughput) &&
+                fits(t.C))
+                return t.C;
+    }
     int best = -1;
     double best_cost = 1e300;
     for (int Cc = 1; Cc <= max_c; ++Cc) {
@@ -595,7 +625,8 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
     plan.slice_last_wave.assign(m->seg_first.size(), -1);
     for (LevelBuild& lb : levels) {
         // one-qubit ops run first, in one wave with no splits when needed
-        size_t j0 = 0;
+        std::vector<char> taken(lb.jobs.size(), 0);
+        size_t remaining = lb.jobs.size();
         bool first = true;
         do {
             Wave w;
@@ -642,11 +673,28 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 M = mode != kJacobiRsvd ? std::max(rows, cols) : cols;
                 N = mode != kJacobiRsvd ? std::min(rows, cols) : ell;
             };
-            const int nj_wave = int(std::min(lb.jobs.size(), j0 + size_t(m->nslots)) - j0);
+            // The wave takes the level's next jobs while their bucket has a
+            // free slot (every job of a level is independent of the others).
+            std::vector<size_t> sel;
+            std::vector<int> sel_slot;
+            {
+                std::vector<int> used(m->bucket_chi.size(), 0);
+                for (size_t k = 0; k < lb.jobs.size(); ++k) {
+                    if (taken[k]) continue;
+                    const int bk = m->bucket_of(lb.jobs[k].chi_max);
+                    if (used[bk] >= m->bucket_cap[bk]) continue;
+                    taken[k] = 1;
+                    sel.push_back(k);
+                    sel_slot.push_back(m->bucket_base[bk] + used[bk]++);
+                }
+                remaining -= sel.size();
+            }
+            const int nj_wave = int(sel.size());
             // A shape beyond every cluster's shared memory goes to the staged
             // kernel (0: no kernel takes it).
             auto cluster_or_staged = [&](int M, int N, size_t elem, int len) {
-                const int c = choose_cluster(M, N, m->ctx->max_cluster, nj_wave, m->ctx->sm_count, elem, m->batch, len);
+                const int c =
+                    choose_cluster(m->ctx, M, N, m->ctx->max_cluster, nj_wave, m->ctx->sm_count, elem, m->batch, len);
                 return c >= 1 ? c : -jacobi_staged_b(len, N, elem, kSmemLimit, nullptr);
             };
             auto keys = [&](int M, int N, int& k1, int& k2) {
@@ -658,13 +706,12 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                     k2 = 0;
                 }
             };
-            const size_t j1 = j0 + size_t(nj_wave);
             w.jobs_off = int(plan.jobs.size());
             w.njobs = nj_wave;
-            for (size_t k = j0; k < j1; ++k) {
+            for (int local = 0; local < nj_wave; ++local) {
+                const size_t k = sel[local];
                 SplitJob J = lb.jobs[k];
-                const int local = int(k - j0);
-                J.slot = local;
+                J.slot = sel_slot[local];
                 plan.jobs.push_back(J);
                 plan.slice_last_wave[lb.job_slice[k]] = std::max(plan.slice_last_wave[lb.job_slice[k]], wave_index);
                 int rows, cols, ell;
@@ -699,7 +746,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                     pc.C = m->ctx->max_cluster;
                     for (int local : locals) {
                         int M, N;
-                        dims(j0 + local, mode, M, N);
+                        dims(sel[local], mode, M, N);
                         sm = std::max(sm, size_t(2) * pc.b * size_t(with_v ? M + N : M) * elem);
                     }
                     pc.smem = sm;
@@ -709,7 +756,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 pc.C = key;
                 for (int local : locals) {
                     int M, N;
-                    dims(j0 + local, mode, M, N);
+                    dims(sel[local], mode, M, N);
                     sm = std::max(sm, jacobi_smem_bytes(with_v ? M + N : M, N, std::max(pc.C, 1), elem));
                     bmax = std::max(bmax, round_up(N, 4 * std::max(pc.C, 1)) / (2 * std::max(pc.C, 1)));
                     mmax = std::max(mmax, M);
@@ -736,8 +783,7 @@ void build_plan(wqc_mps* m, const std::vector<Op>& ops, Plan& plan) {
                 w.groups.push_back(gr);
             }
             plan.waves.push_back(std::move(w));
-            j0 = j1;
-        } while (j0 < lb.jobs.size());
+        } while (remaining > 0);
     }
 }
 
@@ -1200,25 +1246,50 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
         return bail(fail(WQC_ERR_CUDA, "event"));
     if (cudaEventCreateWithFlags(&m->stage_done, cudaEventDisableTiming) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "event"));
     cudaEventRecord(m->stage_done, m->stream);
-    // Budget check before any large allocation (mps.rs:36-48 analogue).
-    const int R = 2 * chi_cap, E = std::min(chi_cap + kRsvdOversample, R);
-    // theta, w, z + range finder + tau (+ the staged Jacobi's workspace when a
-    // two-site matrix can exceed a cluster's shared memory)
+    // Split workspace: one bucket of slots per distinct chi_max, each slot
+    // holding theta, w, z, the range finder's buffers and tau for two-site
+    // matrices up to R x R, R = 2 chi_max (plus the staged Jacobi's workspace
+    // when such a matrix can exceed a cluster's shared memory).  A bucket
+    // gets a slot per two sites of its slices, at most kSlotBudget bytes of
+    // them: waves take as many splits of a bucket as it has slots.
     // The staged Jacobi's workspace holds (R + 32) x R complex128 values: the
     // padded FP64 columns, or the precision form's complex64 columns with V
     // under them ((R + 32) x 2R complex64 values, the same bytes).
     const bool fp32 = precision == WQC_PRECISION_FP32;
     auto no_cluster = [&](int M, int N) {
-        return choose_cluster(M, N, ctx->max_cluster, 1, ctx->sm_count, sizeof(double2), false) < 1 ||
-               (fp32 && choose_cluster(M, N, ctx->max_cluster, 1, ctx->sm_count, sizeof(float2), false, M + N) < 1);
+        return choose_cluster(nullptr, M, N, ctx->max_cluster, 1, ctx->sm_count, sizeof(double2), false) < 1 ||
+               (fp32 &&
+                choose_cluster(nullptr, M, N, ctx->max_cluster, 1, ctx->sm_count, sizeof(float2), false, M + N) < 1);
     };
-    const bool staged = no_cluster(R, R) || no_cluster(R, E);
-    const size_t gs_c = staged ? jacobi_staged_elems(R) : 0;
-    const size_t slot_c = size_t(R) * R * 3 + size_t(R) * E * 6 + E + gs_c;
-    const size_t slot_bytes = ((slot_c * sizeof(double2) + size_t(R) * (sizeof(double) + sizeof(int)) + 4095) / 4096) * 4096;
-    m->nslots = nslots_req > 0 ? nslots_req : std::max(1, n / 2);
+    std::vector<size_t> bucket_bytes, bucket_gs;
+    {
+        std::vector<int> cs(chis);
+        std::sort(cs.begin(), cs.end());
+        cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+        m->nslots = 0;
+        for (int c : cs) {
+            const int R = 2 * c, E = std::min(c + kRsvdOversample, R);
+            const bool staged = no_cluster(R, R) || no_cluster(R, E);
+            const size_t gs_c = staged ? jacobi_staged_elems(R) : 0;
+            const size_t slot_c = size_t(R) * R * 3 + size_t(R) * E * 6 + E + gs_c;
+            const size_t bytes = ((slot_c * sizeof(double2) + size_t(R) * (sizeof(double) + sizeof(int)) + 4095) / 4096) * 4096;
+            long count = 0;
+            for (size_t sl = 0; sl < ns.size(); ++sl)
+                if (chis[sl] == c) count += ns[sl] / 2;
+            long cap = std::max<long>(1, std::min<long>(std::max<long>(count, 1), long(kSlotBudget / bytes)));
+            if (nslots_req > 0) cap = std::min<long>(cap, nslots_req);
+            m->bucket_chi.push_back(c);
+            m->bucket_base.push_back(m->nslots);
+            m->bucket_cap.push_back(int(cap));
+            bucket_bytes.push_back(bytes);
+            bucket_gs.push_back(gs_c);
+            m->nslots += int(cap);
+        }
+    }
+    size_t slot_pool_bytes = 0;
+    for (size_t b = 0; b < m->bucket_chi.size(); ++b) slot_pool_bytes += bucket_bytes[b] * size_t(m->bucket_cap[b]);
     const size_t site_bytes = site_off[n] * sizeof(double2);
-    const uint64_t need = site_bytes + uint64_t(m->nslots) * slot_bytes;
+    const uint64_t need = site_bytes + uint64_t(slot_pool_bytes);
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "cudaMemGetInfo"));
     if (need > fr) return bail(fail_oom(need, fr));
@@ -1233,7 +1304,7 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     m->d_status = m->d_dr + n;
     if (wqc_status st = dmalloc(m, &p, 2 * ns.size() * sizeof(int))) return bail(st);
     m->d_seg = static_cast<int*>(p);
-    if (wqc_status st = dmalloc(m, &p, size_t(m->nslots) * slot_bytes)) return bail(st);
+    if (wqc_status st = dmalloc(m, &p, slot_pool_bytes)) return bail(st);
     m->slot_pool = static_cast<char*>(p);
     if (wqc_status st = dmalloc(m, &p, m->nslots * sizeof(SlotBuffers))) return bail(st);
     m->d_slots = static_cast<SlotBuffers*>(p);
@@ -1273,9 +1344,18 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
         cudaMemcpy(m->d_seg, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(WQC_ERR_CUDA, "initial upload"));
     std::vector<SlotBuffers> slots(m->nslots);
+    m->slot_R.assign(m->nslots, 0);
+    m->slot_E.assign(m->nslots, 0);
+    char* base = m->slot_pool;
     for (int sl = 0; sl < m->nslots; ++sl) {
-        char* base = m->slot_pool + size_t(sl) * slot_bytes;
+        size_t bk = 0;
+        while (bk + 1 < m->bucket_chi.size() && sl >= m->bucket_base[bk + 1]) ++bk;
+        const int R = 2 * m->bucket_chi[bk], E = std::min(m->bucket_chi[bk] + kRsvdOversample, R);
+        const size_t gs_c = bucket_gs[bk];
+        m->slot_R[sl] = R;
+        m->slot_E[sl] = E;
         double2* c = reinterpret_cast<double2*>(base);
+        base += bucket_bytes[bk];
         SlotBuffers& bf = slots[sl];
         bf.theta = c; c += size_t(R) * R;
         bf.w = c; c += size_t(R) * R;
@@ -1961,7 +2041,7 @@ wqc_status wqc_mps_debug_workspace(wqc_mps* m, uint32_t slot, int32_t which, voi
     SlotBuffers b;
     CUDA_TRY(cudaMemcpy(&b, m->d_slots + slot, sizeof(b), cudaMemcpyDeviceToHost));
     const void* src = nullptr;
-    const int R = 2 * m->chi, E = std::min(m->chi + kRsvdOversample, R);
+    const int R = m->slot_R[slot], E = m->slot_E[slot];
     size_t cap = 0;
     switch (which) {
         case 0: src = b.theta; cap = size_t(R) * R * sizeof(double2); break;
@@ -2460,6 +2540,207 @@ void wqc_adjoint_destroy(wqc_adjoint* a) {
         for (char* p : a->cp) dfree(a->m, p, bytes);
     }
     delete a;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Autotuner of the Jacobi SVD's cluster size, with a fingerprinted cache (the
+// pattern of the reference's GEMM side calibration, src/tn/gpu/gemm.rs:
+// 495-543, 649-702: measure once per machine, keep the result in a file keyed
+// by what the measurement depends on, reuse it on later starts).
+//
+// For every saturated shape of the configured chi_max values (2 chi x 2 chi,
+// chi in 16, 32, 64, 128), in the plain form and in the precision form's
+// first phase, and for both kinds of wave -- one latency-bound split, and a
+// batch of 32 splits that fills the device -- each cluster size whose shared
+// memory fits is timed on seeded random sites (Jacobi kernel time from the
+// state's CUDA events, best of three) and the fastest is kept.  Shapes the
+// table does not hold keep the cost model of choose_cluster.
+// ===========================================================================
+namespace {
+
+constexpr int kTuneVersion = 1;
+
+std::string tune_fingerprint(const wqc_cuda_ctx* ctx) {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, ctx->device);
+    int drv = 0, rt = 0;
+    cudaDriverGetVersion(&drv);
+    cudaRuntimeGetVersion(&rt);
+    std::string name(prop.name);
+    for (char& c : name)
+        if (c == '|' || c == '\n' || c == '\r') c = ' ';
+    return "wqc-jacobi-clusters v" + std::to_string(kTuneVersion) + "|" + name + "|sm=" +
+           std::to_string(prop.multiProcessorCount) + "|cc=" + std::to_string(prop.major) + "." +
+           std::to_string(prop.minor) + "|driver=" + std::to_string(drv) + "|runtime=" + std::to_string(rt) +
+           "|max_cluster=" + std::to_string(ctx->max_cluster);
+}
+
+std::string tune_cache_path(const char* path) {
+    if (path && *path) return path;
+    if (const char* p = std::getenv("WQC_TUNE_PATH")) return p;
+    std::string base;
+    if (const char* x = std::getenv("XDG_CACHE_HOME"))
+        base = x;
+    else if (const char* h = std::getenv("HOME"))
+        base = std::string(h) + "/.cache";
+    else
+        base = ".";
+    return base + "/wqc/jacobi-clusters";
+}
+
+bool tune_read(const std::string& path, const std::string& fp, std::vector<wqc_cuda_ctx::Tuned>& out) {
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    char line[512];
+    bool ok = std::fgets(line, sizeof(line), f) != nullptr;
+    if (ok) {
+        std::string first(line);
+        while (!first.empty() && (first.back() == '\n' || first.back() == '\r')) first.pop_back();
+        ok = first == fp;
+    }
+    std::vector<wqc_cuda_ctx::Tuned> t;
+    while (ok && std::fgets(line, sizeof(line), f)) {
+        wqc_cuda_ctx::Tuned e{};
+        if (std::sscanf(line, "%d %d %d %d %d %d", &e.M, &e.N, &e.len, &e.elem, &e.throughput, &e.C) == 6 && e.C >= 1)
+            t.push_back(e);
+    }
+    std::fclose(f);
+    if (ok) out = t;
+    return ok;
+}
+
+bool tune_write(const std::string& path, const std::string& fp, const std::vector<wqc_cuda_ctx::Tuned>& t) {
+    const size_t slash = path.find_last_of('/');
+    if (slash != std::string::npos) {  // create the parent directories
+        std::string dir = path.substr(0, slash);
+        for (size_t i = 1; i <= dir.size(); ++i)
+            if (i == dir.size() || dir[i] == '/') {
+                const std::string part = dir.substr(0, i);
+                if (!part.empty()) mkdir(part.c_str(), 0755);
+            }
+    }
+    const std::string tmp = path + ".tmp";
+    FILE* f = std::fopen(tmp.c_str(), "w");
+    if (!f) return false;
+    std::fprintf(f, "%s\n", fp.c_str());
+    for (const auto& e : t) std::fprintf(f, "%d %d %d %d %d %d\n", e.M, e.N, e.len, e.elem, e.throughput, e.C);
+    const bool ok = std::fclose(f) == 0;
+    return ok && std::rename(tmp.c_str(), path.c_str()) == 0;
+}
+
+// Seeded random complex entries in [-1, 1) (xorshift64*).
+void fill_random(std::vector<double>& v, unsigned long long& state) {
+    for (double& x : v) {
+        state ^= state >> 12;
+        state ^= state << 25;
+        state ^= state >> 27;
+        x = double((state * 2685821657736338717ull) >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+    }
+}
+
+// Jacobi milliseconds of one wave of `count` exact 2chi x 2chi splits at the
+// cluster size the context forces (best of `reps`); < 0 on failure.
+double tune_measure(wqc_cuda_ctx* ctx, int chi, int precision, int count, int reps) {
+    std::vector<uint32_t> qs(count, 4), chis(count, uint32_t(chi));
+    wqc_mps* m = nullptr;
+    if (wqc_batch_create(ctx, uint32_t(count), qs.data(), chis.data(), precision, 0, &m) != WQC_OK) return -1.0;
+    if (count == 1) m->batch = false;  // one split: the latency-bound kind of wave
+    m->exact_only = true;
+    unsigned long long rng = 0x9E3779B97F4A7C15ull ^ (unsigned long long)(chi * 131 + count);
+    const int dims[4][2] = {{1, chi}, {chi, chi}, {chi, chi}, {chi, 1}};
+    std::vector<double> buf;
+    double best = -1.0;
+    for (int rep = 0; rep <= reps; ++rep) {
+        wqc_mps_reset(m);
+        for (int sl = 0; sl < count; ++sl)
+            for (int q = 0; q < 4; ++q) {
+                buf.assign(size_t(dims[q][0]) * 2 * dims[q][1] * 2, 0.0);
+                fill_random(buf, rng);
+                if (wqc_mps_upload_site(m, uint32_t(sl * 4 + q), uint32_t(dims[q][0]), uint32_t(dims[q][1]),
+                                        buf.data()) != WQC_OK) {
+                    wqc_mps_destroy(m);
+                    return -1.0;
+                }
+            }
+        std::vector<wqc_gate> gates(count);
+        std::vector<uint32_t> offs(count + 1);
+        for (int sl = 0; sl < count; ++sl) {
+            gates[sl] = wqc_gate{WQC_GATE_CZ, 1, 2, 0, 0.0};
+            offs[sl] = uint32_t(sl);
+        }
+        offs[count] = uint32_t(count);
+        wqc_mps_reset_stats(m);
+        wqc_mps_set_profiling(m, rep > 0 ? 1 : 0);  // rep 0 warms up
+        wqc_status st = wqc_batch_apply_gates(m, gates.data(), offs.data());
+        wqc_kernel_stats ks{};
+        if (st == WQC_OK) st = wqc_mps_synchronize(m);
+        if (st == WQC_OK) st = wqc_mps_kernel_stats(m, &ks);
+        if (st != WQC_OK) {
+            wqc_mps_destroy(m);
+            return -1.0;
+        }
+        if (rep > 0 && (best < 0 || ks.milliseconds[0] < best)) best = ks.milliseconds[0];
+    }
+    wqc_mps_destroy(m);
+    return best;
+}
+
+}  // namespace
+
+extern "C" {
+
+wqc_status wqc_cuda_autotune(wqc_cuda_ctx* ctx, const char* cache_path, double budget_seconds, uint32_t* entries) {
+    if (!ctx) return fail(WQC_ERR_INVALID, "null context");
+    CUDA_TRY(cudaSetDevice(ctx->device));
+    const std::string fp = tune_fingerprint(ctx);
+    const std::string path = tune_cache_path(cache_path);
+    std::vector<wqc_cuda_ctx::Tuned> table;
+    if (tune_read(path, fp, table)) {
+        ctx->tuned = table;
+        if (entries) *entries = uint32_t(table.size());
+        return WQC_OK;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    auto elapsed = [&]() {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    };
+    ctx->tuned.clear();
+    for (int precision : {WQC_PRECISION_FP64, WQC_PRECISION_FP32}) {
+        for (int chi : {16, 32, 64, 128}) {
+            for (int throughput : {0, 1}) {
+                if (budget_seconds > 0 && elapsed() > budget_seconds) break;
+                const int M = 2 * chi, N = 2 * chi;
+                const size_t elem = precision == WQC_PRECISION_FP32 ? sizeof(float2) : sizeof(double2);
+                const int len = precision == WQC_PRECISION_FP32 ? M + N : M;
+                int best_c = 0;
+                double best_ms = 0.0;
+                for (int c = 1; c <= ctx->max_cluster; ++c) {
+                    if (jacobi_smem_bytes(len, N, c, elem) > kSmemLimit) continue;
+                    const int b = round_up(N, 4 * c) / (2 * c);
+                    if (b > kJacobiThreads / 32) continue;  // more column pairs than warps
+                    ctx->force_C = c;
+                    const double ms = tune_measure(ctx, chi, precision, throughput ? 32 : 1, 3);
+                    ctx->force_C = 0;
+                    if (ms < 0) {
+                        ctx->tuned.clear();
+                        return fail(WQC_ERR_CUDA, std::string("autotune measurement failed: ") + g_err);
+                    }
+                    // A batch is throughput-bound: SM time (ms x C) decides.
+                    const double cost = throughput ? ms * c : ms;
+                    if (!best_c || cost < best_ms) {
+                        best_c = c;
+                        best_ms = cost;
+                    }
+                }
+                if (best_c) ctx->tuned.push_back({M, N, len, int(elem), throughput, best_c});
+            }
+        }
+    }
+    tune_write(path, fp, ctx->tuned);  // a cache that cannot be written only costs the next start a measurement
+    if (entries) *entries = uint32_t(ctx->tuned.size());
+    return WQC_OK;
 }
 
 }  // extern "C"

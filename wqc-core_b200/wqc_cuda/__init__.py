@@ -50,7 +50,7 @@ EXPORTS = (
     "wqc_batch_create", "wqc_batch_apply_gates", "wqc_batch_amplitudes", "wqc_batch_slice_times",
     "wqc_expectation_pauli_noalloc", "wqc_batch_expectation_pauli", "wqc_mps_sample",
     "wqc_mps_overlap", "wqc_cuda_last_oom", "wqc_mps_site_amplitudes_many", "wqc_mps_to_dense",
-    "wqc_adjoint_forward", "wqc_adjoint_backward", "wqc_adjoint_destroy",
+    "wqc_adjoint_forward", "wqc_adjoint_backward", "wqc_adjoint_destroy", "wqc_cuda_autotune",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
@@ -101,6 +101,7 @@ def lib():
         L.wqc_cuda_last_oom.restype = None
         L.wqc_cuda_open.argtypes = [I, ctypes.POINTER(P)]
         L.wqc_cuda_close.argtypes = [P]
+        L.wqc_cuda_autotune.argtypes = [P, ctypes.c_char_p, ctypes.c_double, ctypes.POINTER(U32)]
         L.wqc_cuda_device_info.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
                                            ctypes.POINTER(ctypes.c_int32)]
         L.wqc_mps_workspace_bytes.argtypes = [U32, U32]
@@ -214,6 +215,15 @@ class Context:
         if cls._shared is None:
             cls._shared = Context()
         return cls._shared
+
+    def autotune(self, cache_path: str | None = None, budget_seconds: float = 0.0) -> int:
+        """Measured Jacobi cluster sizes for this device (wqc_cuda_autotune),
+        loaded from the fingerprinted cache when it matches; the number of
+        tuned shapes."""
+        n = ctypes.c_uint32()
+        _check(lib().wqc_cuda_autotune(self._h, cache_path.encode() if cache_path else None, float(budget_seconds),
+                                       ctypes.byref(n)))
+        return n.value
 
     def device_info(self):
         tot, fr, sm = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int32()
