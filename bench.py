@@ -614,6 +614,36 @@ def record_flops(W, recs) -> float:
     return flops
 
 
+def trace_loop_leg(W, ctx, w) -> dict:
+    """The production call pattern of the reference's trace loop
+    (src/tn/trace.rs:55-187) on the headline circuit: rotation runs folded,
+    disjoint layers batched, and before every traced step one
+    wqc_mps_site_amplitudes_many call (control probabilities and first-time
+    target amplitudes), each a synchronising device read; wall clock of the
+    whole loop through the C ABI."""
+    from wqc_cuda import trace_replay as TR
+
+    m = W.CudaMps(w.n, w.chi, ctx=ctx)
+    TR.replay(m, w.n, w.gates[:200])  # warm-up
+    m.reset()
+    t0 = time.perf_counter()
+    reads = TR.replay(m, w.n, w.gates)
+    amp = m.amplitude_at_compact_zero()
+    sec = time.perf_counter() - t0
+    splits = m.split_count()
+    m.close()
+    return {
+        "workload": f"{w.name}: the trace loop's steps and reads, split rule reference",
+        "e2e_applies_per_s": splits / sec,
+        "seconds": sec,
+        "steps_with_reads": len(reads),
+        "reads": int(sum(len(t) for t, _ in reads)),
+        "unit": UNIT,
+        "amplitude": [amp.real, amp.imag],
+        "note": "wall clock of every C ABI call of the loop (gate plans in host memory, reads to host memory)",
+    }
+
+
 def exact_rule_leg(W, torch, ctx, flush) -> dict:
     """The headline circuit under the exact split rule (an exact SVD on every
     split, so the result does not depend on the range finder's rank-48 test
@@ -680,6 +710,11 @@ def run_cuda(args) -> None:
     g0, windows = timed_windows(w, SATURATED_LAYERS.get(args.workload, 0), args.steps)
     rule = W.SPLIT_RULE_EXACT if args.split_rule == "exact" else W.SPLIT_RULE_REFERENCE
     ctx = W.Context(local)
+    # Jacobi cluster sizes measured on this device (or loaded from the
+    # fingerprinted cache), before any timed work.
+    t_tune = time.perf_counter()
+    tuned = 0 if args.no_autotune else ctx.autotune(os.environ.get("WQC_TUNE_PATH"), 120.0)
+    tune_s = time.perf_counter() - t_tune
     m = W.CudaMps(w.n, w.chi, ctx=ctx)
     m.set_split_rule(rule)
     stream = torch.cuda.ExternalStream(m.stream())
@@ -786,6 +821,7 @@ def run_cuda(args) -> None:
             "kernel_ms_per_step": {k: v / steps for k, v in stats["milliseconds"].items()},
             "gpu_launches": stats["total_launches"],
             "clocks": clk,
+            "autotune": {"tuned_shapes": tuned, "seconds": tune_s},
             "amplitude": [amp.real, amp.imag],
             "whole_circuit": {
                 "applies_per_s": whole_splits / (whole_ms * 1e-3),
@@ -807,6 +843,8 @@ def run_cuda(args) -> None:
             }
         if world == 1 and args.workload == "config1" and args.exact_rule_leg:
             line["exact_rule"] = exact_rule_leg(W, torch, ctx, flush)
+        if world == 1 and args.trace_leg:
+            line["trace_loop"] = trace_loop_leg(W, ctx, w)
         if world == 1 and args.batch_slices > 0:
             line["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush,
                                       0.0 if args.no_cpu_baseline else args.cpu_budget)
@@ -841,6 +879,9 @@ def main():
     ap.add_argument("--split-rule", choices=("reference", "exact"), default="reference")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the cost model's Jacobi cluster sizes")
+    ap.add_argument("--no-trace-leg", dest="trace_leg", action="store_false",
+                    help="skip the trace loop's call pattern (per-step reads) on the headline circuit")
     ap.add_argument("--no-exact-rule-leg", dest="exact_rule_leg", action="store_false",
                     help="skip the headline circuit under the exact split rule, checked against the oracle fixture")
     ap.add_argument("--no-differentiation-leg", dest="differentiation_leg", action="store_false",

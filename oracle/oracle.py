@@ -201,6 +201,24 @@ def run(n: int, chi: int, gates: np.ndarray, call_sequence: bool = False, rule: 
     return m
 
 
+def self_drift(n: int, chi: int, gates: np.ndarray, rule: int = 0, call_sequence: bool = False) -> np.ndarray:
+    """Per-split |discarded weight| difference between two oracle runs of the
+    same circuit, one with its Golub-Kahan SVD (the reference's primary) and
+    one with its Jacobi SVD as primary: how far two FP64 SVDs of the same
+    matrices drift apart once truncation carries their rounding on.  Kept
+    chi, paths and shapes must agree between the two."""
+    runs = []
+    for primary in (0, 1):
+        set_primary_svd(primary)
+        try:
+            runs.append(run(n, chi, gates, call_sequence=call_sequence, rule=rule).records())
+        finally:
+            set_primary_svd(0)
+    if not all(np.array_equal(runs[0][k], runs[1][k]) for k in ("rows", "cols", "path", "chi")):
+        raise OracleError("the oracle's two SVDs disagree in a kept chi or path")
+    return np.abs(runs[0]["discarded_weight"] - runs[1]["discarded_weight"])
+
+
 def time_split(n: int, gates: np.ndarray, split: int, max_bond: int) -> complex:
     g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
     out = np.zeros(2)

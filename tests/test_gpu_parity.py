@@ -33,19 +33,8 @@ def amp_err(a: complex, b: complex, n: int) -> float:
 
 
 def oracle_drift(n, chi, gates, rule=0):
-    """Per-split |discarded weight| difference between two oracle runs of the
-    same circuit, one with its Golub-Kahan SVD (the reference's primary) and
-    one with its Jacobi SVD as primary: how far two FP64 SVDs of the same
-    matrices drift apart once truncation carries their rounding on."""
-    runs = []
-    for primary in (0, 1):
-        O.set_primary_svd(primary)
-        try:
-            runs.append(O.run(n, chi, gates, rule=rule).records())
-        finally:
-            O.set_primary_svd(0)
-    assert all(np.array_equal(runs[0][k], runs[1][k]) for k in ("rows", "cols", "path", "chi"))
-    return np.abs(runs[0]["discarded_weight"] - runs[1]["discarded_weight"])
+    """The oracle's own per-split weight drift between its two FP64 SVDs."""
+    return O.self_drift(n, chi, gates, rule=rule)
 
 
 def assert_records_match(got, ref, drift=None):
@@ -271,15 +260,16 @@ def test_precision_form_tracks_the_fp64_oracle(cuda_ctx):
     the first phase of every SVD, then V made orthonormal in FP64, X V formed
     in FP64 and FP64 sweeps to finish.  On the 16-qubit chi 32 brickwork (150
     truncating splits) the amplitude stays within PRECISION_FORM_AMP_RTOL of
-    the FP64 oracle and every split record -- shape, path, kept chi,
-    discarded weight -- is the plain form's."""
+    the FP64 oracle, shapes, paths and kept chi are bit-exact, and the
+    discarded weights agree as the plain form's long runs do (1e-12 plus the
+    oracle's own drift between two FP64 SVDs)."""
     w = C.config0()
     m = W.CudaMps(w.n, w.chi, ctx=cuda_ctx, precision=W.PRECISION_FP32)
     m.apply_gates(w.gates)
     o = O.run(w.n, w.chi, w.gates)
     a, b = m.amplitude_zero(), o.amplitude_zero()
     assert rel_err(a, b) < PRECISION_FORM_AMP_RTOL, (a, b)
-    assert_records_match(m.split_records(), o.records())
+    assert_records_match(m.split_records(), o.records(), drift=oracle_drift(w.n, w.chi, w.gates))
 
 
 def test_precision_form_batch_tracks_the_fp64_oracle(cuda_ctx):

@@ -49,11 +49,16 @@ class OracleState:
         return np.array([self.m.site_amplitudes(int(t)) for t in targets], dtype=np.complex128)
 
 
-def assert_records_equal(got, ref):
+def assert_records_equal(got, ref, drift=None):
+    """Shapes, paths and kept chi bit-exact; discarded weights within 1e-12
+    plus ten times the oracle's own drift between two FP64 SVDs."""
     assert len(got) == len(ref)
     for k in ("left_site", "rows", "cols", "ell", "path", "chi"):
         assert np.array_equal(got[k], ref[k]), k
-    assert np.abs(got["discarded_weight"] - ref["discarded_weight"]).max(initial=0) <= 1e-12
+    tol = 1e-12 * np.maximum(1.0, np.abs(ref["discarded_weight"]))
+    if drift is not None:
+        tol = tol + 10.0 * np.maximum.accumulate(drift)
+    assert np.all(np.abs(got["discarded_weight"] - ref["discarded_weight"]) <= tol)
 
 
 def trace_workload(n=24, depth=12, seed=31):
@@ -80,7 +85,8 @@ def test_trace_loop_reads_and_splits_match_oracle(cuda_ctx):
     for (tg, ag), (tr, ar) in zip(got, ref):
         assert np.array_equal(tg, tr)
         assert np.abs(ag - ar).max() <= READ_RTOL * scale, (tg, ag, ar)
-    assert_records_equal(m.split_records(), o.m.records())
+    drift = O.self_drift(n, chi, gates, call_sequence=True)
+    assert_records_equal(m.split_records(), o.m.records(), drift)
     # the oracle's own restatement of the call sequence gives the same splits
     assert_records_equal(o.m.records(), O.run(n, chi, gates, call_sequence=True).records())
     a, b = m.amplitude_zero(), o.m.amplitude_zero()
@@ -107,9 +113,9 @@ def test_cached_environments_follow_every_operation(cuda_ctx):
             ref = np.array([o.site_amplitudes(t) for t in targets])
             scale = max(scale, np.abs(ref).max())
             assert np.abs(got - ref).max() <= READ_RTOL * scale, (i, targets)
-    s = m.site(9)
-    m.set_site(9, 0.5 * s)
-    o.set_site(9, 0.5 * s)
+    # an upload (each side scales its own site 9: the two gauges differ)
+    m.set_site(9, 0.5 * m.site(9))
+    o.set_site(9, 0.5 * o.site(9))
     for t in (0, 9, n - 1):
         assert np.abs(np.array(m.site_amplitudes(t)) - np.array(o.site_amplitudes(t))).max() <= READ_RTOL * scale
     m.apply_gates(C.gates_array([C.g3(4, 12, 8)]))
