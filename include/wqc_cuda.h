@@ -54,8 +54,8 @@ enum wqc_precision {
                                first sweeps complex64 columns (FP32 dot products and
                                rotation updates, FP64 rotation parameters, tolerance and
                                convergence tests) that carry X V and the accumulated V;
-                               V is then made orthonormal to FP64 rounding (one
-                               Newton-Schulz step) and X V formed in FP64, and FP64
+                               V is then made orthonormal to FP64 rounding (two
+                               Newton-Schulz steps) and X V formed in FP64, and FP64
                                sweeps finish from there (quadratic convergence: a few
                                sweeps).  Sites, merges, range finder, sort and cut stay
                                FP64, so results carry FP64-level error. */

@@ -54,7 +54,7 @@ wqc_status fail_oom(uint64_t required, uint64_t available) {
 
 constexpr int kMaxSweeps = 60;
 constexpr int kDenseMaxQubits = 28;  // 2^28 complex128 = 4 GiB on the host
-constexpr size_t kSlotBudget = size_t(2) << 30;  // split workspace per chi_max bucket
+constexpr size_t kSlotBudget = size_t(1) << 30;  // split workspace per chi_max bucket
 constexpr size_t kSmemLimit = 232448 - 1024;  // 227 KB opt-in per block, minus static shared memory
 
 struct Mat2 {
@@ -921,11 +921,11 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
             }
             if (!any) return WQC_OK;
             if (m->fp32) {
-                // G = V^H V, V' = V (3 I - G) / 2, X V' for every job of the mode, then the FP64 finish.
+                // V orthonormalised (two Newton-Schulz steps), X V for every job of the mode, then the FP64 finish.
                 Timed t(m, 0, on);
                 const int side = std::max(w.max_rows, w.max_cols);
                 const dim3 g((side + 31) / 32, (side + 31) / 32, nj);
-                for (int stage = 0; stage < 3; ++stage) {
+                for (int stage = 0; stage < kPrecondStages; ++stage) {
                     precond_gemm_kernel<<<g, 256, 0, on>>>(d_jobs, m->d_state, m->d_slots, mode, stage);
                     count_launch(m, 0);
                 }

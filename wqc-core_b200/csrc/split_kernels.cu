@@ -1508,26 +1508,30 @@ __global__ void __launch_bounds__(256) precond_gemm_kernel(const SplitJob* jobs,
     int sr, sc, ld, rows_of_src;
     jacobi_task(J, S, B, mode, src, sr, sc, ld, rows_of_src);
     const int M = rows_of_src ? sc : sr, N = rows_of_src ? sr : sc;
-    const int m = stage == 2 ? M : N, n = N, k = N;
+    const bool last = stage == kPrecondXV;
+    const int m = last ? M : N, n = N, k = N;
     const int i0 = blockIdx.y * kGemmT, n0 = blockIdx.x * kGemmT;
     if (i0 >= m || n0 >= n) return;
-    const double2* V = B.z;
+    // Two Newton-Schulz steps: V (z) -> zr -> z; then X V from z.
+    const bool second = stage >= kPrecondGram2;
+    const double2* V = last ? B.z : (second ? B.zr : B.z);
     double2* G = B.omega;
-    double2* V2 = B.zr;
+    double2* Vout = second ? B.z : B.zr;
+    const bool gram = stage == kPrecondGram1 || stage == kPrecondGram2;
     const double dust2 = kDustRel * kDustRel * S.fro2;
     auto a_at = [&](int i, int kk) -> double2 {
-        if (stage == 0) return cconj(V[size_t(i) * N + kk]);  // V^H
-        if (stage == 1) return V[size_t(kk) * N + i];
+        if (gram) return cconj(V[size_t(i) * N + kk]);  // V^H
+        if (!last) return V[size_t(kk) * N + i];
         const double2 x = rows_of_src ? cconj(src[size_t(kk) * ld + i]) : src[size_t(i) * ld + kk];
         return cnorm2(x) < dust2 ? cmake(0, 0) : x;  // X, dust-zeroed as the first phase loaded it
     };
     auto b_at = [&](int kk, int jj) -> double2 {
-        if (stage == 0) return V[size_t(jj) * N + kk];
-        if (stage == 1) {
+        if (gram) return V[size_t(jj) * N + kk];
+        if (!last) {
             const double2 g = G[size_t(jj) * N + kk];
             return cmake((kk == jj ? 1.5 : 0.0) - 0.5 * g.x, -0.5 * g.y);
         }
-        return V2[size_t(jj) * N + kk];
+        return V[size_t(jj) * N + kk];
     };
     __shared__ double2 As[kGemmT][kGemmK + 1];
     __shared__ double2 Bs[kGemmK][kGemmT + 1];
@@ -1554,8 +1558,8 @@ __global__ void __launch_bounds__(256) precond_gemm_kernel(const SplitJob* jobs,
         }
         __syncthreads();
     }
-    double2* C = stage == 0 ? G : stage == 1 ? V2 : B.w;
-    const int ldc = stage == 2 ? M : N;
+    double2* C = gram ? G : last ? B.w : Vout;
+    const int ldc = last ? M : N;
     for (int x = 0; x < 2; ++x)
         for (int y = 0; y < 2; ++y) {
             const int i = i0 + tr + 16 * x, jj = n0 + tc + 16 * y;

@@ -57,9 +57,11 @@ cudaError_t launch_jacobi_staged(bool fp32, const cudaLaunchConfig_t& cfg, const
                                  const SlotBuffers* slots, const int* idx, int mode, int phase, int max_sweeps, int b,
                                  int* status, unsigned long long* counters);
 // The precision form's FP64 products between its two Jacobi phases, for the
-// jobs active in `mode`: stage 0, G = V^H V; stage 1, V' = V (3 I - G) / 2
-// (one Newton-Schulz step: orthonormal to FP64 rounding); stage 2, X V'
-// into the slot's W buffer, X dust-zeroed as the first phase loaded it.
+// jobs active in `mode`, in stage order: G = V^H V and V <- V (3 I - G) / 2
+// twice (Newton-Schulz: V^H V - I goes from ~1e-6 after the complex64
+// rotations to ~1e-12, then to FP64 rounding), then X V into the slot's W
+// buffer, X dust-zeroed as the first phase loaded it.
+enum { kPrecondGram1 = 0, kPrecondStep1, kPrecondGram2, kPrecondStep2, kPrecondXV, kPrecondStages };
 __global__ void precond_gemm_kernel(const SplitJob* jobs, const SplitState* st, const SlotBuffers* slots, int mode,
                                     int stage);
 // Shape of the staged Jacobi for an M x N working matrix on a cluster of C
