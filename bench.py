@@ -618,6 +618,67 @@ def record_flops(W, recs) -> float:
     return flops
 
 
+def measured_copy_peak(torch) -> float:
+    """Device-to-device copy bandwidth (GB/s, read + write bytes), best of 5
+    over 1 GiB: the HBM roofline of the streaming kernels."""
+    x = torch.empty(1 << 27, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    x.fill_(1.0)
+    y.copy_(x)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        y.copy_(x)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * x.numel() * 8 / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del x, y
+    return best
+
+
+def one_qubit_layer_leg(W, torch, ctx, peak_gbs: float) -> dict:
+    """apply_1q_kernel on a wave that streams: a layer of RY on every site of
+    a saturated chi 256, 100-site state (98 sites of 256 x 2 x 256 complex128,
+    ~200 MB, read and written once by one launch), timed by the kernel's own
+    CUDA events; algorithmic bytes 2 * sum_i l_i 2 r_i * 16."""
+    n, chi = 100, 256
+    m = W.CudaMps(n, chi, ctx=ctx)
+    rng = np.random.default_rng(11)
+    nbytes = 0
+    for q in range(n):
+        l = 1 if q == 0 else chi
+        r = 1 if q == n - 1 else chi
+        t = (rng.standard_normal((l, 2, r)) + 1j * rng.standard_normal((l, 2, r))) / np.sqrt(2 * r)
+        m.set_site(q, t)
+        nbytes += 2 * t.size * 16
+    layer = C.gates_array([C.g1(C.RY, q, 0.1 + 0.01 * q) for q in range(n)])
+    m.apply_gates(layer)  # warm-up
+    m.synchronize()
+    best_ms = None
+    for _ in range(5):
+        m.reset_stats()
+        m.set_profiling(True)
+        m.apply_gates(layer)
+        m.synchronize()
+        st = m.kernel_stats()
+        m.set_profiling(False)
+        ms = st["milliseconds"]["one_qubit"]
+        best_ms = ms if best_ms is None else min(best_ms, ms)
+    m.close()
+    gbs = nbytes / (best_ms * 1e-3) / 1e9
+    return {
+        "kernel": "apply_1q_kernel",
+        "bytes_per_launch": nbytes,
+        "ms_per_launch": best_ms,
+        "achieved_gbs": gbs,
+        "peak_gbs": peak_gbs,
+        "frac": gbs / peak_gbs if peak_gbs else None,
+        "peak_source": "device-to-device copy of 1 GiB measured in this run (MEASURED_PEAKS.json absent)",
+    }
+
+
 def trace_loop_leg(W, ctx, w) -> dict:
     """The production call pattern of the reference's trace loop
     (src/tn/trace.rs:55-187) on the headline circuit: rotation runs folded,
@@ -860,6 +921,8 @@ def run_cuda(args) -> None:
             line["exact_rule"] = exact_rule_leg(W, torch, ctx, flush)
         if world == 1 and args.trace_leg:
             line["trace_loop"] = trace_loop_leg(W, ctx, w)
+        if world == 1 and args.hbm_leg:
+            line["one_qubit_layer"] = one_qubit_layer_leg(W, torch, ctx, measured_copy_peak(torch))
         if world == 1 and args.batch_slices > 0:
             line["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush,
                                       0.0 if args.no_cpu_baseline else args.cpu_budget)
@@ -895,6 +958,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the cost model's Jacobi cluster sizes")
+    ap.add_argument("--no-hbm-leg", dest="hbm_leg", action="store_false",
+                    help="skip the one-qubit layer over a saturated chi 256 state (HBM bandwidth of apply_1q_kernel)")
     ap.add_argument("--no-trace-leg", dest="trace_leg", action="store_false",
                     help="skip the trace loop's call pattern (per-step reads) on the headline circuit")
     ap.add_argument("--no-exact-rule-leg", dest="exact_rule_leg", action="store_false",

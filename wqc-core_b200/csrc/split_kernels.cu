@@ -600,6 +600,31 @@ struct JacobiReal<float2> {
     using R = float;
 };
 
+// Warp sums of four values, every lane receiving the same four totals (so
+// branches on them stay warp-uniform).  Instead of four butterflies (20
+// shuffles) the first two levels split the values between the lane halves
+// (lanes with bit 4 clear keep a, b and pass g, h; then bit 3 picks one of
+// the two), three more levels finish one value per quarter of the warp, and
+// four broadcasts from lanes 0, 8, 16, 24 hand out the totals: 10 shuffles,
+// on the dependent chain of every rotation round.
+template <typename R>
+__device__ __forceinline__ void warp_sum4(R& a, R& b, R& g, R& h, int lane) {
+    const bool hi = lane & 16;
+    R k0 = hi ? g : a, k1 = hi ? h : b;
+    k0 += __shfl_xor_sync(0xffffffffu, hi ? a : g, 16);
+    k1 += __shfl_xor_sync(0xffffffffu, hi ? b : h, 16);
+    const bool b3 = lane & 8;
+    R v = b3 ? k1 : k0;
+    v += __shfl_xor_sync(0xffffffffu, b3 ? k0 : k1, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    a = __shfl_sync(0xffffffffu, v, 0);
+    b = __shfl_sync(0xffffffffu, v, 8);
+    g = __shfl_sync(0xffffffffu, v, 16);
+    h = __shfl_sync(0xffffffffu, v, 24);
+}
+
 // Rotation parameters from alpha = |p|^2, beta = |q|^2, gamma = <p, q>:
 // returns false when the pair is left alone (noise-level column, or already
 // orthogonal to tol), else c and w = s * phase.
@@ -672,13 +697,7 @@ __device__ __forceinline__ int jacobi_rotate(T* __restrict__ xp, T* __restrict__
     b_ += b1;
     gr_ += gr1;
     gi_ += gi1;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a_ += __shfl_xor_sync(0xffffffffu, a_, o);
-        b_ += __shfl_xor_sync(0xffffffffu, b_, o);
-        gr_ += __shfl_xor_sync(0xffffffffu, gr_, o);
-        gi_ += __shfl_xor_sync(0xffffffffu, gi_, o);
-    }
+    warp_sum4(a_, b_, gr_, gi_, lane);
     double c64, wr64, wi64;
     if (!jacobi_params(a_, b_, gr_, gi_, tol, noise_floor, relmax, c64, wr64, wi64)) return 0;
     const R wr = R(wr64), wi = R(wi64), cr = R(c64);
@@ -751,13 +770,7 @@ __device__ __forceinline__ int jacobi_rotate_reg(T (&u)[kJacobiRegRows], T* __re
     b_ += b1;
     gr_ += gr1;
     gi_ += gi1;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a_ += __shfl_xor_sync(0xffffffffu, a_, o);
-        b_ += __shfl_xor_sync(0xffffffffu, b_, o);
-        gr_ += __shfl_xor_sync(0xffffffffu, gr_, o);
-        gi_ += __shfl_xor_sync(0xffffffffu, gi_, o);
-    }
+    warp_sum4(a_, b_, gr_, gi_, lane);
     double c64, wr64, wi64;
     if (!jacobi_params(a_, b_, gr_, gi_, tol, noise_floor, relmax, c64, wr64, wi64)) return 0;
     const R wr = R(wr64), wi = R(wi64), cr = R(c64);
