@@ -70,3 +70,47 @@ def test_sample_counts_builds_the_reference_keys():
     # a later measure into the same classical bit wins, as in outcome_key
     m2 = _FakeDraws(2, [0b10])
     assert m2.sample_counts([(0, 0), (1, 0)], 1, 1, seed=0) == {"1": 1}
+
+
+def test_trace_replay_steps_follow_the_oracle_call_sequence():
+    """wqc_cuda/trace_replay.py folds the gate list as trace.rs does (H runs,
+    rotation runs with the full-turn rule, disjoint layers above 16 qubits):
+    driven on the oracle it leaves the same state and split records as the
+    oracle's own restatement of the call sequence, and it reads each
+    control's probability and each target's amplitudes at most as the
+    reference's resolve_pre_amps does."""
+    import math
+
+    import oracle as O
+    from wqc_cuda import trace_replay as TR
+
+    class OracleState:
+        def __init__(self, n, chi):
+            self.m = O.OracleMps(n, chi)
+
+        def apply_gates(self, g):
+            self.m.apply_gates(g)
+
+        def apply_adjacent_disjoint_gates(self, g):
+            self.m.apply_layer(g)
+
+        def site_amplitudes_many(self, targets):
+            return np.array([self.m.site_amplitudes(int(t)) for t in targets], dtype=np.complex128)
+
+    n, chi = 18, 8
+    g = C.random_layers(n, 4, seed=3)
+    g += [C.g1(C.RZ, 2, math.pi), C.g1(C.RZ, 2, math.pi), C.g1(C.RY, 4, 0.2), C.g1(C.RY, 4, 0.3)]
+    g += [C.g1(C.H, 6), C.g1(C.H, 6), C.g1(C.H, 7)] + [C.g2(C.CZ, q, q + 1) for q in range(0, n - 1, 2)]
+    gates = C.gates_array(g)
+    kinds = [k for k, _, _ in TR.steps(n, gates)]
+    assert {"layer", "net", "silent", "one"} <= set(kinds)
+    st = OracleState(n, chi)
+    reads = TR.replay(st, n, gates)
+    ref = O.run(n, chi, gates, call_sequence=True)
+    a, b = st.m.records(), ref.records()
+    assert len(a) == len(b) and np.array_equal(a["chi"], b["chi"])
+    assert abs(st.m.amplitude_zero() - ref.amplitude_zero()) <= 1e-12 * max(1.0, abs(ref.amplitude_zero()))
+    # each qubit's amplitudes are read once as a target; controls at every 2q gate
+    targets_seen = [int(t) for tg, _ in reads for t in tg]
+    n2q = int(np.isin(gates["kind"], [C.CNOT, C.CZ]).sum()) + 2 * int((gates["kind"] == C.CCNOT).sum())
+    assert len(targets_seen) <= n2q + n
