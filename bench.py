@@ -679,6 +679,100 @@ def one_qubit_layer_leg(W, torch, ctx, peak_gbs: float) -> dict:
     }
 
 
+def unfused_pass_bytes(tree) -> int:
+    """Bytes a gate-at-a-time executor moves on this tree: every gate node
+    reads and writes its whole state once (2 * 16 * 2^legs)."""
+    legs = {}
+    total = 0
+    for i, nd in enumerate(tree["nodes"]):
+        ops = [nd["left"], nd["right"]]
+        if any("gate" in r for r in ops):
+            st = next(r for r in ops if "gate" not in r)
+            k = legs.pop(st["node"]) if "node" in st else 1
+            total += 2 * (16 << k)
+            legs[i] = k
+        else:
+            legs[i] = sum(legs.pop(r["node"]) if "node" in r else 1 for r in ops)
+    return total
+
+
+def oracle_exact_sample(n: int, gates, budget_s: float) -> tuple[float, int, float]:
+    """The oracle's C loops (exact.rs's apply_in_place, one thread, as the
+    reference runs it) applying the circuit's gates to a full n-qubit state
+    until the budget is spent: (seconds per gate, gates applied, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import exact as OX
+
+    rng = np.random.default_rng(5)
+    data = (rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)) * (2.0 ** (-(n + 1) / 2))
+    wires = list(range(n))
+    t0 = time.perf_counter()
+    done = 0
+    while done < len(gates) and time.perf_counter() - t0 < budget_s:
+        OX.apply_in_place(data, wires, gates[done])
+        done += 1
+    sec = time.perf_counter() - t0
+    return sec / max(done, 1), done, sec
+
+
+def exact_tree_leg(W, ctx, peak_gbs: float, cpu_budget: float) -> dict:
+    """An exact contraction tree (src/tn/exact.rs) on the device: the greedy
+    plan (src/tn/plan.rs) of a 25-qubit RY + CNOT brickwork of depth 20, the
+    widest state the 1 GiB peak admits, contracted for the amplitude of
+    |0...0>.  The state (512 MiB) is larger than L2, so no flush is needed
+    between repetitions.  Device time from the executor's CUDA events; the
+    passes' bytes are 2 * 16 * 2^legs per pass over the 25-leg state."""
+    from wqc_cuda import exact as X
+    from wqc_cuda import exact_plan as P
+
+    n, depth = 25, 20
+    gates = C.ry_cnot_brickwork(n, depth)
+    tree = P.plan_greedy(n, gates)
+    ex = X.ExactContractor(ctx)
+    ex.contract(n, gates, tree, 0)  # warm-up: arena and tables
+    runs = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        amp = ex.contract(n, gates, tree, 0)
+        wall = time.perf_counter() - t0
+        runs.append((ex.stats(), wall))
+    ex.close()
+    st, wall = min(runs, key=lambda r: r[0]["device_ms"])
+    best_wall = min(r[1] for r in runs)
+    pass_gbs = st["pass_bytes"] / (st["pass_ms"] * 1e-3) / 1e9
+    unfused = unfused_pass_bytes(tree)
+    out = {
+        "workload": f"brickwork{n}_d{depth}: {n} qubits, RY + CNOT brickwork of depth {depth} ({len(gates)} gates), "
+                    f"greedy exact tree ({len(tree['nodes'])} nodes, declared peak {tree['peak_bytes']} B)",
+        "gates_per_s": len(gates) / (st["device_ms"] * 1e-3),
+        "e2e_gates_per_s": len(gates) / best_wall,
+        "device_ms": st["device_ms"],
+        "e2e_ms": best_wall * 1e3,
+        "launches": st["launches"],
+        "passes": st["passes"],
+        "outer_products": st["outer_products"],
+        "amplitude": [amp.real, amp.imag],
+        "roofline": {
+            "bound": "hbm", "kernel": "exact_pass_kernel (passes over tensors of >= 2^20 amplitudes)",
+            "achieved": pass_gbs, "peak": peak_gbs, "unit": "GB/s", "frac": pass_gbs / peak_gbs if peak_gbs else None,
+            "pass_ms": st["pass_ms"], "pass_bytes": st["pass_bytes"],
+            "peak_source": "device-to-device copy of 1 GiB measured in this run (MEASURED_PEAKS.json absent)",
+        },
+        "unfused_bytes": unfused,
+        "unfused_ms_at_peak": unfused / (peak_gbs * 1e9) * 1e3 if peak_gbs else None,
+        "note": "e2e: wall clock of wqc_exact_contract (host walk and plan, table upload, device work, amplitude "
+                "to host); unfused_ms_at_peak: the HBM time a gate-at-a-time pass would need at the copy peak",
+    }
+    if cpu_budget > 0:
+        per_gate, done, sec = oracle_exact_sample(n, gates, cpu_budget)
+        out["cpu_baseline"] = {
+            "value": 1.0 / per_gate, "unit": "gates/s", "cores": 1, "kind": "port",
+            "sample": f"the oracle's C loops of exact.rs's apply_in_place (one thread, as the reference) on a "
+                      f"{n}-qubit state: the circuit's first {done} gates in {sec:.1f} s",
+        }
+    return out
+
+
 def trace_loop_leg(W, ctx, w) -> dict:
     """The production call pattern of the reference's trace loop
     (src/tn/trace.rs:55-187) on the headline circuit: rotation runs folded,
@@ -771,6 +865,13 @@ def run_cuda(args) -> None:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.exact_tree_only:
+        # The exact-tree leg alone (profiling runs): one JSON line with the leg.
+        ctx = W.Context(local)
+        leg = exact_tree_leg(W, ctx, measured_copy_peak(torch), 0.0 if args.no_cpu_baseline else args.cpu_budget)
+        if rank == 0:
+            print(json.dumps({"exact_tree": leg}), flush=True)
+        return
     w = workload(args.workload, args.depth)
     g0, windows = timed_windows(w, SATURATED_LAYERS.get(args.workload, 0), args.steps)
     rule = W.SPLIT_RULE_EXACT if args.split_rule == "exact" else W.SPLIT_RULE_REFERENCE
@@ -921,8 +1022,11 @@ def run_cuda(args) -> None:
             line["exact_rule"] = exact_rule_leg(W, torch, ctx, flush)
         if world == 1 and args.trace_leg:
             line["trace_loop"] = trace_loop_leg(W, ctx, w)
+        copy_peak = measured_copy_peak(torch) if world == 1 and (args.hbm_leg or args.exact_tree_leg) else 0.0
         if world == 1 and args.hbm_leg:
-            line["one_qubit_layer"] = one_qubit_layer_leg(W, torch, ctx, measured_copy_peak(torch))
+            line["one_qubit_layer"] = one_qubit_layer_leg(W, torch, ctx, copy_peak)
+        if world == 1 and args.exact_tree_leg:
+            line["exact_tree"] = exact_tree_leg(W, ctx, copy_peak, 0.0 if args.no_cpu_baseline else args.cpu_budget)
         if world == 1 and args.batch_slices > 0:
             line["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush,
                                       0.0 if args.no_cpu_baseline else args.cpu_budget)
@@ -960,6 +1064,10 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the cost model's Jacobi cluster sizes")
     ap.add_argument("--no-hbm-leg", dest="hbm_leg", action="store_false",
                     help="skip the one-qubit layer over a saturated chi 256 state (HBM bandwidth of apply_1q_kernel)")
+    ap.add_argument("--no-exact-tree-leg", dest="exact_tree_leg", action="store_false",
+                    help="skip the 25-qubit exact contraction tree (wqc_exact_contract)")
+    ap.add_argument("--exact-tree-only", action="store_true",
+                    help="run only the exact contraction tree leg and print it (for profiling)")
     ap.add_argument("--no-trace-leg", dest="trace_leg", action="store_false",
                     help="skip the trace loop's call pattern (per-step reads) on the headline circuit")
     ap.add_argument("--no-exact-rule-leg", dest="exact_rule_leg", action="store_false",

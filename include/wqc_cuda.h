@@ -384,6 +384,102 @@ WQC_API void wqc_mps_reset_stats(wqc_mps* mps);
  * time or order work around it. */
 WQC_API void* wqc_mps_stream(wqc_mps* mps);
 
+/* ---------------------------------------------------------------------------
+ * Exact contraction trees (src/tn/exact.rs): a ContractionTree whose nodes
+ * are all Contract { left, right } (src/tn/tree.rs), walked with its state
+ * tensors in device memory.  A node joins two states with no wire in common
+ * by an outer product, or applies a gate to the state that holds all of the
+ * gate's wires; gates are consumed in circuit order; at most 26 open legs per
+ * tensor and a declared peak of at most 1 GiB (exact.rs:25-27).
+ * ------------------------------------------------------------------------- */
+
+/* TensorRef (src/tn/tree.rs).  Only KET0, GATE and NODE are leaves of an exact
+ * tree; the others are rejected with the reference's messages
+ * (exact.rs:243-258). */
+enum wqc_tree_ref_kind {
+    WQC_TREE_KET0 = 0,    /* Ket0(wire): |0> on one wire */
+    WQC_TREE_GATE = 1,    /* Gate(index): gates[index] */
+    WQC_TREE_NODE = 2,    /* Node(index): result of nodes[index] */
+    WQC_TREE_LEFT = 3,    /* Left(_)    -> "exact contraction has no split" */
+    WQC_TREE_RIGHT = 4,   /* Right(_)   -> "exact contraction has no split" */
+    WQC_TREE_BRA0 = 5,    /* Bra0(_)    -> "exact contraction has no bra0" */
+    WQC_TREE_CONTROL = 6, /* Control(_) -> "exact contraction has no gate halves" */
+    WQC_TREE_TARGET = 7   /* Target(_)  -> "exact contraction has no gate halves" */
+};
+typedef struct wqc_tree_ref {
+    int32_t kind; /* enum wqc_tree_ref_kind */
+    uint32_t index;
+} wqc_tree_ref;
+
+/* ContractionNode: op 0 is Contract { left, right }; any other op is a sweep
+ * step (Site, Swap, Pair, ...), which an exact tree may not hold
+ * ("contraction tree mixes sweep steps and exact contractions"). */
+typedef struct wqc_tree_node {
+    int32_t op;
+    wqc_tree_ref left, right;
+} wqc_tree_node;
+
+/* ContractionTree { site_order, nodes, peak_bytes } (src/tn/tree.rs).  The
+ * site order must be empty or the identity (exact trees keep the parent's
+ * wire numbers); has_peak 0 stands for peak_bytes: None. */
+typedef struct wqc_tree {
+    const wqc_tree_node* nodes;
+    uint32_t node_count;
+    const uint32_t* site_order;
+    uint32_t site_order_len;
+    int32_t has_peak;
+    uint64_t peak_bytes;
+} wqc_tree;
+
+typedef struct wqc_exact wqc_exact;
+
+/* An executor of exact trees on ctx's device: its own stream, a device arena
+ * that holds the live tensors (reused, grown on demand) and the pass tables. */
+WQC_API wqc_status wqc_exact_create(wqc_cuda_ctx* ctx, wqc_exact** out);
+WQC_API void wqc_exact_destroy(wqc_exact* ex);
+
+/* exact::validate (exact.rs:48-58): the declared peak and the tree's shape,
+ * host only.  mps_site_order may be NULL (None); otherwise it must be the
+ * identity over qubit_count wires. */
+WQC_API wqc_status wqc_exact_validate(uint32_t qubit_count, const wqc_gate* gates, uint32_t gate_count,
+                                      const wqc_tree* tree, const uint64_t* mps_site_order, uint32_t mps_site_order_len);
+
+/* The peak of the walk without evaluating (exact.rs:650-658, `measured_peak`):
+ * the value a tree declares.  Host only; the declared peak is not read. */
+WQC_API wqc_status wqc_exact_measured_peak(uint32_t qubit_count, const wqc_gate* gates, uint32_t gate_count,
+                                           const wqc_tree* tree, uint64_t* peak);
+
+/* contract_exact_at (exact.rs:70-85) for `count` basis vectors at once: the
+ * tree is contracted once and out[2k], out[2k+1] receive the amplitude of
+ * bits[k] (bit q of bits[k] is wire q).  count 1 is the reference's call;
+ * bits 0 is contract_exact (exact.rs:60-68).  Every failure the reference
+ * reports (tree shape, circuit order, shared wires, legs, peak, declared
+ * peak mismatch) is returned before any device work, with its message in
+ * wqc_cuda_last_error.  Synchronous. */
+WQC_API wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t qubit_count, const wqc_gate* gates, uint32_t gate_count,
+                                      const wqc_tree* tree, const uint64_t* mps_site_order,
+                                      uint32_t mps_site_order_len, const uint64_t* bits, uint32_t count, double* out);
+
+/* Stop a contraction in progress (the reference's cancel::check per gate,
+ * exact.rs:419-421): the running call returns WQC_ERR_CANCELLED at its next
+ * launch; a cancel that arrives between calls stops the next call.  Safe to
+ * call from another thread. */
+WQC_API void wqc_exact_cancel(wqc_exact* ex);
+
+/* What the last wqc_exact_contract did on the device. */
+typedef struct wqc_exact_stats {
+    uint32_t launches;       /* kernels launched */
+    uint32_t passes;         /* gate passes (each: one sweep of a tensor through shared memory) */
+    uint32_t outer_products; /* outer-product joins */
+    uint32_t gates;          /* gates applied */
+    double device_ms;        /* CUDA-event time of the device work, first launch to last */
+    double pass_ms;          /* part of device_ms in passes over tensors of at least 2^20 amplitudes */
+    uint64_t pass_bytes;     /* bytes those passes read and wrote (16 B per amplitude, both ways) */
+    uint64_t bytes_moved;    /* bytes every launch read and wrote, by its access pattern */
+    uint64_t arena_bytes;    /* device arena the tensors were placed in */
+} wqc_exact_stats;
+WQC_API wqc_status wqc_exact_last_stats(wqc_exact* ex, wqc_exact_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

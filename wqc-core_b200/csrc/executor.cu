@@ -1120,6 +1120,14 @@ wqc_status sync_status(wqc_mps* m) {
 // that wqc_cuda_last_error returns.
 namespace wqc {
 wqc_status record_error(wqc_status code, const std::string& msg) { return fail(code, msg); }
+wqc_status record_oom(uint64_t required, uint64_t available) { return fail_oom(required, available); }
+wqc_status check_circuit_gate(int n, const wqc_gate& g) { return check_gate(n, g); }
+void gate_matrix_2x2(int kind, double theta, double2 out[4]) {
+    const Mat2 m = unary_matrix(kind, theta);
+    for (int i = 0; i < 4; ++i) out[i] = m.u[i];
+}
+int context_device(const wqc_cuda_ctx* ctx) { return ctx->device; }
+int context_sm_count(const wqc_cuda_ctx* ctx) { return ctx->sm_count; }
 }  // namespace wqc
 
 // ===========================================================================

@@ -51,6 +51,8 @@ EXPORTS = (
     "wqc_expectation_pauli_noalloc", "wqc_batch_expectation_pauli", "wqc_mps_sample",
     "wqc_mps_overlap", "wqc_cuda_last_oom", "wqc_mps_site_amplitudes_many", "wqc_mps_to_dense",
     "wqc_adjoint_forward", "wqc_adjoint_backward", "wqc_adjoint_destroy", "wqc_cuda_autotune",
+    "wqc_exact_create", "wqc_exact_destroy", "wqc_exact_validate", "wqc_exact_measured_peak", "wqc_exact_contract",
+    "wqc_exact_cancel", "wqc_exact_last_stats",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")

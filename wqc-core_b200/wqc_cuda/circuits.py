@@ -235,3 +235,22 @@ def split_plan(gates: np.ndarray) -> int:
             for a, b in ((c2, t), (c1, t), (c2, t), (c1, t), (c1, c2), (c1, c2)):
                 total += 1 + 2 * (abs(a - b) - 1)
     return total
+
+
+def ry_cnot_brickwork(n: int, depth: int) -> np.ndarray:
+    """Layers of RY(0.17 + 0.01 (q + layer)) on every qubit, then CNOT on
+    alternating neighbour pairs (the exact-tree workload of
+    src/tn/plan.rs:396-410)."""
+    gates = []
+    for layer in range(depth):
+        for q in range(n):
+            gates.append(g1(RY, q, 0.17 + 0.01 * (q + layer)))
+        for q in range(layer % 2, n - 1, 2):
+            gates.append(g2(CNOT, q, q + 1))
+    return gates_array(gates)
+
+
+def star(n: int) -> np.ndarray:
+    """H on qubit 0, then CNOT(0, q) for every other qubit (a GHZ star,
+    src/tn/exact.rs:668-676)."""
+    return gates_array([g1(H, 0)] + [g2(CNOT, 0, q) for q in range(1, n)])
