@@ -729,16 +729,23 @@ def exact_tree_leg(W, ctx, peak_gbs: float, cpu_budget: float) -> dict:
     gates = C.ry_cnot_brickwork(n, depth)
     tree = P.plan_greedy(n, gates)
     ex = X.ExactContractor(ctx)
-    ex.contract(n, gates, tree, 0)  # warm-up: arena and tables
-    runs = []
-    for _ in range(5):
-        t0 = time.perf_counter()
-        amp = ex.contract(n, gates, tree, 0)
-        wall = time.perf_counter() - t0
-        runs.append((ex.stats(), wall))
+    tiles = {}
+    for tile in (12, 13):
+        ex.set_tile_bits(tile)
+        ex.contract(n, gates, tree, 0)  # warm-up: arena and tables
+        runs = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            amp = ex.contract(n, gates, tree, 0)
+            wall = time.perf_counter() - t0
+            runs.append((ex.stats(), wall, amp))
+        tiles[tile] = runs
     ex.close()
-    st, wall = min(runs, key=lambda r: r[0]["device_ms"])
-    best_wall = min(r[1] for r in runs)
+    by_tile = {t: min(r[0]["device_ms"] for r in runs) for t, runs in tiles.items()}
+    tile = min(by_tile, key=by_tile.get)
+    st, wall, amp = min(tiles[tile], key=lambda r: r[0]["device_ms"])
+    best_wall = min(r[1] for r in tiles[tile])
+    amps_equal = all(r[2] == amp for runs in tiles.values() for r in runs)
     pass_gbs = st["pass_bytes"] / (st["pass_ms"] * 1e-3) / 1e9
     unfused = unfused_pass_bytes(tree)
     out = {
@@ -750,10 +757,14 @@ def exact_tree_leg(W, ctx, peak_gbs: float, cpu_budget: float) -> dict:
         "e2e_ms": best_wall * 1e3,
         "launches": st["launches"],
         "passes": st["passes"],
+        "exchanges": st["exchanges"],
         "outer_products": st["outer_products"],
+        "tile_bits": tile,
+        "device_ms_by_tile_bits": by_tile,
         "amplitude": [amp.real, amp.imag],
+        "amplitude_same_for_every_tile_and_run": amps_equal,
         "roofline": {
-            "bound": "hbm", "kernel": "exact_pass_kernel (passes over tensors of >= 2^20 amplitudes)",
+            "bound": "hbm", "kernel": "exact_pass_reg_kernel (passes over tensors of >= 2^20 amplitudes)",
             "achieved": pass_gbs, "peak": peak_gbs, "unit": "GB/s", "frac": pass_gbs / peak_gbs if peak_gbs else None,
             "pass_ms": st["pass_ms"], "pass_bytes": st["pass_bytes"],
             "peak_source": "device-to-device copy of 1 GiB measured in this run (MEASURED_PEAKS.json absent)",
@@ -769,6 +780,74 @@ def exact_tree_leg(W, ctx, peak_gbs: float, cpu_budget: float) -> dict:
             "value": 1.0 / per_gate, "unit": "gates/s", "cores": 1, "kind": "port",
             "sample": f"the oracle's C loops of exact.rs's apply_in_place (one thread, as the reference) on a "
                       f"{n}-qubit state: the circuit's first {done} gates in {sec:.1f} s",
+        }
+    return out
+
+
+def network_tree_leg(W, ctx, fp64_peak: float, cpu_budget: float) -> dict:
+    """A network contraction tree (src/tn/network.rs) on the device: the
+    plain greedy tree (the orchestrator's first pass) of the 5 x 5 grid
+    circuit of depth 12 -- 25 qubits, 769 contractions, 290 GFLOP of complex
+    GEMM, declared peak 554 MB -- contracted for <0...0|U|0...0>.  Device
+    time from the executor's CUDA events; the GEMMs' flops (8 m n k each)
+    over their own event time, against the FP64 DGEMM measured in this run."""
+    from wqc_cuda import network as N
+    from wqc_cuda import network_plan as NP
+
+    n, side, depth = 25, 5, 12
+    gates = C.grid(side, depth)
+    tree = NP.greedy_tree(n, gates)
+    net = N.NetworkContractor(ctx)
+    net.contract(n, gates, tree)  # warm-up: arena, cuBLAS
+    runs = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        amp = net.contract(n, gates, tree)
+        runs.append((net.stats(), time.perf_counter() - t0, amp))
+    net.close()
+    st, _, amp = min(runs, key=lambda r: r[0]["device_ms"])
+    best_wall = min(r[1] for r in runs)
+    tflops = st["gemm_flops"] / (st["gemm_ms"] * 1e-3) / 1e12 if st["gemm_ms"] else None
+    out = {
+        "workload": f"grid{side}x{side}_d{depth}: {n} qubits, RY + RZ on every qubit and CNOTs along rows and "
+                    f"columns, depth {depth} ({len(gates)} gates); greedy network tree ({len(tree['nodes'])} "
+                    f"contractions, declared peak {tree['peak_bytes']} B)",
+        "contractions_per_s": len(tree["nodes"]) / (st["device_ms"] * 1e-3),
+        "device_ms": st["device_ms"],
+        "e2e_ms": best_wall * 1e3,
+        "gemm_ms": st["gemm_ms"],
+        "permute_ms": st["permute_ms"],
+        "gemms": st["gemms"],
+        "permutes": st["permutes"],
+        "gemm_gflop": st["gemm_flops"] / 1e9,
+        "permute_bytes": st["permute_bytes"],
+        "amplitude": [amp.real, amp.imag],
+        "amplitude_same_every_run": all(r[2] == amp for r in runs),
+        "roofline": {
+            "bound": "fp64", "kernel": "cuBLAS ZGEMM of the contractions (GEMMs with results of >= 2^16 amplitudes "
+                                       "timed one by one; smaller ones are in device_ms only)",
+            "achieved": tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+            "frac": tflops / fp64_peak if tflops and fp64_peak else None,
+            "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
+        },
+        "note": "e2e: wall clock of wqc_network_contract (host walk and plan, leaf upload, device work, amplitude "
+                "to host)",
+    }
+    if cpu_budget > 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import network as ON
+
+        kinds = {"ket0": ON.KET0, "gate": ON.GATE, "node": ON.NODE, "bra0": ON.BRA0, "control": ON.CONTROL,
+                 "target": ON.TARGET}
+        nodes = [tuple((kinds[k], v) for side_ in (nd["left"], nd["right"]) for k, v in side_.items())
+                 for nd in tree["nodes"]]
+        t0 = time.perf_counter()
+        ON.contract(n, gates, nodes, tree["peak_bytes"])
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {
+            "value": len(tree["nodes"]) / sec, "unit": "contractions/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"the oracle (numpy permutes, multithreaded BLAS ZGEMM on the host's {os.cpu_count()} "
+                      f"threads) on the whole tree: {sec:.2f} s",
         }
     return out
 
@@ -865,12 +944,17 @@ def run_cuda(args) -> None:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    if args.exact_tree_only:
-        # The exact-tree leg alone (profiling runs): one JSON line with the leg.
+    if args.tree_only:
+        # The contraction-tree legs alone (profiling runs): one JSON line.
         ctx = W.Context(local)
-        leg = exact_tree_leg(W, ctx, measured_copy_peak(torch), 0.0 if args.no_cpu_baseline else args.cpu_budget)
+        budget = 0.0 if args.no_cpu_baseline else args.cpu_budget
+        legs = {}
+        if args.tree_only in ("exact", "both"):
+            legs["exact_tree"] = exact_tree_leg(W, ctx, measured_copy_peak(torch), budget)
+        if args.tree_only in ("network", "both"):
+            legs["network_tree"] = network_tree_leg(W, ctx, measured_fp64_peak(torch), budget)
         if rank == 0:
-            print(json.dumps({"exact_tree": leg}), flush=True)
+            print(json.dumps(legs), flush=True)
         return
     w = workload(args.workload, args.depth)
     g0, windows = timed_windows(w, SATURATED_LAYERS.get(args.workload, 0), args.steps)
@@ -1027,6 +1111,8 @@ def run_cuda(args) -> None:
             line["one_qubit_layer"] = one_qubit_layer_leg(W, torch, ctx, copy_peak)
         if world == 1 and args.exact_tree_leg:
             line["exact_tree"] = exact_tree_leg(W, ctx, copy_peak, 0.0 if args.no_cpu_baseline else args.cpu_budget)
+        if world == 1 and args.network_tree_leg:
+            line["network_tree"] = network_tree_leg(W, ctx, peak, 0.0 if args.no_cpu_baseline else args.cpu_budget)
         if world == 1 and args.batch_slices > 0:
             line["batch"] = batch_leg(W, torch, ctx, args.batch_slices, flush,
                                       0.0 if args.no_cpu_baseline else args.cpu_budget)
@@ -1066,8 +1152,10 @@ def main():
                     help="skip the one-qubit layer over a saturated chi 256 state (HBM bandwidth of apply_1q_kernel)")
     ap.add_argument("--no-exact-tree-leg", dest="exact_tree_leg", action="store_false",
                     help="skip the 25-qubit exact contraction tree (wqc_exact_contract)")
-    ap.add_argument("--exact-tree-only", action="store_true",
-                    help="run only the exact contraction tree leg and print it (for profiling)")
+    ap.add_argument("--no-network-tree-leg", dest="network_tree_leg", action="store_false",
+                    help="skip the 25-qubit grid network contraction tree (wqc_network_contract)")
+    ap.add_argument("--tree-only", choices=("exact", "network", "both"), default=None,
+                    help="run only the contraction-tree leg(s) and print them (for profiling)")
     ap.add_argument("--no-trace-leg", dest="trace_leg", action="store_false",
                     help="skip the trace loop's call pattern (per-step reads) on the headline circuit")
     ap.add_argument("--no-exact-rule-leg", dest="exact_rule_leg", action="store_false",

@@ -419,9 +419,11 @@ typedef struct wqc_tree_node {
     wqc_tree_ref left, right;
 } wqc_tree_node;
 
-/* ContractionTree { site_order, nodes, peak_bytes } (src/tn/tree.rs).  The
- * site order must be empty or the identity (exact trees keep the parent's
- * wire numbers); has_peak 0 stands for peak_bytes: None. */
+/* ContractionTree { kind, site_order, nodes, peak_bytes } (src/tn/tree.rs).
+ * The site order must be empty or the identity (exact and network trees keep
+ * the parent's wire numbers); has_peak 0 stands for peak_bytes: None; kind 1
+ * is ContractionKind::Network, 0 an absent kind (the caller's dispatch picks
+ * wqc_exact_* or wqc_network_* by it, tree.rs:178-205). */
 typedef struct wqc_tree {
     const wqc_tree_node* nodes;
     uint32_t node_count;
@@ -429,6 +431,7 @@ typedef struct wqc_tree {
     uint32_t site_order_len;
     int32_t has_peak;
     uint64_t peak_bytes;
+    int32_t kind;
 } wqc_tree;
 
 typedef struct wqc_exact wqc_exact;
@@ -460,6 +463,11 @@ WQC_API wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t qubit_count, const
                                       const wqc_tree* tree, const uint64_t* mps_site_order,
                                       uint32_t mps_site_order_len, const uint64_t* bits, uint32_t count, double* out);
 
+/* Size of the register tiles that states of 12 or more legs are swept in:
+ * 2^bits amplitudes per block, bits 12 (256 threads) or 13 (512 threads,
+ * the default).  A tuning knob: results do not depend on it. */
+WQC_API wqc_status wqc_exact_set_tile_bits(wqc_exact* ex, int32_t bits);
+
 /* Stop a contraction in progress (the reference's cancel::check per gate,
  * exact.rs:419-421): the running call returns WQC_ERR_CANCELLED at its next
  * launch; a cancel that arrives between calls stops the next call.  Safe to
@@ -477,8 +485,57 @@ typedef struct wqc_exact_stats {
     uint64_t pass_bytes;     /* bytes those passes read and wrote (16 B per amplitude, both ways) */
     uint64_t bytes_moved;    /* bytes every launch read and wrote, by its access pattern */
     uint64_t arena_bytes;    /* device arena the tensors were placed in */
+    uint32_t exchanges;      /* register-tile exchanges through shared memory, over all passes */
 } wqc_exact_stats;
 WQC_API wqc_status wqc_exact_last_stats(wqc_exact* ex, wqc_exact_stats* out);
+
+/* ---------------------------------------------------------------------------
+ * Network contraction trees (src/tn/network.rs): <0...0|U|0...0> of the
+ * circuit as one tensor network.  Wire w starts at a ket0(w) leaf and ends
+ * at a bra0(w) leaf; unitary gate i is a gate(i) leaf with an input and an
+ * output leg per wire, or, for CNOT and CZ, two halves control(i) and
+ * target(i) joined by a bond.  A node contracts two tensors over the legs
+ * they share (a permutation of each operand, then a complex GEMM), at most
+ * 26 legs per tensor and a declared peak of at most 1 GiB, with the
+ * reference's byte accounting (network.rs:17-27).  The tree's kind must be 1.
+ * ------------------------------------------------------------------------- */
+typedef struct wqc_network wqc_network;
+WQC_API wqc_status wqc_network_create(wqc_cuda_ctx* ctx, wqc_network** out);
+WQC_API void wqc_network_destroy(wqc_network* net);
+
+/* network::validate (network.rs:128-143): the declared peak against the
+ * walk's, host only. */
+WQC_API wqc_status wqc_network_validate(uint32_t qubit_count, const wqc_gate* gates, uint32_t gate_count,
+                                        const wqc_tree* tree, const uint64_t* mps_site_order,
+                                        uint32_t mps_site_order_len);
+
+/* measured_peak (network.rs:162-169): the walk's peak, host only. */
+WQC_API wqc_status wqc_network_measured_peak(uint32_t qubit_count, const wqc_gate* gates, uint32_t gate_count,
+                                             const wqc_tree* tree, uint64_t* peak);
+
+/* contract_network (network.rs:145-160): out[0], out[1] = <0...0|U|0...0>.
+ * Every failure the reference reports is returned before any device work.
+ * Synchronous. */
+WQC_API wqc_status wqc_network_contract(wqc_network* net, uint32_t qubit_count, const wqc_gate* gates,
+                                        uint32_t gate_count, const wqc_tree* tree, const uint64_t* mps_site_order,
+                                        uint32_t mps_site_order_len, double out[2]);
+
+/* As wqc_exact_cancel (network.rs:202-204 checks per node). */
+WQC_API void wqc_network_cancel(wqc_network* net);
+
+typedef struct wqc_network_stats {
+    uint32_t nodes;          /* contractions */
+    uint32_t permutes;       /* operands reordered on the device */
+    uint32_t gemms;          /* complex GEMMs (cuBLAS ZGEMM) */
+    uint32_t launches;       /* device launches, the GEMMs' included */
+    double device_ms;        /* CUDA-event time of the device work */
+    double permute_ms;       /* part of it in permutations (timed one by one) */
+    double gemm_ms;          /* part of it in GEMMs (timed one by one) */
+    uint64_t permute_bytes;  /* bytes the permutations read and wrote */
+    double gemm_flops;       /* real flops of the GEMMs (8 m n k each) */
+    uint64_t arena_bytes;    /* device arena of the tensors */
+} wqc_network_stats;
+WQC_API wqc_status wqc_network_last_stats(wqc_network* net, wqc_network_stats* out);
 
 #ifdef __cplusplus
 }

@@ -81,7 +81,7 @@ def test_plan_rs_known_answers(ex):
         d = dense(n, gates)
         assert np.max(np.abs(got - d[bits])) < DENSE_TOL, (n, bits)
         for b, a in zip(bits, got):
-            assert abs(a - oracle_amp(n, gates, tree, b)) <= ORACLE_TOL
+            assert abs(a - oracle_amp(n, gates, tree, b)) <= ORACLE_TOL, (n, b)
     gates = C.gates_array([C.g1(C.H, q) for q in range(50)])
     assert abs(ex.contract(50, gates, P.plan_greedy(50, gates)) - 2.0 ** -25) < 1e-15
 
@@ -120,6 +120,29 @@ def test_wide_pass_trees_against_dense(ex):
     n, gates = 18, C.ry_cnot_brickwork(18, 6)
     tree = P.plan_greedy(n, gates)
     assert abs(ex.contract(n, gates, tree, 77) - oracle_amp(n, gates, tree, 77)) <= ORACLE_TOL
+
+
+@pytest.mark.parametrize("tile", [12, 13])
+def test_register_tiles_every_gate_kind(cuda_ctx, tile):
+    """States past the tile size with every gate kind: targets on lane,
+    register and warp bits (exchanges), controls and diagonal bits inside and
+    outside the tile, exact gates moved past others; equal to the oracle."""
+    ex = X.ExactContractor(cuda_ctx)
+    ex.set_tile_bits(tile)
+    rng = np.random.default_rng(tile)
+    for n in (tile, 15, 17):
+        gates = random_circuit(rng, n, 320)
+        tree = P.plan_greedy(n, gates)
+        bits = rng.integers(0, 1 << n, size=256)
+        got = ex.contract(n, gates, tree, bits)
+        st = ex.stats()
+        assert st["exchanges"] > 0 and st["gates"] == len(gates)
+        assert np.max(np.abs(got - dense(n, gates)[bits])) < DENSE_TOL, n
+        for b, a in zip(bits[:3], got[:3]):
+            assert a == oracle_amp(n, gates, tree, int(b)), (n, int(b))
+    with pytest.raises(WqcCudaError, match="12 or 13"):
+        ex.set_tile_bits(11)
+    ex.close()
 
 
 def inverse(gates):

@@ -31,27 +31,17 @@
 #include <vector>
 
 #include "../../include/wqc_cuda.h"
-
-namespace wqc {
-wqc_status record_error(wqc_status code, const std::string& msg);  // executor.cu
-wqc_status record_oom(uint64_t required, uint64_t available);
-wqc_status check_circuit_gate(int n, const wqc_gate& g);
-void gate_matrix_2x2(int kind, double theta, double2 out[4]);
-int context_device(const wqc_cuda_ctx* ctx);
-int context_sm_count(const wqc_cuda_ctx* ctx);
-}  // namespace wqc
+#include "tree_common.h"
 
 using namespace wqc;
+using namespace wqc::tree;
 
 namespace {
 
-constexpr int kMaxOpenLegs = 26;                 // exact.rs:25
-constexpr uint64_t kMaxPeakBytes = 1ull << 30;   // exact.rs:27
 constexpr int kLowBits = 4;                      // positions every pass holds: 16 amplitudes, 256 bytes
 constexpr int kMaxPassBits = 12;                 // 4096 amplitudes, 64 KB of shared memory per block
 constexpr int kPassThreads = 256;
 constexpr int kOuterThreads = 256;
-constexpr uint64_t kAlign = 256;                 // arena placement granularity (bytes)
 constexpr int kTimedPassLegs = 20;               // passes timed one by one for the stats
 
 enum PassKind : int32_t { kOne = 0, kCnot = 1, kCz = 2, kCcnot = 3 };
@@ -166,6 +156,203 @@ __global__ void __launch_bounds__(kPassThreads) exact_pass_kernel(double2* __res
     for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) state[base + hi_off[j >> low] + (j & low_mask)] = amp[j];
 }
 
+// ---------------------------------------------------------------------------
+// Register-tiled passes over tensors of at least 5 + WB + 4 legs.
+//
+// A block holds a tile of 2^(9 + WB) amplitudes: its local bits 0-4 are the
+// tensor's positions 0-4 (the lanes of a warp, so every warp-wide load or
+// store is 512 contiguous bytes), the other 4 + WB local bits are the tile's
+// high positions, of which 4 are register bits (each thread holds 16
+// amplitudes) and WB are warp bits.  A gate whose target is a register bit
+// runs inside the thread; a target on a lane bit takes its partner by a warp
+// shuffle; a target on a warp bit first needs an exchange, which rewrites the
+// tile through shared memory with another choice of register bits.  Controls,
+// diagonal gates and CZ act where their bits are, in the tile or outside it
+// (bits of the block's base index).  The host plans the ops and the exchanges.
+// ---------------------------------------------------------------------------
+enum RegOpKind : int32_t { kXchg = 0, kDense = 1, kPerm = 2, kNeg = 3, kDiag = 4 };
+enum RegForm : int32_t { kGeneral = 0, kReal = 1 };
+constexpr int kLaneTarget = 16;  // RegOp::tgt >= kLaneTarget: lane bit tgt - kLaneTarget
+
+struct RegOp {
+    int32_t kind;  // RegOpKind
+    int32_t form;  // kDense: RegForm
+    int32_t tgt;   // kDense / kPerm: register bit 0..3, or kLaneTarget + lane bit
+    uint32_t c_lane, c_warp, c_reg, c_out;  // bits that must be set: controls (kPerm), the sign bits (kNeg),
+                                            // the one bit that picks u[3] over u[0] (kDiag); c_out over the tensor
+    uint32_t x_reg, x_warp;                 // kXchg: register / warp bits among the tile's high local bits
+    uint32_t pad;
+    double2 u[4];  // kDense / kDiag: the gate's matrix, row-major
+};
+
+struct RegPassHdr {
+    uint32_t mask;  // tensor positions of the tile (0-4 and the high ones)
+    int32_t legs;
+    int32_t nops;
+    uint32_t reg0, warp0;  // register / warp bits among the high local bits at the start
+};
+
+// The reference's two output amplitudes of a one-qubit gate on (v0, v1):
+// u00 v0 + u01 v1 and u10 v0 + u11 v1.  The real form drops the products of
+// zero imaginary parts, which are signed zeros that leave every sum's value
+// unchanged.
+template <int FORM>
+__device__ __forceinline__ double2 one_out(double2 a, double2 b, double2 v0, double2 v1) {
+    if (FORM == kReal)
+        return make_double2(__dadd_rn(__dmul_rn(a.x, v0.x), __dmul_rn(b.x, v1.x)),
+                            __dadd_rn(__dmul_rn(a.x, v0.y), __dmul_rn(b.x, v1.y)));
+    return xadd(xmul(a, v0), xmul(b, v1));
+}
+
+__device__ __forceinline__ double2 shfl_xor2(double2 v, int m) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+// The four register bits' places among the high local bits, and the high
+// local index of register r: the OR of the places of r's set bits, folded at
+// compile time for each unrolled r.
+struct RegBits {
+    uint32_t b[4];
+    __device__ __forceinline__ void set(uint32_t regm) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            b[i] = regm & (0u - regm);
+            regm &= regm - 1;
+        }
+    }
+    __device__ __forceinline__ uint32_t at(int r) const {
+        return ((r & 1) ? b[0] : 0u) | ((r & 2) ? b[1] : 0u) | ((r & 4) ? b[2] : 0u) | ((r & 8) ? b[3] : 0u);
+    }
+};
+
+__device__ __forceinline__ double2 sel(bool c, double2 a, double2 b) {
+    return make_double2(c ? a.x : b.x, c ? a.y : b.y);
+}
+
+// Gates on a register bit: pairs (r, r | 1 << TR) inside the thread.
+// Controlled forms select per pair, so the code stays straight-line.
+template <int TR, int FORM>
+__device__ __forceinline__ void dense_reg(double2 (&v)[16], const double2 (&u)[4]) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        if (r & (1 << TR)) continue;
+        const int r1 = r | (1 << TR);
+        const double2 v0 = v[r], v1 = v[r1];
+        v[r] = one_out<FORM>(u[0], u[1], v0, v1);
+        v[r1] = one_out<FORM>(u[2], u[3], v0, v1);
+    }
+}
+
+// A gate on a lane bit: the partner's amplitude by a warp shuffle.  The lane
+// with the bit clear computes u00 v0 + u01 v1, its partner u10 v0 + u11 v1;
+// v0 is the clear lane's amplitude on both.
+template <int FORM>
+__device__ __forceinline__ void dense_lane(double2 (&v)[16], const double2 (&u)[4], int tl, uint32_t lane) {
+    const bool hi = (lane >> tl) & 1u;
+    const double2 a = hi ? u[2] : u[0], b = hi ? u[3] : u[1];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        const double2 p = shfl_xor2(v[r], 1 << tl);
+        v[r] = one_out<FORM>(a, b, sel(hi, p, v[r]), sel(hi, v[r], p));
+    }
+}
+
+template <int TR>
+__device__ __forceinline__ void perm_reg(double2 (&v)[16], bool thread_ok, uint32_t c_reg) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        if (r & (1 << TR)) continue;
+        const int r1 = r | (1 << TR);
+        const bool ok = thread_ok && (uint32_t(r) & c_reg) == c_reg;
+        const double2 v0 = v[r], v1 = v[r1];
+        v[r] = sel(ok, v1, v0);
+        v[r1] = sel(ok, v0, v1);
+    }
+}
+
+// One-qubit gates with two nonzero entries per row (H, Y, RX, RY); they
+// carry no controls.
+template <int FORM>
+__device__ __forceinline__ void dense_dispatch(double2 (&v)[16], const double2 (&u)[4], int t, uint32_t lane) {
+    switch (t) {
+        case 0: dense_reg<0, FORM>(v, u); return;
+        case 1: dense_reg<1, FORM>(v, u); return;
+        case 2: dense_reg<2, FORM>(v, u); return;
+        case 3: dense_reg<3, FORM>(v, u); return;
+        default: dense_lane<FORM>(v, u, t - kLaneTarget, lane); return;
+    }
+}
+
+template <int WB>
+__global__ void __launch_bounds__(32 << WB, (WB == 3 ? 2 : 1))
+    exact_pass_reg_kernel(double2* __restrict__ state, RegPassHdr h, const RegOp* __restrict__ ops) {
+    constexpr int HB = WB + 4;  // high local bits
+    extern __shared__ double2 xbuf[];  // 2^(9 + WB) amplitudes, used by exchanges
+    __shared__ uint32_t hi_off[1 << HB];
+    const uint32_t all = h.legs >= 32 ? ~0u : ((1u << h.legs) - 1u);
+    const uint32_t base = deposit(blockIdx.x, all & ~h.mask);
+    for (uint32_t t = threadIdx.x; t < (1u << HB); t += blockDim.x) hi_off[t] = deposit(t, h.mask & ~31u);
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    constexpr uint32_t kHiAll = (1u << HB) - 1u;  // keeps every tile index below 2^(9 + WB)
+    RegBits rb;
+    rb.set(h.reg0 & kHiAll);
+    uint32_t wdep = deposit(w, h.warp0 & kHiAll);
+    double2 v[16];
+    const double2* src = state + base + lane;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = src[hi_off[wdep | rb.at(r)]];
+    for (int o = 0; o < h.nops; ++o) {
+        const RegOp& op = ops[o];
+        const int kind = op.kind;
+        if (kind == kXchg) {
+            __syncthreads();  // the previous exchange's reads are done
+#pragma unroll
+            for (int r = 0; r < 16; ++r) xbuf[lane | ((wdep | rb.at(r)) << 5)] = v[r];
+            __syncthreads();
+            rb.set(op.x_reg & kHiAll);
+            wdep = deposit(w, op.x_warp & kHiAll);
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = xbuf[lane | ((wdep | rb.at(r)) << 5)];
+            continue;
+        }
+        const uint32_t c_lane = op.c_lane, c_warp = op.c_warp, c_reg = op.c_reg, c_out = op.c_out;
+        const bool thread_ok = (lane & c_lane) == c_lane && (w & c_warp) == c_warp && (base & c_out) == c_out;
+        if (kind == kDense) {
+            const double2 u[4] = {op.u[0], op.u[1], op.u[2], op.u[3]};
+            if (op.form == kReal) dense_dispatch<kReal>(v, u, op.tgt, lane);
+            else dense_dispatch<kGeneral>(v, u, op.tgt, lane);
+        } else if (kind == kPerm) {
+            switch (op.tgt) {
+                case 0: perm_reg<0>(v, thread_ok, c_reg); break;
+                case 1: perm_reg<1>(v, thread_ok, c_reg); break;
+                case 2: perm_reg<2>(v, thread_ok, c_reg); break;
+                case 3: perm_reg<3>(v, thread_ok, c_reg); break;
+                default: {
+                    const int m = 1 << (op.tgt - kLaneTarget);
+#pragma unroll
+                    for (int r = 0; r < 16; ++r) {
+                        const double2 p = shfl_xor2(v[r], m);
+                        v[r] = sel(thread_ok && (uint32_t(r) & c_reg) == c_reg, p, v[r]);
+                    }
+                }
+            }
+        } else if (kind == kNeg) {
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+                v[r] = sel(thread_ok && (uint32_t(r) & c_reg) == c_reg, make_double2(-v[r].x, -v[r].y), v[r]);
+        } else {  // kDiag: exactly one of c_lane, c_warp, c_reg, c_out holds the gate's bit
+            const bool thread_bit = (lane & c_lane) | (w & c_warp) | (base & c_out);
+            const double2 u0 = op.u[0], u3 = op.u[3];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = xmul(sel(thread_bit || (uint32_t(r) & c_reg), u3, u0), v[r]);
+        }
+    }
+    double2* dst = state + base + lane;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) dst[hi_off[wdep | rb.at(r)]] = v[r];
+}
+
 // out[i] = left[extract(i, lmask)] * right[extract(i, rmask)] over the sorted
 // union of the two tensors' wires (exact.rs:444-480).  The extractions come
 // from four 7-bit tables per operand (28 bits >= 26 legs).  Bounds: i <
@@ -210,62 +397,6 @@ __global__ void exact_gather_kernel(const double2* __restrict__ arena, const uin
 // Host side: the walk.
 // ---------------------------------------------------------------------------
 
-wqc_status failx(const std::string& msg) { return record_error(WQC_ERR_INVALID, msg); }
-wqc_status fail_index(uint64_t index, uint64_t limit) {
-    return record_error(WQC_ERR_QUBIT_OUT_OF_RANGE, "Qubit index " + std::to_string(index) +
-                                                        " out of bounds (limit: " + std::to_string(limit) + ")");
-}
-
-bool is_unitary(int kind) { return kind >= WQC_GATE_H && kind <= WQC_GATE_CCNOT; }
-
-std::vector<uint32_t> wires_of(const wqc_gate& g) {
-    switch (g.kind) {
-        case WQC_GATE_CNOT: case WQC_GATE_CZ: return {uint32_t(g.q0), uint32_t(g.q1)};
-        case WQC_GATE_CCNOT: return {uint32_t(g.q0), uint32_t(g.q1), uint32_t(g.q2)};
-        default: return {uint32_t(g.q0)};
-    }
-}
-
-// canonicalize_site_order (src/tn/tree.rs:442-457) with validate_site_order
-// (src/tn/site_order.rs:7-31): an empty or identity order is "no order".
-wqc_status canonical_empty(uint32_t n, const uint64_t* order, uint32_t len, bool* empty) {
-    *empty = true;
-    if (len == 0) return WQC_OK;
-    if (len != n)
-        return failx("mps_site_order length " + std::to_string(len) + " != qubit_count " + std::to_string(n));
-    std::vector<char> seen(n, 0);
-    for (uint32_t i = 0; i < len; ++i) {
-        if (order[i] >= n) return fail_index(order[i], n);
-        if (seen[order[i]])
-            return failx("mps_site_order is not a permutation (duplicate logical " + std::to_string(order[i]) + ")");
-        seen[order[i]] = 1;
-    }
-    for (uint32_t i = 0; i < len; ++i)
-        if (order[i] != i) *empty = false;
-    return WQC_OK;
-}
-
-// check_shape (exact.rs:99-134).
-wqc_status check_shape(uint32_t n, const wqc_gate* gates, uint32_t gate_count, const wqc_tree* tree,
-                       const uint64_t* mps_order, uint32_t mps_len) {
-    if (n == 0) return record_error(WQC_ERR_INVALID_QUBIT_COUNT, "Invalid qubit count: 0. Max limit is 40.");
-    if (gate_count && !gates) return failx("null gate list");
-    for (uint32_t i = 0; i < gate_count; ++i)
-        if (wqc_status s = check_circuit_gate(int(std::min<uint32_t>(n, 0x7fffffff)), gates[i])) return s;
-    if (tree->site_order_len && !tree->site_order) return failx("null site order");
-    std::vector<uint64_t> so(tree->site_order, tree->site_order + tree->site_order_len);
-    bool empty = true;
-    if (wqc_status s = canonical_empty(n, so.data(), uint32_t(so.size()), &empty)) return s;
-    if (!empty) return failx("contraction tree keeps parent wire numbers");
-    if (mps_order) {
-        for (uint32_t i = 0; i < mps_len; ++i)
-            if (mps_order[i] > 0xffffffffull) return failx("qubit index exceeds u32");
-        if (wqc_status s = canonical_empty(n, mps_order, mps_len, &empty)) return s;
-        if (!empty) return failx("mps_site_order does not match the contraction tree");
-    }
-    return WQC_OK;
-}
-
 // declared_peak (exact.rs:87-97).
 wqc_status declared_peak(const wqc_tree* tree, uint64_t* out) {
     if (!tree->has_peak) return failx("exact contraction tree requires a peak");
@@ -285,70 +416,42 @@ struct Buffer {
     std::vector<uint32_t> pending;  // gates queued on this state, circuit order
 };
 struct Item {
-    int kind;  // 0 pass, 1 outer
+    int kind;  // 0 shared-memory pass, 1 outer product, 2 register-tiled pass
     PassHdr hdr;
+    RegPassHdr rhdr;
     int buf;             // pass: the state; outer: the result
     int lbuf, rbuf;      // outer: the operands
-    uint32_t gate_off;   // pass: first gate in the pass-gate table
+    uint32_t gate_off;   // pass: first gate (kind 0) or op (kind 2) in its table
+    bool xchg;           // kind 2: the pass exchanges (needs the shared-memory tile)
     uint32_t lmask, rmask;
     int legs;
 };
 
-// First-fit placement of tensors in the arena, done while planning; the
-// device work runs in plan order on one stream, so a freed range is reused
-// only by work that comes after its last reader.
-struct Placer {
-    std::map<uint64_t, uint64_t> free_;  // byte offset -> bytes
-    uint64_t top = 0;
-    uint64_t alloc(uint64_t bytes) {
-        bytes = (bytes + kAlign - 1) / kAlign * kAlign;
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second >= bytes) {
-                const uint64_t off = it->first, rest = it->second - bytes;
-                free_.erase(it);
-                if (rest) free_[off + bytes] = rest;
-                return off;
-            }
-        }
-        // Grow from the top, merging a free range that ends there.
-        if (!free_.empty()) {
-            auto last = std::prev(free_.end());
-            if (last->first + last->second == top) {
-                const uint64_t off = last->first;
-                free_.erase(last);
-                top = off + bytes;
-                return off;
-            }
-        }
-        const uint64_t off = top;
-        top += bytes;
-        return off;
-    }
-    void release(uint64_t off, uint64_t bytes) {
-        bytes = (bytes + kAlign - 1) / kAlign * kAlign;
-        auto it = free_.emplace(off, bytes).first;
-        auto next = std::next(it);
-        if (next != free_.end() && it->first + it->second == next->first) {
-            it->second += next->second;
-            free_.erase(next);
-        }
-        if (it != free_.begin()) {
-            auto prev = std::prev(it);
-            if (prev->first + prev->second == it->first) {
-                prev->second += it->second;
-                free_.erase(it);
-            }
-        }
-    }
+// How a gate runs in a register-tiled pass, and whether it may move past
+// gates on other positions.  Gates whose arithmetic rounds (H, T, RX, RY, RZ)
+// keep their circuit order among themselves; the others (X, Y, Z, S, CNOT,
+// CZ, CCNOT) only permute amplitudes and multiply them by +-1 or +-i, which
+// commutes exactly with any gate on other positions.
+struct Sched {
+    int kind = kDense;  // RegOpKind
+    int form = kGeneral;
+    bool exact = false;
+    int tgt = -1;        // tensor position of the target (kDense, kPerm)
+    uint32_t bits = 0;   // controls (kPerm), sign bits (kNeg), the bit (kDiag)
+    uint32_t all = 0;    // every position the gate touches
+    double2 u[4] = {};
 };
 
 struct Plan {
     bool on = false;
     int pass_bits = kMaxPassBits;
+    int tile_wb = 4;  // warp bits of a register tile: tiles of 2^(9 + tile_wb) amplitudes
     const wqc_gate* gates = nullptr;
     std::vector<Buffer> bufs;
     std::vector<Item> items;
     std::vector<PassGate> pass_gates;
+    std::vector<RegOp> reg_ops;
+    uint32_t exchanges = 0;
     Placer placer;
     uint32_t kets = 0;  // ket slots (32 bytes each) at the arena's start
     uint64_t bytes_moved = 0;
@@ -374,12 +477,168 @@ struct Plan {
         if (!b.ket) placer.release(b.off * 16, 16ull << b.legs);
     }
 
+    Sched classify(const wqc_gate& g, const std::vector<uint32_t>& wires) const {
+        auto pos = [&](int q) { return int(std::lower_bound(wires.begin(), wires.end(), uint32_t(q)) - wires.begin()); };
+        Sched s;
+        switch (g.kind) {
+            case WQC_GATE_CNOT:
+                s.kind = kPerm, s.exact = true, s.tgt = pos(g.q1), s.bits = 1u << pos(g.q0);
+                break;
+            case WQC_GATE_CCNOT:
+                s.kind = kPerm, s.exact = true, s.tgt = pos(g.q2), s.bits = (1u << pos(g.q0)) | (1u << pos(g.q1));
+                break;
+            case WQC_GATE_CZ:
+                s.kind = kNeg, s.exact = true, s.bits = (1u << pos(g.q0)) | (1u << pos(g.q1));
+                break;
+            case WQC_GATE_X:
+                s.kind = kPerm, s.exact = true, s.tgt = pos(g.q0);
+                break;
+            case WQC_GATE_Z:
+                s.kind = kNeg, s.exact = true, s.bits = 1u << pos(g.q0);
+                break;
+            case WQC_GATE_S: case WQC_GATE_T: case WQC_GATE_RZ:
+                s.kind = kDiag, s.exact = g.kind == WQC_GATE_S, s.bits = 1u << pos(g.q0);
+                gate_matrix_2x2(g.kind, g.angle, s.u);
+                break;
+            default:  // H, Y, RX, RY
+                s.kind = kDense, s.exact = g.kind == WQC_GATE_Y, s.tgt = pos(g.q0);
+                gate_matrix_2x2(g.kind, g.angle, s.u);
+                s.form = (s.u[0].y == 0.0 && s.u[1].y == 0.0 && s.u[2].y == 0.0 && s.u[3].y == 0.0) ? kReal : kGeneral;
+                break;
+        }
+        s.all = s.bits | (s.tgt >= 0 ? 1u << s.tgt : 0u);
+        return s;
+    }
+
+    // One register-tiled pass: the gates `g` (execution order) on a state of
+    // `legs` legs whose targets outside positions 0-4 are `targets`.
+    void emit_reg_pass(int id, int legs, const std::vector<Sched>& g, uint32_t targets) {
+        const int HB = tile_wb + 4;
+        std::vector<int> hi;  // tensor positions of the high local bits, ascending
+        for (int p = 5; p < legs; ++p)
+            if (targets & (1u << p)) hi.push_back(p);
+        for (int p = 5; p < legs && int(hi.size()) < HB; ++p)
+            if (!(targets & (1u << p))) hi.push_back(p);
+        std::sort(hi.begin(), hi.end());
+        uint32_t mask = 0x1fu;
+        for (int p : hi) mask |= 1u << p;
+        auto hb_of = [&](int p) { return int(std::lower_bound(hi.begin(), hi.end(), p) - hi.begin()); };
+        auto rank = [](uint32_t m, int b) { return __builtin_popcount(m & ((1u << b) - 1u)); };
+        const uint32_t hi_all = (1u << HB) - 1u;
+        // The high bit each op needs in registers, or -1.
+        std::vector<int> use(g.size(), -1);
+        for (size_t i = 0; i < g.size(); ++i)
+            if ((g[i].kind == kDense || g[i].kind == kPerm) && g[i].tgt >= 5) use[i] = hb_of(g[i].tgt);
+        uint32_t regm = 0;
+        for (size_t i = 0; i < g.size() && __builtin_popcount(regm) < 4; ++i)
+            if (use[i] >= 0) regm |= 1u << use[i];
+        for (int b = 0; b < HB && __builtin_popcount(regm) < 4; ++b) regm |= 1u << b;
+        Item it{};
+        it.kind = 2;
+        it.buf = id;
+        it.legs = legs;
+        it.gate_off = uint32_t(reg_ops.size());
+        it.rhdr.mask = mask;
+        it.rhdr.legs = legs;
+        it.rhdr.reg0 = regm;
+        it.rhdr.warp0 = hi_all & ~regm;
+        for (size_t i = 0; i < g.size(); ++i) {
+            if (use[i] >= 0 && !(regm & (1u << use[i]))) {
+                // Keep in registers the four high bits needed soonest (Belady).
+                std::vector<std::pair<size_t, int>> next;  // (next use, bit)
+                for (int b = 0; b < HB; ++b) {
+                    size_t nu = g.size() + 1;
+                    for (size_t j = i; j < g.size(); ++j)
+                        if (use[j] == b) {
+                            nu = j;
+                            break;
+                        }
+                    // prefer bits already in registers on ties
+                    next.emplace_back(nu * 2 + ((regm >> b) & 1u ? 0 : 1), b);
+                }
+                std::sort(next.begin(), next.end());
+                uint32_t nm = 0;
+                for (int k = 0; k < 4; ++k) nm |= 1u << next[size_t(k)].second;
+                RegOp x{};
+                x.kind = kXchg;
+                x.x_reg = nm;
+                x.x_warp = hi_all & ~nm;
+                reg_ops.push_back(x);
+                regm = nm;
+                it.xchg = true;
+                ++exchanges;
+            }
+            const uint32_t warpm = hi_all & ~regm;
+            RegOp op{};
+            op.kind = g[i].kind;
+            op.form = g[i].form;
+            for (int k = 0; k < 4; ++k) op.u[k] = g[i].u[k];
+            if (g[i].tgt >= 0)
+                op.tgt = g[i].tgt < 5 ? kLaneTarget + g[i].tgt : rank(regm, hb_of(g[i].tgt));
+            for (uint32_t m = g[i].bits; m; m &= m - 1) {
+                const int p = __builtin_ctz(m);
+                if (p < 5) {
+                    op.c_lane |= 1u << p;
+                } else if (mask & (1u << p)) {
+                    const int b = hb_of(p);
+                    if (regm & (1u << b)) op.c_reg |= 1u << rank(regm, b);
+                    else op.c_warp |= 1u << rank(warpm, b);
+                } else {
+                    op.c_out |= 1u << p;
+                }
+            }
+            reg_ops.push_back(op);
+        }
+        it.rhdr.nops = int(reg_ops.size() - it.gate_off);
+        items.push_back(it);
+        bytes_moved += 2 * (16ull << legs);
+    }
+
+    // The queued gates of a state of at least 9 + tile_wb legs as register-
+    // tiled passes.  A pass takes, in circuit order, every gate whose target
+    // fits its 4 + tile_wb high positions; a gate that does not fit waits for
+    // the next pass, and so does every later gate that shares a position with
+    // a waiting gate, or that rounds while a rounding gate waits.  The waiting
+    // gates keep their order.
+    void flush_reg(Buffer& b, const std::vector<uint32_t>& wires, int id) {
+        const int cap = tile_wb + 4;
+        std::vector<Sched> pending;
+        for (uint32_t gi : b.pending) pending.push_back(classify(gates[gi], wires));
+        while (!pending.empty()) {
+            std::vector<Sched> placed, waiting;
+            uint32_t targets = 0, blocked = 0;
+            bool chain_blocked = false;
+            for (const Sched& s : pending) {
+                bool take = !(s.all & blocked) && (s.exact || !chain_blocked);
+                if (take && s.tgt >= 5 && !(targets & (1u << s.tgt))) {
+                    if (__builtin_popcount(targets) < cap) targets |= 1u << s.tgt;
+                    else take = false;
+                }
+                if (take) {
+                    placed.push_back(s);
+                } else {
+                    waiting.push_back(s);
+                    blocked |= s.all;
+                    if (!s.exact) chain_blocked = true;
+                }
+            }
+            emit_reg_pass(id, b.legs, placed, targets);
+            pending.swap(waiting);
+        }
+    }
+
     // Turn the queued gates of a state into passes (wires are the state's
     // sorted open wires; position p holds wires[p]).
     void flush(int id, const std::vector<uint32_t>& wires) {
         Buffer& b = bufs[size_t(id)];
         if (b.pending.empty()) return;
         const int legs = b.legs;
+        if (legs >= 9 + tile_wb) {
+            flush_reg(b, wires, id);
+            gate_total += uint32_t(b.pending.size());
+            b.pending.clear();
+            return;
+        }
         auto pos_of = [&](uint32_t wire) {
             return int(std::lower_bound(wires.begin(), wires.end(), wire) - wires.begin());
         };
@@ -609,11 +868,6 @@ struct Walker {
     }
 };
 
-wqc_status check_tree(const wqc_tree* tree) {
-    if (!tree) return failx("null contraction tree");
-    if (tree->node_count && !tree->nodes) return failx("null contraction tree nodes");
-    return WQC_OK;
-}
 
 }  // namespace
 
@@ -625,6 +879,7 @@ struct wqc_exact {
     int device = 0;
     int sm_count = 148;
     int pass_bits = kMaxPassBits;
+    int tile_bits = 13;  // register tiles of 2^13 amplitudes (512 threads x 16)
     cudaStream_t stream = nullptr;
     double2* arena = nullptr;
     uint64_t arena_bytes = 0;
@@ -702,14 +957,16 @@ wqc_status wqc_exact_create(wqc_cuda_ctx* ctx, wqc_exact** out) {
     ex->ctx = ctx;
     ex->device = context_device(ctx);
     ex->sm_count = context_sm_count(ctx);
-    if (const char* env = std::getenv("WQC_EXACT_PASS_BITS")) {
-        const int b = std::atoi(env);
-        if (b >= kLowBits + 3 && b <= kMaxPassBits) ex->pass_bits = b;
-    }
     cudaError_t e = cudaSetDevice(ex->device);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(exact_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sizeof(double2)) << kMaxPassBits);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(exact_pass_reg_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sizeof(double2)) << 12);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(exact_pass_reg_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sizeof(double2)) << 13);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ex->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete ex;
@@ -729,6 +986,13 @@ void wqc_exact_destroy(wqc_exact* ex) {
     if (ex->staging) cudaFreeHost(ex->staging);
     if (ex->stream) cudaStreamDestroy(ex->stream);
     delete ex;
+}
+
+wqc_status wqc_exact_set_tile_bits(wqc_exact* ex, int32_t bits) {
+    if (!ex) return failx("null executor");
+    if (bits != 12 && bits != 13) return failx("tile bits must be 12 or 13");
+    ex->tile_bits = bits;
+    return WQC_OK;
 }
 
 void wqc_exact_cancel(wqc_exact* ex) {
@@ -773,6 +1037,7 @@ wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t n, const wqc_gate* gates, 
     Plan plan;
     plan.on = true;
     plan.pass_bits = ex->pass_bits;
+    plan.tile_wb = ex->tile_bits - 9;
     plan.gates = gates;
     Walker w(n, gates, gate_count, tree->node_count, &plan);
     uint64_t peak = 0;
@@ -796,7 +1061,9 @@ wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t n, const wqc_gate* gates, 
     const size_t T = order.size();
     const uint64_t gather_n = uint64_t(count) * T;
     if (gather_n > (1ull << 28)) return failx("too many amplitudes for one contraction");
-    const uint64_t gates_bytes = (plan.pass_gates.size() * sizeof(PassGate) + kAlign - 1) / kAlign * kAlign;
+    const uint64_t pg_bytes = (plan.pass_gates.size() * sizeof(PassGate) + kAlign - 1) / kAlign * kAlign;
+    const uint64_t ops_bytes = (plan.reg_ops.size() * sizeof(RegOp) + kAlign - 1) / kAlign * kAlign;
+    const uint64_t gates_bytes = pg_bytes + ops_bytes;
     const uint64_t where_bytes = (gather_n * sizeof(uint64_t) + kAlign - 1) / kAlign * kAlign;
     const uint64_t comp_bytes = std::max<uint64_t>(gather_n * sizeof(double2), 16);
     const uint64_t table_need = gates_bytes + where_bytes + comp_bytes;
@@ -809,6 +1076,8 @@ wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t n, const wqc_gate* gates, 
     // Stage the pass gates and the gather offsets.
     if (!plan.pass_gates.empty())
         std::memcpy(ex->staging, plan.pass_gates.data(), plan.pass_gates.size() * sizeof(PassGate));
+    if (!plan.reg_ops.empty())
+        std::memcpy(ex->staging + pg_bytes, plan.reg_ops.data(), plan.reg_ops.size() * sizeof(RegOp));
     uint64_t* where = reinterpret_cast<uint64_t*>(ex->staging + gates_bytes);
     const uint64_t tensor_base = ket_bytes / 16;  // element offset of the tensor region
     for (uint32_t k = 0; k < count; ++k) {
@@ -827,6 +1096,7 @@ wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t n, const wqc_gate* gates, 
         if (cudaError_t e = cudaMemcpyAsync(ex->table, ex->staging, upload, cudaMemcpyHostToDevice, st))
             return cuda_fail("cudaMemcpyAsync(exact tables)", e);
     const PassGate* d_gates = reinterpret_cast<const PassGate*>(ex->table);
+    const RegOp* d_ops = reinterpret_cast<const RegOp*>(ex->table + pg_bytes);
     const uint64_t* d_where = reinterpret_cast<const uint64_t*>(ex->table + gates_bytes);
     double2* d_comp = reinterpret_cast<double2*>(ex->table + gates_bytes + where_bytes);
     double2* kets = ex->arena;
@@ -852,7 +1122,7 @@ wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t n, const wqc_gate* gates, 
     }
     for (const Item& it : plan.items) {
         if (ex->cancel.exchange(0)) return bail(record_error(WQC_ERR_CANCELLED, "computation cancelled: the client has gone"));
-        if (it.kind == 0) {
+        if (it.kind == 0 || it.kind == 2) {
             const bool time_it = it.legs >= kTimedPassLegs;
             cudaEvent_t a = nullptr, b = nullptr;
             if (time_it) {
@@ -861,9 +1131,19 @@ wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t n, const wqc_gate* gates, 
                 if (!a || !b) return bail(record_error(WQC_ERR_CUDA, "cudaEventCreate failed"));
                 cudaEventRecord(a, st);
             }
-            const uint32_t grid = 1u << (it.legs - it.hdr.local);
-            exact_pass_kernel<<<grid, kPassThreads, size_t(16) << it.hdr.local, st>>>(at(it.buf), it.hdr,
-                                                                                       d_gates + it.gate_off);
+            if (it.kind == 0) {
+                const uint32_t grid = 1u << (it.legs - it.hdr.local);
+                exact_pass_kernel<<<grid, kPassThreads, size_t(16) << it.hdr.local, st>>>(at(it.buf), it.hdr,
+                                                                                           d_gates + it.gate_off);
+            } else {
+                const int tile = 9 + plan.tile_wb;  // grid: one block per tile, 2^(legs - tile) tiles
+                const uint32_t grid = 1u << (it.legs - tile);
+                const size_t smem = it.xchg ? size_t(16) << tile : 0;
+                if (plan.tile_wb == 3)
+                    exact_pass_reg_kernel<3><<<grid, 256, smem, st>>>(at(it.buf), it.rhdr, d_ops + it.gate_off);
+                else
+                    exact_pass_reg_kernel<4><<<grid, 512, smem, st>>>(at(it.buf), it.rhdr, d_ops + it.gate_off);
+            }
             if (time_it) {
                 cudaEventRecord(b, st);
                 timed.emplace_back(a, b);
@@ -916,6 +1196,7 @@ wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t n, const wqc_gate* gates, 
         ex->stats.pass_ms += t;
     }
     ex->stats.launches = launches;
+    ex->stats.exchanges = plan.exchanges;
     ex->stats.passes = passes;
     ex->stats.outer_products = outers;
     ex->stats.gates = plan.gate_total;

@@ -52,7 +52,9 @@ EXPORTS = (
     "wqc_mps_overlap", "wqc_cuda_last_oom", "wqc_mps_site_amplitudes_many", "wqc_mps_to_dense",
     "wqc_adjoint_forward", "wqc_adjoint_backward", "wqc_adjoint_destroy", "wqc_cuda_autotune",
     "wqc_exact_create", "wqc_exact_destroy", "wqc_exact_validate", "wqc_exact_measured_peak", "wqc_exact_contract",
-    "wqc_exact_cancel", "wqc_exact_last_stats",
+    "wqc_exact_cancel", "wqc_exact_last_stats", "wqc_exact_set_tile_bits",
+    "wqc_network_create", "wqc_network_destroy", "wqc_network_validate", "wqc_network_measured_peak",
+    "wqc_network_contract", "wqc_network_cancel", "wqc_network_last_stats",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")

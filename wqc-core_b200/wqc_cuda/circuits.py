@@ -254,3 +254,38 @@ def star(n: int) -> np.ndarray:
     """H on qubit 0, then CNOT(0, q) for every other qubit (a GHZ star,
     src/tn/exact.rs:668-676)."""
     return gates_array([g1(H, 0)] + [g2(CNOT, 0, q) for q in range(1, n)])
+
+
+def ry_rz_cnot_brickwork(n: int, depth: int) -> np.ndarray:
+    """Layers of RY(0.17 + 0.013 (q + 3 layer)) and RZ(0.31 + 0.007 (2q + layer))
+    on every qubit, then CNOT on alternating neighbour pairs (the network-tree
+    workload of src/tn/network.rs:1022-1036)."""
+    gates = []
+    for layer in range(depth):
+        for q in range(n):
+            gates.append(g1(RY, q, 0.17 + 0.013 * (q + 3 * layer)))
+            gates.append(g1(RZ, q, 0.31 + 0.007 * (2 * q + layer)))
+        for q in range(layer % 2, n - 1, 2):
+            gates.append(g2(CNOT, q, q + 1))
+    return gates_array(gates)
+
+
+def grid(side: int, depth: int) -> np.ndarray:
+    """RY(0.17) and RZ(0.31) on every qubit of a side x side grid, then CNOTs
+    on alternating pairs, two layers along rows and two along columns (the
+    orchestrator's grid circuit, src/tn/network.rs:1114-1139)."""
+    gates = []
+    at = lambda row, col: row * side + col  # noqa: E731
+    for layer in range(depth):
+        for q in range(side * side):
+            gates.append(g1(RY, q, 0.17))
+            gates.append(g1(RZ, q, 0.31))
+        if layer % 4 < 2:
+            for row in range(side):
+                for col in range(layer % 2, side - 1, 2):
+                    gates.append(g2(CNOT, at(row, col), at(row, col + 1)))
+        else:
+            for row in range(layer % 2, side - 1, 2):
+                for col in range(side):
+                    gates.append(g2(CNOT, at(row, col), at(row + 1, col)))
+    return gates_array(gates)

@@ -33,6 +33,7 @@ class _Tree(ctypes.Structure):
         ("site_order_len", ctypes.c_uint32),
         ("has_peak", ctypes.c_int32),
         ("peak_bytes", ctypes.c_uint64),
+        ("kind", ctypes.c_int32),
     ]
 
 
@@ -47,6 +48,7 @@ class ExactStats(ctypes.Structure):
         ("pass_bytes", ctypes.c_uint64),
         ("bytes_moved", ctypes.c_uint64),
         ("arena_bytes", ctypes.c_uint64),
+        ("exchanges", ctypes.c_uint32),
     ]
 
 
@@ -64,6 +66,7 @@ def _bind(L):
     L.wqc_exact_measured_peak.argtypes = [U32, P, U32, T, ctypes.POINTER(U64)]
     L.wqc_exact_contract.argtypes = [P, U32, P, U32, T, P, U32, P, U32, P]
     L.wqc_exact_last_stats.argtypes = [P, ctypes.POINTER(ExactStats)]
+    L.wqc_exact_set_tile_bits.argtypes = [P, ctypes.c_int32]
     L._exact_bound = True
     return L
 
@@ -103,10 +106,13 @@ class _TreeArgs:
         self.nodes = tree_nodes(tree.get("nodes", []))
         self.site_order = np.ascontiguousarray(tree.get("site_order", []) or [], dtype=np.uint32)
         pb = tree.get("peak_bytes") if peak else None
+        kind = tree.get("kind")
+        if kind not in (None, "network"):
+            raise ValueError(f"unknown contraction tree kind {kind!r}")
         self.struct = _Tree(
             self.nodes.ctypes.data if len(self.nodes) else None, len(self.nodes),
             self.site_order.ctypes.data if len(self.site_order) else None, len(self.site_order),
-            0 if pb is None else 1, 0 if pb is None else int(pb))
+            0 if pb is None else 1, 0 if pb is None else int(pb), 1 if kind == "network" else 0)
 
 
 def _gates(gates) -> np.ndarray:
@@ -175,6 +181,11 @@ class ExactContractor:
 
     def cancel(self) -> None:
         lib().wqc_exact_cancel(self._h)
+
+    def set_tile_bits(self, bits: int) -> None:
+        """Register tiles of 2^bits amplitudes (12 or 13) for states of 12 or
+        more legs; results do not depend on it."""
+        _check(lib().wqc_exact_set_tile_bits(self._h, bits))
 
     def contract(self, n: int, gates, tree, bits=0, mps_site_order=None):
         """Amplitude(s) of basis vector(s) `bits` (bit q = wire q): a complex
