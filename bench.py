@@ -818,14 +818,16 @@ def network_tree_leg(W, ctx, fp64_peak: float, cpu_budget: float) -> dict:
         "gemm_ms": st["gemm_ms"],
         "permute_ms": st["permute_ms"],
         "gemms": st["gemms"],
+        "small_contractions": st["small"],
+        "launches": st["launches"],
         "permutes": st["permutes"],
         "gemm_gflop": st["gemm_flops"] / 1e9,
         "permute_bytes": st["permute_bytes"],
         "amplitude": [amp.real, amp.imag],
         "amplitude_same_every_run": all(r[2] == amp for r in runs),
         "roofline": {
-            "bound": "fp64", "kernel": "cuBLAS ZGEMM of the contractions (GEMMs with results of >= 2^16 amplitudes "
-                                       "timed one by one; smaller ones are in device_ms only)",
+            "bound": "fp64", "kernel": "cuBLAS ZGEMM of the large contractions (each timed with CUDA events; the "
+                                       "level-batched small ones are in device_ms only)",
             "achieved": tflops, "peak": fp64_peak, "unit": "TFLOP/s",
             "frac": tflops / fp64_peak if tflops and fp64_peak else None,
             "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",

@@ -526,14 +526,15 @@ WQC_API void wqc_network_cancel(wqc_network* net);
 typedef struct wqc_network_stats {
     uint32_t nodes;          /* contractions */
     uint32_t permutes;       /* operands reordered on the device */
-    uint32_t gemms;          /* complex GEMMs (cuBLAS ZGEMM) */
+    uint32_t gemms;          /* complex GEMMs (cuBLAS ZGEMM) of the large contractions */
     uint32_t launches;       /* device launches, the GEMMs' included */
     double device_ms;        /* CUDA-event time of the device work */
-    double permute_ms;       /* part of it in permutations (timed one by one) */
-    double gemm_ms;          /* part of it in GEMMs (timed one by one) */
+    double permute_ms;       /* part of it in the large contractions' permutations (each timed) */
+    double gemm_ms;          /* part of it in their GEMMs (each timed) */
     uint64_t permute_bytes;  /* bytes the permutations read and wrote */
     double gemm_flops;       /* real flops of the GEMMs (8 m n k each) */
     uint64_t arena_bytes;    /* device arena of the tensors */
+    uint32_t small;          /* small contractions, run one block each in level-batched launches */
 } wqc_network_stats;
 WQC_API wqc_status wqc_network_last_stats(wqc_network* net, wqc_network_stats* out);
 

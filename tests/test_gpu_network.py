@@ -62,7 +62,7 @@ def test_orchestrator_trees(net):
         tree = json.loads(load_grid(name))
         check(net, 16, grid, tree, expected)
         st = net.stats()
-        assert st["gemms"] == len(tree["nodes"]) and st["launches"] >= st["gemms"]
+        assert st["gemms"] + st["small"] == len(tree["nodes"]) and st["launches"] >= st["gemms"]
 
 
 def test_skipped_ops_outer_products_and_reordered_copies(net):
@@ -131,6 +131,7 @@ def test_grid_5x5_depth_12_against_the_oracle(net):
     assert abs(got - ref) < ORACLE_TOL, (got, ref)
     st = net.stats()
     assert st["gemm_flops"] > 2e11 and st["gemm_ms"] > 0
+    assert st["small"] > 700 and st["launches"] < 200  # the small joins run level-batched
 
 
 def test_failures_come_before_device_work_and_cancel(net):

@@ -174,15 +174,18 @@ enum RegOpKind : int32_t { kXchg = 0, kDense = 1, kPerm = 2, kNeg = 3, kDiag = 4
 enum RegForm : int32_t { kGeneral = 0, kReal = 1 };
 constexpr int kLaneTarget = 16;  // RegOp::tgt >= kLaneTarget: lane bit tgt - kLaneTarget
 
+// One op of a register-tiled pass, read by every thread with one 16-byte load
+// plus the matrix it needs.  code: kind (bits 0-3) | form << 4 | tgt << 8 |
+// c_lane << 16 | c_warp << 21 | c_reg << 26, where the c_ masks are the bits
+// that must be set -- controls (kPerm), the sign bits (kNeg), the one bit that
+// picks u[3] over u[0] (kDiag) -- among the lane, warp and register bits;
+// c_out the same among the tensor positions outside the tile.  tgt is a
+// register bit 0..3, or kLaneTarget + a lane bit.
 struct RegOp {
-    int32_t kind;  // RegOpKind
-    int32_t form;  // kDense: RegForm
-    int32_t tgt;   // kDense / kPerm: register bit 0..3, or kLaneTarget + lane bit
-    uint32_t c_lane, c_warp, c_reg, c_out;  // bits that must be set: controls (kPerm), the sign bits (kNeg),
-                                            // the one bit that picks u[3] over u[0] (kDiag); c_out over the tensor
-    uint32_t x_reg, x_warp;                 // kXchg: register / warp bits among the tile's high local bits
-    uint32_t pad;
-    double2 u[4];  // kDense / kDiag: the gate's matrix, row-major
+    uint32_t code;
+    uint32_t c_out;
+    uint32_t x_reg, x_warp;  // kXchg: register / warp bits among the tile's high local bits
+    double2 u[4];  // kDense, form kReal: u[0] = (u00, u01), u[1] = (u10, u11) real parts; otherwise the matrix
 };
 
 struct RegPassHdr {
@@ -192,15 +195,14 @@ struct RegPassHdr {
     uint32_t reg0, warp0;  // register / warp bits among the high local bits at the start
 };
 
-// The reference's two output amplitudes of a one-qubit gate on (v0, v1):
-// u00 v0 + u01 v1 and u10 v0 + u11 v1.  The real form drops the products of
-// zero imaginary parts, which are signed zeros that leave every sum's value
-// unchanged.
-template <int FORM>
-__device__ __forceinline__ double2 one_out(double2 a, double2 b, double2 v0, double2 v1) {
-    if (FORM == kReal)
-        return make_double2(__dadd_rn(__dmul_rn(a.x, v0.x), __dmul_rn(b.x, v1.x)),
-                            __dadd_rn(__dmul_rn(a.x, v0.y), __dmul_rn(b.x, v1.y)));
+// The reference's output amplitude A v0 + B v1 of a one-qubit gate row
+// (u00 v0 + u01 v1, u10 v0 + u11 v1).  The real form drops the products of
+// zero imaginary parts, signed zeros that leave every sum's value unchanged.
+__device__ __forceinline__ double2 row_real(double a, double b, double2 v0, double2 v1) {
+    return make_double2(__dadd_rn(__dmul_rn(a, v0.x), __dmul_rn(b, v1.x)),
+                        __dadd_rn(__dmul_rn(a, v0.y), __dmul_rn(b, v1.y)));
+}
+__device__ __forceinline__ double2 row_general(double2 a, double2 b, double2 v0, double2 v1) {
     return xadd(xmul(a, v0), xmul(b, v1));
 }
 
@@ -229,34 +231,51 @@ __device__ __forceinline__ double2 sel(bool c, double2 a, double2 b) {
     return make_double2(c ? a.x : b.x, c ? a.y : b.y);
 }
 
-// Gates on a register bit: pairs (r, r | 1 << TR) inside the thread.
-// Controlled forms select per pair, so the code stays straight-line.
-template <int TR, int FORM>
-__device__ __forceinline__ void dense_reg(double2 (&v)[16], const double2 (&u)[4]) {
+// One-qubit gates with two nonzero entries per row (H, Y, RX, RY; no
+// controls).  On a register bit: pairs (r, r | 1 << TR) inside the thread.
+template <int TR>
+__device__ __forceinline__ void dense_reg_real(double2 (&v)[16], double a, double b, double c, double d) {
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
         if (r & (1 << TR)) continue;
         const int r1 = r | (1 << TR);
         const double2 v0 = v[r], v1 = v[r1];
-        v[r] = one_out<FORM>(u[0], u[1], v0, v1);
-        v[r1] = one_out<FORM>(u[2], u[3], v0, v1);
+        v[r] = row_real(a, b, v0, v1);
+        v[r1] = row_real(c, d, v0, v1);
     }
 }
-
-// A gate on a lane bit: the partner's amplitude by a warp shuffle.  The lane
-// with the bit clear computes u00 v0 + u01 v1, its partner u10 v0 + u11 v1;
-// v0 is the clear lane's amplitude on both.
-template <int FORM>
-__device__ __forceinline__ void dense_lane(double2 (&v)[16], const double2 (&u)[4], int tl, uint32_t lane) {
-    const bool hi = (lane >> tl) & 1u;
-    const double2 a = hi ? u[2] : u[0], b = hi ? u[3] : u[1];
+template <int TR>
+__device__ __forceinline__ void dense_reg_general(double2 (&v)[16], const double2 (&u)[4]) {
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
-        const double2 p = shfl_xor2(v[r], 1 << tl);
-        v[r] = one_out<FORM>(a, b, sel(hi, p, v[r]), sel(hi, v[r], p));
+        if (r & (1 << TR)) continue;
+        const int r1 = r | (1 << TR);
+        const double2 v0 = v[r], v1 = v[r1];
+        v[r] = row_general(u[0], u[1], v0, v1);
+        v[r1] = row_general(u[2], u[3], v0, v1);
     }
 }
 
+// On a lane bit: the partner's amplitude by a warp shuffle.  The lane with
+// the bit clear computes u00 v + u01 p, the lane with it set u11 v + u10 p
+// -- the reference's u10 v0 + u11 v1 with the two terms of the sum swapped,
+// which IEEE addition leaves bit-identical.
+__device__ __forceinline__ void dense_lane_real(double2 (&v)[16], double a, double b, double c, double d, int tl,
+                                                uint32_t lane) {
+    const bool hi = (lane >> tl) & 1u;
+    const double own = hi ? d : a, other = hi ? c : b;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = row_real(own, other, v[r], shfl_xor2(v[r], 1 << tl));
+}
+__device__ __forceinline__ void dense_lane_general(double2 (&v)[16], const double2 (&u)[4], int tl, uint32_t lane) {
+    const bool hi = (lane >> tl) & 1u;
+    const double2 own = hi ? u[3] : u[0], other = hi ? u[2] : u[1];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = row_general(own, other, v[r], shfl_xor2(v[r], 1 << tl));
+}
+
+// Swaps of the target pairs where the controls are set: thread-level
+// controls select whole pairs; register-bit controls select pair by pair.
 template <int TR>
 __device__ __forceinline__ void perm_reg(double2 (&v)[16], bool thread_ok, uint32_t c_reg) {
 #pragma unroll
@@ -267,19 +286,6 @@ __device__ __forceinline__ void perm_reg(double2 (&v)[16], bool thread_ok, uint3
         const double2 v0 = v[r], v1 = v[r1];
         v[r] = sel(ok, v1, v0);
         v[r1] = sel(ok, v0, v1);
-    }
-}
-
-// One-qubit gates with two nonzero entries per row (H, Y, RX, RY); they
-// carry no controls.
-template <int FORM>
-__device__ __forceinline__ void dense_dispatch(double2 (&v)[16], const double2 (&u)[4], int t, uint32_t lane) {
-    switch (t) {
-        case 0: dense_reg<0, FORM>(v, u); return;
-        case 1: dense_reg<1, FORM>(v, u); return;
-        case 2: dense_reg<2, FORM>(v, u); return;
-        case 3: dense_reg<3, FORM>(v, u); return;
-        default: dense_lane<FORM>(v, u, t - kLaneTarget, lane); return;
     }
 }
 
@@ -303,33 +309,62 @@ __global__ void __launch_bounds__(32 << WB, (WB == 3 ? 2 : 1))
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = src[hi_off[wdep | rb.at(r)]];
     for (int o = 0; o < h.nops; ++o) {
-        const RegOp& op = ops[o];
-        const int kind = op.kind;
+        const uint4 hd = __ldg(reinterpret_cast<const uint4*>(ops + o));
+        const uint32_t code = hd.x;
+        const int kind = int(code & 15u);
+        const int tgt = int((code >> 8) & 255u);
         if (kind == kXchg) {
             __syncthreads();  // the previous exchange's reads are done
 #pragma unroll
             for (int r = 0; r < 16; ++r) xbuf[lane | ((wdep | rb.at(r)) << 5)] = v[r];
             __syncthreads();
-            rb.set(op.x_reg & kHiAll);
-            wdep = deposit(w, op.x_warp & kHiAll);
+            rb.set(hd.z & kHiAll);
+            wdep = deposit(w, hd.w & kHiAll);
 #pragma unroll
             for (int r = 0; r < 16; ++r) v[r] = xbuf[lane | ((wdep | rb.at(r)) << 5)];
             continue;
         }
-        const uint32_t c_lane = op.c_lane, c_warp = op.c_warp, c_reg = op.c_reg, c_out = op.c_out;
-        const bool thread_ok = (lane & c_lane) == c_lane && (w & c_warp) == c_warp && (base & c_out) == c_out;
+        const double2* u = ops[o].u;
         if (kind == kDense) {
-            const double2 u[4] = {op.u[0], op.u[1], op.u[2], op.u[3]};
-            if (op.form == kReal) dense_dispatch<kReal>(v, u, op.tgt, lane);
-            else dense_dispatch<kGeneral>(v, u, op.tgt, lane);
-        } else if (kind == kPerm) {
-            switch (op.tgt) {
+            if (((code >> 4) & 15u) == kReal) {
+                const double2 ab = __ldg(u), cd = __ldg(u + 1);
+                switch (tgt) {
+                    case 0: dense_reg_real<0>(v, ab.x, ab.y, cd.x, cd.y); break;
+                    case 1: dense_reg_real<1>(v, ab.x, ab.y, cd.x, cd.y); break;
+                    case 2: dense_reg_real<2>(v, ab.x, ab.y, cd.x, cd.y); break;
+                    case 3: dense_reg_real<3>(v, ab.x, ab.y, cd.x, cd.y); break;
+                    default: dense_lane_real(v, ab.x, ab.y, cd.x, cd.y, tgt - kLaneTarget, lane); break;
+                }
+            } else {
+                const double2 m[4] = {__ldg(u), __ldg(u + 1), __ldg(u + 2), __ldg(u + 3)};
+                switch (tgt) {
+                    case 0: dense_reg_general<0>(v, m); break;
+                    case 1: dense_reg_general<1>(v, m); break;
+                    case 2: dense_reg_general<2>(v, m); break;
+                    case 3: dense_reg_general<3>(v, m); break;
+                    default: dense_lane_general(v, m, tgt - kLaneTarget, lane); break;
+                }
+            }
+            continue;
+        }
+        const uint32_t c_lane = (code >> 16) & 31u, c_warp = (code >> 21) & 15u, c_reg = (code >> 26) & 15u;
+        const uint32_t c_out = hd.y;
+        if (kind == kDiag) {  // exactly one of the masks holds the gate's bit
+            const bool thread_bit = (lane & c_lane) | (w & c_warp) | (base & c_out);
+            const double2 u0 = __ldg(u), u3 = __ldg(u + 3);
+#pragma unroll
+            for (int r = 0; r < 16; ++r) v[r] = xmul(sel(thread_bit || (uint32_t(r) & c_reg), u3, u0), v[r]);
+            continue;
+        }
+        const bool thread_ok = (lane & c_lane) == c_lane && (w & c_warp) == c_warp && (base & c_out) == c_out;
+        if (kind == kPerm) {
+            switch (tgt) {
                 case 0: perm_reg<0>(v, thread_ok, c_reg); break;
                 case 1: perm_reg<1>(v, thread_ok, c_reg); break;
                 case 2: perm_reg<2>(v, thread_ok, c_reg); break;
                 case 3: perm_reg<3>(v, thread_ok, c_reg); break;
                 default: {
-                    const int m = 1 << (op.tgt - kLaneTarget);
+                    const int m = 1 << (tgt - kLaneTarget);
 #pragma unroll
                     for (int r = 0; r < 16; ++r) {
                         const double2 p = shfl_xor2(v[r], m);
@@ -337,15 +372,10 @@ __global__ void __launch_bounds__(32 << WB, (WB == 3 ? 2 : 1))
                     }
                 }
             }
-        } else if (kind == kNeg) {
+        } else {  // kNeg
 #pragma unroll
             for (int r = 0; r < 16; ++r)
                 v[r] = sel(thread_ok && (uint32_t(r) & c_reg) == c_reg, make_double2(-v[r].x, -v[r].y), v[r]);
-        } else {  // kDiag: exactly one of c_lane, c_warp, c_reg, c_out holds the gate's bit
-            const bool thread_bit = (lane & c_lane) | (w & c_warp) | (base & c_out);
-            const double2 u0 = op.u[0], u3 = op.u[3];
-#pragma unroll
-            for (int r = 0; r < 16; ++r) v[r] = xmul(sel(thread_bit || (uint32_t(r) & c_reg), u3, u0), v[r]);
         }
     }
     double2* dst = state + base + lane;
@@ -560,7 +590,7 @@ struct Plan {
                 uint32_t nm = 0;
                 for (int k = 0; k < 4; ++k) nm |= 1u << next[size_t(k)].second;
                 RegOp x{};
-                x.kind = kXchg;
+                x.code = uint32_t(kXchg);
                 x.x_reg = nm;
                 x.x_warp = hi_all & ~nm;
                 reg_ops.push_back(x);
@@ -570,23 +600,29 @@ struct Plan {
             }
             const uint32_t warpm = hi_all & ~regm;
             RegOp op{};
-            op.kind = g[i].kind;
-            op.form = g[i].form;
-            for (int k = 0; k < 4; ++k) op.u[k] = g[i].u[k];
+            uint32_t tgt = 0, c_lane = 0, c_warp = 0, c_reg = 0;
+            if (g[i].kind == kDense && g[i].form == kReal) {
+                op.u[0] = make_double2(g[i].u[0].x, g[i].u[1].x);
+                op.u[1] = make_double2(g[i].u[2].x, g[i].u[3].x);
+            } else {
+                for (int k = 0; k < 4; ++k) op.u[k] = g[i].u[k];
+            }
             if (g[i].tgt >= 0)
-                op.tgt = g[i].tgt < 5 ? kLaneTarget + g[i].tgt : rank(regm, hb_of(g[i].tgt));
+                tgt = g[i].tgt < 5 ? uint32_t(kLaneTarget + g[i].tgt) : uint32_t(rank(regm, hb_of(g[i].tgt)));
             for (uint32_t m = g[i].bits; m; m &= m - 1) {
                 const int p = __builtin_ctz(m);
                 if (p < 5) {
-                    op.c_lane |= 1u << p;
+                    c_lane |= 1u << p;
                 } else if (mask & (1u << p)) {
                     const int b = hb_of(p);
-                    if (regm & (1u << b)) op.c_reg |= 1u << rank(regm, b);
-                    else op.c_warp |= 1u << rank(warpm, b);
+                    if (regm & (1u << b)) c_reg |= 1u << rank(regm, b);
+                    else c_warp |= 1u << rank(warpm, b);
                 } else {
                     op.c_out |= 1u << p;
                 }
             }
+            op.code = uint32_t(g[i].kind) | uint32_t(g[i].form) << 4 | tgt << 8 | c_lane << 16 | c_warp << 21 |
+                      c_reg << 26;
             reg_ops.push_back(op);
         }
         it.rhdr.nops = int(reg_ops.size() - it.gate_off);

@@ -7,12 +7,16 @@
 // device work while it walks.  Leaves (|0> and <0| vectors, gate tensors,
 // gate halves) are built on the host -- at most 64 amplitudes each -- and
 // uploaded together into a region of the arena that is never reused; every
-// other tensor gets a place in the arena's reusable region.  A node reorders
-// each operand that is not already in [shared legs, free legs] order
-// (network_permute_kernel, a gather through four 7-bit index tables) and
-// multiplies the two with a complex GEMM (cuBLAS ZGEMM): the result's legs
-// are the right operand's free legs (low bits), then the left's
-// (network.rs:591-664).  Nothing reaches the device until the whole walk has
+// other tensor gets a place in the arena's reusable region.  A large node
+// reorders each operand that is not already in [shared legs, free legs]
+// order (network_permute_kernel, a gather through four 7-bit index tables)
+// and multiplies the two with a complex GEMM (cuBLAS ZGEMM): the result's
+// legs are the right operand's free legs (low bits), then the left's
+// (network.rs:591-664).  Small nodes -- most of a circuit's tree -- read
+// their operands in place through index tables, one block each, and every
+// run of them between two large nodes is launched level by level (a node's
+// level: one more than its deepest input made in the same run), so a tree of
+// hundreds of small joins costs a few launches.  Nothing reaches the device until the whole walk has
 // passed, so every failure the reference reports comes back before any
 // launch.
 #include <cublas_v2.h>
@@ -34,7 +38,6 @@ using namespace wqc::tree;
 namespace {
 
 constexpr int kPermuteThreads = 256;
-constexpr int kTimedLegs = 16;  // permutes and GEMMs with results of >= 2^16 amplitudes are timed one by one
 
 // ---------------------------------------------------------------------------
 // Device side.
@@ -66,6 +69,42 @@ __global__ void __launch_bounds__(kPermuteThreads) network_permute_kernel(double
     const uint32_t total = 1u << legs;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
         dst[i] = src[tab[0][i & 127] | tab[1][(i >> 7) & 127] | tab[2][(i >> 14) & 127] | tab[3][(i >> 21) & 127]];
+}
+
+// One small contraction per block: C[i][j] = sum_x L[lf[i] + ls[x]] R[rf[j] + rs[x]]
+// with the operands read in place through offset tables (no reordered
+// copies), x ascending.  The result is row-major m x n: index j | i << log2 n,
+// the right operand's free legs low (network.rs:591-664).
+struct SmallJob {
+    uint64_t l, r, c;      // element offsets in the arena
+    uint32_t m, n, k;
+    uint32_t lf, ls, rf, rs;  // offsets of the four index tables in the table array
+};
+
+constexpr int kSmallThreads = 128;
+
+__global__ void __launch_bounds__(kSmallThreads) network_small_kernel(double2* __restrict__ arena,
+                                                                      const SmallJob* __restrict__ jobs,
+                                                                      const uint32_t* __restrict__ tab) {
+    const SmallJob J = jobs[blockIdx.x];
+    const double2* L = arena + J.l;
+    const double2* R = arena + J.r;
+    double2* out = arena + J.c;
+    const uint32_t* lf = tab + J.lf;
+    const uint32_t* ls = tab + J.ls;
+    const uint32_t* rf = tab + J.rf;
+    const uint32_t* rs = tab + J.rs;
+    for (uint32_t o = threadIdx.x; o < J.m * J.n; o += blockDim.x) {
+        const uint32_t i = o / J.n, j = o - i * J.n;
+        const uint32_t li = lf[i], rj = rf[j];
+        double re = 0.0, im = 0.0;
+        for (uint32_t x = 0; x < J.k; ++x) {
+            const double2 a = L[li + ls[x]], b = R[rj + rs[x]];
+            re = fma(a.x, b.x, fma(-a.y, b.y, re));
+            im = fma(a.x, b.y, fma(a.y, b.x, im));
+        }
+        out[o] = make_double2(re, im);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -196,13 +235,20 @@ struct Buffer {
 };
 
 struct Op {
-    int kind;  // 0 permute, 1 gemm
+    int kind;  // 0 permute, 1 gemm, 2 small contraction (batched by level)
     int src, dst;          // permute
     PermuteMap map;
     int legs;
-    int a, b, c;           // gemm: C (m x n) = A (m x k) B (n x k)^T, row-major
+    int a, b, c;           // gemm / small: C (m x n) = A (m x k) B (n x k)^T, row-major
     uint64_t m, k, n;
+    int level;             // small: 1 + the deepest small input of its segment
+    uint32_t lf, ls, rf, rs;  // small: index tables
 };
+
+// A contraction this small (result, work and operands) runs in one block of
+// a batched launch; the rest reorder and go through cuBLAS.
+constexpr uint64_t kSmallResult = 1ull << 14, kSmallWork = 1ull << 16;
+constexpr size_t kSmallLegs = 14;
 
 struct NetPlan {
     bool on = false;
@@ -212,6 +258,18 @@ struct NetPlan {
     Placer placer;
     uint64_t permute_bytes = 0;
     double gemm_flops = 0;
+    std::vector<uint32_t> tables;       // small contractions' index tables
+    std::map<int, int> seg_level;       // buffers made in the open segment of small contractions -> level
+    std::vector<int> seg_frees;         // buffers the open segment consumed, released when it closes
+
+    // Small contractions between two large ones form a segment; its
+    // launches run level by level, so a range it frees is reused only after
+    // the segment.
+    void close_segment() {
+        for (int id : seg_frees) drop(id);
+        seg_frees.clear();
+        seg_level.clear();
+    }
 
     int new_leaf(const std::vector<double2>& data, int legs) {
         Buffer b;
@@ -347,6 +405,49 @@ struct NetWalker {
         *working = work;
         result->legs = legs;
         if (!plan->on) return WQC_OK;
+        const uint64_t m = 1ull << left_free.size(), k = 1ull << shared.size(), n_ = 1ull << right_free.size();
+        if (m * n_ <= kSmallResult && m * n_ * k <= kSmallWork && left.legs.size() <= kSmallLegs &&
+            right.legs.size() <= kSmallLegs) {
+            // One block of a batched launch reads both operands in place.
+            auto table = [&](const std::vector<uint32_t>& of, const std::vector<uint32_t>& legs_) {
+                const uint32_t at = uint32_t(plan->tables.size());
+                for (uint64_t x = 0; x < (1ull << legs_.size()); ++x) {
+                    uint32_t off = 0;
+                    for (size_t b = 0; b < legs_.size(); ++b)
+                        if ((x >> b) & 1)
+                            off |= 1u << (std::find(of.begin(), of.end(), legs_[b]) - of.begin());
+                    plan->tables.push_back(off);
+                }
+                return at;
+            };
+            Op op{};
+            op.kind = 2;
+            op.a = left.buf;
+            op.b = right.buf;
+            result->buf = plan->new_tensor(int(legs.size()));
+            op.c = result->buf;
+            op.m = m;
+            op.k = k;
+            op.n = n_;
+            op.legs = int(legs.size());
+            op.lf = table(left.legs, left_free);
+            op.ls = table(left.legs, shared);
+            op.rf = table(right.legs, right_free);
+            op.rs = table(right.legs, shared);
+            int lv = 0;
+            for (int in : {left.buf, right.buf}) {
+                auto it = plan->seg_level.find(in);
+                if (it != plan->seg_level.end()) lv = std::max(lv, it->second);
+            }
+            op.level = lv + 1;
+            plan->seg_level[result->buf] = op.level;
+            plan->ops.push_back(op);
+            plan->gemm_flops += 8.0 * double(m) * double(n_) * double(k);
+            plan->seg_frees.push_back(left.buf);
+            plan->seg_frees.push_back(right.buf);
+            return WQC_OK;
+        }
+        plan->close_segment();
         // Device work: reorder what is out of order, then C = A B^T.
         auto reorder = [&](const Tensor& t, const std::vector<uint32_t>& to) {
             const int L = int(t.legs.size());
@@ -438,6 +539,8 @@ struct wqc_network {
     cublasHandle_t blas = nullptr;
     double2* arena = nullptr;
     uint64_t arena_bytes = 0;
+    unsigned char* table = nullptr;  // small contractions' index tables and jobs
+    uint64_t table_bytes = 0;
     double2* host_root = nullptr;  // pinned
     unsigned char* staging = nullptr;  // pinned leaf upload
     uint64_t staging_bytes = 0;
@@ -493,6 +596,7 @@ void wqc_network_destroy(wqc_network* net) {
     if (net->blas) cublasDestroy(net->blas);
     for (cudaEvent_t e : net->events) cudaEventDestroy(e);
     if (net->arena) cudaFree(net->arena);
+    if (net->table) cudaFree(net->table);
     if (net->host_root) cudaFreeHost(net->host_root);
     if (net->staging) cudaFreeHost(net->staging);
     if (net->stream) cudaStreamDestroy(net->stream);
@@ -557,6 +661,43 @@ wqc_status wqc_network_contract(wqc_network* net, uint32_t n, const wqc_gate* ga
 
     const uint64_t leaf_bytes = (plan.leaf_data.size() * 16 + kAlign - 1) / kAlign * kAlign;
     const uint64_t need = std::max<uint64_t>(leaf_bytes + plan.placer.top, kAlign);
+    auto offset_of = [&](int id) {
+        const Buffer& B = plan.bufs[size_t(id)];
+        return (B.leaf ? 0 : leaf_bytes / 16) + B.off;
+    };
+    // The small contractions' launches: each run of them between two large
+    // contractions, level by level (`batches`: first job, job count, and the
+    // op index the run ends before).
+    std::vector<SmallJob> jobs;
+    struct Batch {
+        uint32_t first, count;
+        size_t before;
+    };
+    std::vector<Batch> batches;
+    for (size_t i = 0; i < plan.ops.size();) {
+        if (plan.ops[i].kind != 2) {
+            ++i;
+            continue;
+        }
+        size_t j = i;
+        int top = 0;
+        while (j < plan.ops.size() && plan.ops[j].kind == 2) top = std::max(top, plan.ops[j++].level);
+        for (int lv = 1; lv <= top; ++lv) {
+            Batch b{uint32_t(jobs.size()), 0, j};
+            for (size_t q = i; q < j; ++q) {
+                const Op& op = plan.ops[q];
+                if (op.level != lv) continue;
+                jobs.push_back(SmallJob{offset_of(op.a), offset_of(op.b), offset_of(op.c), uint32_t(op.m),
+                                        uint32_t(op.n), uint32_t(op.k), op.lf, op.ls, op.rf, op.rs});
+                ++b.count;
+            }
+            if (b.count) batches.push_back(b);
+        }
+        i = j;
+    }
+    const uint64_t tab_bytes = (plan.tables.size() * 4 + kAlign - 1) / kAlign * kAlign;
+    const uint64_t jobs_bytes = (jobs.size() * sizeof(SmallJob) + kAlign - 1) / kAlign * kAlign;
+    const uint64_t stage_bytes = std::max<uint64_t>(leaf_bytes + tab_bytes + jobs_bytes, kAlign);
     if (cudaError_t e = cudaSetDevice(net->device)) return ncuda("cudaSetDevice", e);
     if (net->arena_bytes < need) {
         if (net->arena) cudaFree(net->arena);
@@ -570,15 +711,27 @@ wqc_status wqc_network_contract(wqc_network* net, uint32_t n, const wqc_gate* ga
         }
         net->arena_bytes = need;
     }
-    if (net->staging_bytes < leaf_bytes) {
+    if (net->table_bytes < tab_bytes + jobs_bytes) {
+        if (net->table) cudaFree(net->table);
+        net->table = nullptr;
+        net->table_bytes = 0;
+        if (cudaMalloc(reinterpret_cast<void**>(&net->table), tab_bytes + jobs_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            size_t fr = 0, tot = 0;
+            cudaMemGetInfo(&fr, &tot);
+            return record_oom(tab_bytes + jobs_bytes, fr);
+        }
+        net->table_bytes = tab_bytes + jobs_bytes;
+    }
+    if (net->staging_bytes < stage_bytes) {
         if (net->staging) cudaFreeHost(net->staging);
         net->staging = nullptr;
         net->staging_bytes = 0;
-        if (cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&net->staging), leaf_bytes)) {
+        if (cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&net->staging), stage_bytes)) {
             cudaGetLastError();
             return ncuda("cudaMallocHost(network leaves)", e);
         }
-        net->staging_bytes = leaf_bytes;
+        net->staging_bytes = stage_bytes;
     }
     cudaStream_t st = net->stream;
     double2* leaves = net->arena;
@@ -600,12 +753,36 @@ wqc_status wqc_network_contract(wqc_network* net, uint32_t n, const wqc_gate* ga
         if (cudaError_t e = cudaMemcpyAsync(leaves, net->staging, plan.leaf_data.size() * 16, cudaMemcpyHostToDevice, st))
             return bail(ncuda("cudaMemcpyAsync(network leaves)", e));
     }
+    const uint32_t* d_tab = reinterpret_cast<const uint32_t*>(net->table);
+    const SmallJob* d_jobs = reinterpret_cast<const SmallJob*>(net->table + tab_bytes);
+    if (!jobs.empty()) {
+        unsigned char* h = net->staging + leaf_bytes;
+        std::memcpy(h, plan.tables.data(), plan.tables.size() * 4);
+        std::memcpy(h + tab_bytes, jobs.data(), jobs.size() * sizeof(SmallJob));
+        if (cudaError_t e = cudaMemcpyAsync(net->table, h, tab_bytes + jobs.size() * sizeof(SmallJob),
+                                            cudaMemcpyHostToDevice, st))
+            return bail(ncuda("cudaMemcpyAsync(network jobs)", e));
+    }
+    size_t next_batch = 0;
+    uint32_t small_launches = 0;
+    auto run_batches = [&](size_t before) -> wqc_status {
+        while (next_batch < batches.size() && batches[next_batch].before <= before) {
+            const Batch& b = batches[next_batch++];
+            network_small_kernel<<<b.count, kSmallThreads, 0, st>>>(net->arena, d_jobs + b.first, d_tab);
+            if (cudaError_t e = cudaGetLastError()) return ncuda("network small-contraction launch", e);
+            ++small_launches;
+        }
+        return WQC_OK;
+    };
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> timed;
     uint32_t permutes = 0, gemms = 0;
     const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
-    for (const Op& op : plan.ops) {
+    for (size_t oi = 0; oi < plan.ops.size(); ++oi) {
+        const Op& op = plan.ops[oi];
+        if (op.kind == 2) continue;  // launched in batches
+        if (wqc_status s = run_batches(oi)) return bail(s);
         if (net->cancel.exchange(0)) return bail(record_error(WQC_ERR_CANCELLED, "computation cancelled: the client has gone"));
-        const bool time_it = op.legs >= kTimedLegs;
+        const bool time_it = true;  // the large contractions are few: each is timed
         cudaEvent_t a = nullptr, b = nullptr;
         if (time_it) {
             a = net_event(net, ev++);
@@ -636,6 +813,7 @@ wqc_status wqc_network_contract(wqc_network* net, uint32_t n, const wqc_gate* ga
             timed.push_back({op.kind, {a, b}});
         }
     }
+    if (wqc_status s = run_batches(plan.ops.size())) return bail(s);
     if (cudaError_t e = cudaMemcpyAsync(net->host_root, at(root), sizeof(double2), cudaMemcpyDeviceToHost, st))
         return bail(ncuda("cudaMemcpyAsync(network root)", e));
     cudaEventRecord(e1, st);
@@ -653,7 +831,8 @@ wqc_status wqc_network_contract(wqc_network* net, uint32_t n, const wqc_gate* ga
     net->stats.nodes = tree->node_count;
     net->stats.permutes = permutes;
     net->stats.gemms = gemms;
-    net->stats.launches = permutes + gemms;
+    net->stats.launches = permutes + gemms + small_launches;
+    net->stats.small = uint32_t(jobs.size());
     net->stats.permute_bytes = plan.permute_bytes;
     net->stats.gemm_flops = plan.gemm_flops;
     net->stats.arena_bytes = net->arena_bytes;

@@ -28,6 +28,7 @@ class NetworkStats(ctypes.Structure):
         ("permute_bytes", ctypes.c_uint64),
         ("gemm_flops", ctypes.c_double),
         ("arena_bytes", ctypes.c_uint64),
+        ("small", ctypes.c_uint32),
     ]
 
 
