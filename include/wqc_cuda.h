@@ -463,9 +463,9 @@ WQC_API wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t qubit_count, const
                                       const wqc_tree* tree, const uint64_t* mps_site_order,
                                       uint32_t mps_site_order_len, const uint64_t* bits, uint32_t count, double* out);
 
-/* Size of the register tiles that states of 12 or more legs are swept in:
- * 2^bits amplitudes per block, bits 12 (256 threads) or 13 (512 threads,
- * the default).  A tuning knob: results do not depend on it. */
+/* Size of the register tiles that states of at least `bits` legs are swept
+ * in: 2^bits amplitudes per block, bits 12 (256 threads, the default) or 13
+ * (512 threads).  A tuning knob: results do not depend on it. */
 WQC_API wqc_status wqc_exact_set_tile_bits(wqc_exact* ex, int32_t bits);
 
 /* Stop a contraction in progress (the reference's cancel::check per gate,

@@ -915,7 +915,7 @@ struct wqc_exact {
     int device = 0;
     int sm_count = 148;
     int pass_bits = kMaxPassBits;
-    int tile_bits = 13;  // register tiles of 2^13 amplitudes (512 threads x 16)
+    int tile_bits = 12;  // register tiles of 2^12 amplitudes (256 threads x 16)
     cudaStream_t stream = nullptr;
     double2* arena = nullptr;
     uint64_t arena_bytes = 0;

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kPermuteThreads) network_permute_kernel(double
 
 // One small contraction per block: C[i][j] = sum_x L[lf[i] + ls[x]] R[rf[j] + rs[x]]
 // with the operands read in place through offset tables (no reordered
-// copies), x ascending.  The result is row-major m x n: index j | i << log2 n,
+// copies).  The result is row-major m x n: index j | i << log2 n,
 // the right operand's free legs low (network.rs:591-664).
 struct SmallJob {
     uint64_t l, r, c;      // element offsets in the arena
@@ -83,9 +83,13 @@ struct SmallJob {
 
 constexpr int kSmallThreads = 128;
 
+// When a join has fewer outputs than threads (down to a single scalar), the
+// threads of one output split its sum over x and add their parts through
+// shared memory; the parts are added in thread order.
 __global__ void __launch_bounds__(kSmallThreads) network_small_kernel(double2* __restrict__ arena,
                                                                       const SmallJob* __restrict__ jobs,
                                                                       const uint32_t* __restrict__ tab) {
+    __shared__ double2 part[kSmallThreads];
     const SmallJob J = jobs[blockIdx.x];
     const double2* L = arena + J.l;
     const double2* R = arena + J.r;
@@ -94,16 +98,36 @@ __global__ void __launch_bounds__(kSmallThreads) network_small_kernel(double2* _
     const uint32_t* ls = tab + J.ls;
     const uint32_t* rf = tab + J.rf;
     const uint32_t* rs = tab + J.rs;
-    for (uint32_t o = threadIdx.x; o < J.m * J.n; o += blockDim.x) {
-        const uint32_t i = o / J.n, j = o - i * J.n;
-        const uint32_t li = lf[i], rj = rf[j];
+    const uint32_t outs = J.m * J.n;  // a power of two
+    const uint32_t tpo = outs >= kSmallThreads ? 1u : kSmallThreads / outs;  // threads per output
+    const uint32_t slot = threadIdx.x / tpo, piece = threadIdx.x % tpo;
+    for (uint32_t first = 0; first < outs; first += kSmallThreads / tpo) {
+        const uint32_t o = first + slot;
         double re = 0.0, im = 0.0;
-        for (uint32_t x = 0; x < J.k; ++x) {
-            const double2 a = L[li + ls[x]], b = R[rj + rs[x]];
-            re = fma(a.x, b.x, fma(-a.y, b.y, re));
-            im = fma(a.x, b.y, fma(a.y, b.x, im));
+        if (o < outs) {
+            const uint32_t i = o / J.n, j = o - i * J.n;
+            const uint32_t li = lf[i], rj = rf[j];
+            for (uint32_t x = piece; x < J.k; x += tpo) {
+                const double2 a = L[li + ls[x]], b = R[rj + rs[x]];
+                re = fma(a.x, b.x, fma(-a.y, b.y, re));
+                im = fma(a.x, b.y, fma(a.y, b.x, im));
+            }
         }
-        out[o] = make_double2(re, im);
+        if (tpo == 1) {
+            if (o < outs) out[o] = make_double2(re, im);
+            continue;
+        }
+        part[threadIdx.x] = make_double2(re, im);
+        __syncthreads();
+        if (piece == 0 && o < outs) {
+            double2 acc = part[threadIdx.x];
+            for (uint32_t q = 1; q < tpo; ++q) {
+                acc.x += part[threadIdx.x + q].x;
+                acc.y += part[threadIdx.x + q].y;
+            }
+            out[o] = acc;
+        }
+        __syncthreads();
     }
 }
 
