@@ -85,16 +85,16 @@ def tree_nodes(nodes) -> np.ndarray:
     """The nodes as the C ABI's wqc_tree_node records.  A node is a dict of
     the reference's JSON form (op "contract" is 0; any other op is a sweep
     step and is passed on as such) or a (left, right) pair of references."""
-    out = np.zeros(len(nodes), dtype=TREE_NODE_DTYPE)
-    for i, node in enumerate(nodes):
+    rows = []
+    for node in nodes:
+        op = 0
         if isinstance(node, dict):
-            op = node.get("op", "contract")
-            out[i]["op"] = 0 if op == "contract" else 1
+            op = 0 if node.get("op", "contract") == "contract" else 1
             left, right = node.get("left", node.get("tensor", {"ket0": 0})), node.get("right", {"ket0": 0})
         else:
             left, right = node
-        (out[i]["lkind"], out[i]["lindex"]), (out[i]["rkind"], out[i]["rindex"]) = _ref(left), _ref(right)
-    return out
+        rows.append((op, *_ref(left), *_ref(right)))
+    return np.array(rows, dtype=TREE_NODE_DTYPE) if rows else np.zeros(0, dtype=TREE_NODE_DTYPE)
 
 
 class _TreeArgs:
