@@ -153,6 +153,18 @@ def inverse(gates):
     return inv
 
 
+def test_brickwork_25_equals_the_oracle_at_full_width(ex):
+    """The widest state the 1 GiB peak admits, against the oracle's own walk
+    (its C loops take ~10 s on the 2^25-amplitude state): equal amplitudes."""
+    n = 25
+    gates = C.ry_cnot_brickwork(n, 3)
+    tree = P.plan_greedy(n, gates)
+    bits = 0b1011001110001111000011111
+    got = ex.contract(n, gates, tree, bits)
+    assert ex.stats()["pass_bytes"] > 0  # passes over the full 25-leg state ran
+    assert got == oracle_amp(n, gates, tree, bits)
+
+
 def test_brickwork_25_then_inverse_returns_zero(ex):
     n = 25
     fwd = C.ry_cnot_brickwork(n, 12)
