@@ -157,12 +157,12 @@ __global__ void __launch_bounds__(kPassThreads) exact_pass_kernel(double2* __res
 }
 
 // ---------------------------------------------------------------------------
-// Register-tiled passes over tensors of at least 5 + WB + 4 legs.
+// Register-tiled passes over tensors of at least 5 + WB + RB legs.
 //
-// A block holds a tile of 2^(9 + WB) amplitudes: its local bits 0-4 are the
-// tensor's positions 0-4 (the lanes of a warp, so every warp-wide load or
-// store is 512 contiguous bytes), the other 4 + WB local bits are the tile's
-// high positions, of which 4 are register bits (each thread holds 16
+// A block holds a tile of 2^(5 + WB + RB) amplitudes: its local bits 0-4 are
+// the tensor's positions 0-4 (the lanes of a warp, so every warp-wide load or
+// store is 512 contiguous bytes), the other WB + RB local bits are the tile's
+// high positions, of which RB are register bits (each thread holds 2^RB
 // amplitudes) and WB are warp bits.  A gate whose target is a register bit
 // runs inside the thread; a target on a lane bit takes its partner by a warp
 // shuffle; a target on a warp bit first needs an exchange, which rewrites the
@@ -213,17 +213,21 @@ __device__ __forceinline__ double2 shfl_xor2(double2 v, int m) {
 // The four register bits' places among the high local bits, and the high
 // local index of register r: the OR of the places of r's set bits, folded at
 // compile time for each unrolled r.
+template <int RB>
 struct RegBits {
-    uint32_t b[4];
+    uint32_t b[RB];
     __device__ __forceinline__ void set(uint32_t regm) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < RB; ++i) {
             b[i] = regm & (0u - regm);
             regm &= regm - 1;
         }
     }
     __device__ __forceinline__ uint32_t at(int r) const {
-        return ((r & 1) ? b[0] : 0u) | ((r & 2) ? b[1] : 0u) | ((r & 4) ? b[2] : 0u) | ((r & 8) ? b[3] : 0u);
+        uint32_t x = 0;
+#pragma unroll
+        for (int i = 0; i < RB; ++i) x |= ((r >> i) & 1) ? b[i] : 0u;
+        return x;
     }
 };
 
@@ -233,26 +237,30 @@ __device__ __forceinline__ double2 sel(bool c, double2 a, double2 b) {
 
 // One-qubit gates with two nonzero entries per row (H, Y, RX, RY; no
 // controls).  On a register bit: pairs (r, r | 1 << TR) inside the thread.
-template <int TR>
-__device__ __forceinline__ void dense_reg_real(double2 (&v)[16], double a, double b, double c, double d) {
+template <int NR, int TR>
+__device__ __forceinline__ void dense_reg_real(double2 (&v)[NR], double a, double b, double c, double d) {
+    if constexpr ((1 << TR) < NR) {
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
+    for (int r = 0; r < NR; ++r) {
         if (r & (1 << TR)) continue;
         const int r1 = r | (1 << TR);
         const double2 v0 = v[r], v1 = v[r1];
         v[r] = row_real(a, b, v0, v1);
         v[r1] = row_real(c, d, v0, v1);
     }
+    }
 }
-template <int TR>
-__device__ __forceinline__ void dense_reg_general(double2 (&v)[16], const double2 (&u)[4]) {
+template <int NR, int TR>
+__device__ __forceinline__ void dense_reg_general(double2 (&v)[NR], const double2 (&u)[4]) {
+    if constexpr ((1 << TR) < NR) {
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
+    for (int r = 0; r < NR; ++r) {
         if (r & (1 << TR)) continue;
         const int r1 = r | (1 << TR);
         const double2 v0 = v[r], v1 = v[r1];
         v[r] = row_general(u[0], u[1], v0, v1);
         v[r1] = row_general(u[2], u[3], v0, v1);
+    }
     }
 }
 
@@ -260,26 +268,29 @@ __device__ __forceinline__ void dense_reg_general(double2 (&v)[16], const double
 // the bit clear computes u00 v + u01 p, the lane with it set u11 v + u10 p
 // -- the reference's u10 v0 + u11 v1 with the two terms of the sum swapped,
 // which IEEE addition leaves bit-identical.
-__device__ __forceinline__ void dense_lane_real(double2 (&v)[16], double a, double b, double c, double d, int tl,
+template <int NR>
+__device__ __forceinline__ void dense_lane_real(double2 (&v)[NR], double a, double b, double c, double d, int tl,
                                                 uint32_t lane) {
     const bool hi = (lane >> tl) & 1u;
     const double own = hi ? d : a, other = hi ? c : b;
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = row_real(own, other, v[r], shfl_xor2(v[r], 1 << tl));
+    for (int r = 0; r < NR; ++r) v[r] = row_real(own, other, v[r], shfl_xor2(v[r], 1 << tl));
 }
-__device__ __forceinline__ void dense_lane_general(double2 (&v)[16], const double2 (&u)[4], int tl, uint32_t lane) {
+template <int NR>
+__device__ __forceinline__ void dense_lane_general(double2 (&v)[NR], const double2 (&u)[4], int tl, uint32_t lane) {
     const bool hi = (lane >> tl) & 1u;
     const double2 own = hi ? u[3] : u[0], other = hi ? u[2] : u[1];
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = row_general(own, other, v[r], shfl_xor2(v[r], 1 << tl));
+    for (int r = 0; r < NR; ++r) v[r] = row_general(own, other, v[r], shfl_xor2(v[r], 1 << tl));
 }
 
 // Swaps of the target pairs where the controls are set: thread-level
 // controls select whole pairs; register-bit controls select pair by pair.
-template <int TR>
-__device__ __forceinline__ void perm_reg(double2 (&v)[16], bool thread_ok, uint32_t c_reg) {
+template <int NR, int TR>
+__device__ __forceinline__ void perm_reg(double2 (&v)[NR], bool thread_ok, uint32_t c_reg) {
+    if constexpr ((1 << TR) < NR) {
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
+    for (int r = 0; r < NR; ++r) {
         if (r & (1 << TR)) continue;
         const int r1 = r | (1 << TR);
         const bool ok = thread_ok && (uint32_t(r) & c_reg) == c_reg;
@@ -287,12 +298,14 @@ __device__ __forceinline__ void perm_reg(double2 (&v)[16], bool thread_ok, uint3
         v[r] = sel(ok, v1, v0);
         v[r1] = sel(ok, v0, v1);
     }
+    }
 }
 
-template <int WB>
+template <int WB, int RB>
 __global__ void __launch_bounds__(32 << WB, (WB == 3 ? 2 : 1))
     exact_pass_reg_kernel(double2* __restrict__ state, RegPassHdr h, const RegOp* __restrict__ ops) {
-    constexpr int HB = WB + 4;  // high local bits
+    constexpr int HB = WB + RB;  // high local bits
+    constexpr int NR = 1 << RB;  // amplitudes per thread
     extern __shared__ double2 xbuf[];  // 2^(9 + WB) amplitudes, used by exchanges
     __shared__ uint32_t hi_off[1 << HB];
     const uint32_t all = h.legs >= 32 ? ~0u : ((1u << h.legs) - 1u);
@@ -301,13 +314,13 @@ __global__ void __launch_bounds__(32 << WB, (WB == 3 ? 2 : 1))
     __syncthreads();
     const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
     constexpr uint32_t kHiAll = (1u << HB) - 1u;  // keeps every tile index below 2^(9 + WB)
-    RegBits rb;
+    RegBits<RB> rb;
     rb.set(h.reg0 & kHiAll);
     uint32_t wdep = deposit(w, h.warp0 & kHiAll);
-    double2 v[16];
+    double2 v[NR];
     const double2* src = state + base + lane;
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = src[hi_off[wdep | rb.at(r)]];
+    for (int r = 0; r < NR; ++r) v[r] = src[hi_off[wdep | rb.at(r)]];
     for (int o = 0; o < h.nops; ++o) {
         const uint4 hd = __ldg(reinterpret_cast<const uint4*>(ops + o));
         const uint32_t code = hd.x;
@@ -316,12 +329,12 @@ __global__ void __launch_bounds__(32 << WB, (WB == 3 ? 2 : 1))
         if (kind == kXchg) {
             __syncthreads();  // the previous exchange's reads are done
 #pragma unroll
-            for (int r = 0; r < 16; ++r) xbuf[lane | ((wdep | rb.at(r)) << 5)] = v[r];
+            for (int r = 0; r < NR; ++r) xbuf[lane | ((wdep | rb.at(r)) << 5)] = v[r];
             __syncthreads();
             rb.set(hd.z & kHiAll);
             wdep = deposit(w, hd.w & kHiAll);
 #pragma unroll
-            for (int r = 0; r < 16; ++r) v[r] = xbuf[lane | ((wdep | rb.at(r)) << 5)];
+            for (int r = 0; r < NR; ++r) v[r] = xbuf[lane | ((wdep | rb.at(r)) << 5)];
             continue;
         }
         const double2* u = ops[o].u;
@@ -329,20 +342,20 @@ __global__ void __launch_bounds__(32 << WB, (WB == 3 ? 2 : 1))
             if (((code >> 4) & 15u) == kReal) {
                 const double2 ab = __ldg(u), cd = __ldg(u + 1);
                 switch (tgt) {
-                    case 0: dense_reg_real<0>(v, ab.x, ab.y, cd.x, cd.y); break;
-                    case 1: dense_reg_real<1>(v, ab.x, ab.y, cd.x, cd.y); break;
-                    case 2: dense_reg_real<2>(v, ab.x, ab.y, cd.x, cd.y); break;
-                    case 3: dense_reg_real<3>(v, ab.x, ab.y, cd.x, cd.y); break;
-                    default: dense_lane_real(v, ab.x, ab.y, cd.x, cd.y, tgt - kLaneTarget, lane); break;
+                    case 0: dense_reg_real<NR, 0>(v, ab.x, ab.y, cd.x, cd.y); break;
+                    case 1: dense_reg_real<NR, 1>(v, ab.x, ab.y, cd.x, cd.y); break;
+                    case 2: dense_reg_real<NR, 2>(v, ab.x, ab.y, cd.x, cd.y); break;
+                    case 3: dense_reg_real<NR, 3>(v, ab.x, ab.y, cd.x, cd.y); break;
+                    default: dense_lane_real<NR>(v, ab.x, ab.y, cd.x, cd.y, tgt - kLaneTarget, lane); break;
                 }
             } else {
                 const double2 m[4] = {__ldg(u), __ldg(u + 1), __ldg(u + 2), __ldg(u + 3)};
                 switch (tgt) {
-                    case 0: dense_reg_general<0>(v, m); break;
-                    case 1: dense_reg_general<1>(v, m); break;
-                    case 2: dense_reg_general<2>(v, m); break;
-                    case 3: dense_reg_general<3>(v, m); break;
-                    default: dense_lane_general(v, m, tgt - kLaneTarget, lane); break;
+                    case 0: dense_reg_general<NR, 0>(v, m); break;
+                    case 1: dense_reg_general<NR, 1>(v, m); break;
+                    case 2: dense_reg_general<NR, 2>(v, m); break;
+                    case 3: dense_reg_general<NR, 3>(v, m); break;
+                    default: dense_lane_general<NR>(v, m, tgt - kLaneTarget, lane); break;
                 }
             }
             continue;
@@ -353,20 +366,20 @@ __global__ void __launch_bounds__(32 << WB, (WB == 3 ? 2 : 1))
             const bool thread_bit = (lane & c_lane) | (w & c_warp) | (base & c_out);
             const double2 u0 = __ldg(u), u3 = __ldg(u + 3);
 #pragma unroll
-            for (int r = 0; r < 16; ++r) v[r] = xmul(sel(thread_bit || (uint32_t(r) & c_reg), u3, u0), v[r]);
+            for (int r = 0; r < NR; ++r) v[r] = xmul(sel(thread_bit || (uint32_t(r) & c_reg), u3, u0), v[r]);
             continue;
         }
         const bool thread_ok = (lane & c_lane) == c_lane && (w & c_warp) == c_warp && (base & c_out) == c_out;
         if (kind == kPerm) {
             switch (tgt) {
-                case 0: perm_reg<0>(v, thread_ok, c_reg); break;
-                case 1: perm_reg<1>(v, thread_ok, c_reg); break;
-                case 2: perm_reg<2>(v, thread_ok, c_reg); break;
-                case 3: perm_reg<3>(v, thread_ok, c_reg); break;
+                case 0: perm_reg<NR, 0>(v, thread_ok, c_reg); break;
+                case 1: perm_reg<NR, 1>(v, thread_ok, c_reg); break;
+                case 2: perm_reg<NR, 2>(v, thread_ok, c_reg); break;
+                case 3: perm_reg<NR, 3>(v, thread_ok, c_reg); break;
                 default: {
                     const int m = 1 << (tgt - kLaneTarget);
 #pragma unroll
-                    for (int r = 0; r < 16; ++r) {
+                    for (int r = 0; r < NR; ++r) {
                         const double2 p = shfl_xor2(v[r], m);
                         v[r] = sel(thread_ok && (uint32_t(r) & c_reg) == c_reg, p, v[r]);
                     }
@@ -374,13 +387,13 @@ __global__ void __launch_bounds__(32 << WB, (WB == 3 ? 2 : 1))
             }
         } else {  // kNeg
 #pragma unroll
-            for (int r = 0; r < 16; ++r)
+            for (int r = 0; r < NR; ++r)
                 v[r] = sel(thread_ok && (uint32_t(r) & c_reg) == c_reg, make_double2(-v[r].x, -v[r].y), v[r]);
         }
     }
     double2* dst = state + base + lane;
 #pragma unroll
-    for (int r = 0; r < 16; ++r) dst[hi_off[wdep | rb.at(r)]] = v[r];
+    for (int r = 0; r < NR; ++r) dst[hi_off[wdep | rb.at(r)]] = v[r];
 }
 
 // out[i] = left[extract(i, lmask)] * right[extract(i, rmask)] over the sorted
@@ -475,7 +488,8 @@ struct Sched {
 struct Plan {
     bool on = false;
     int pass_bits = kMaxPassBits;
-    int tile_wb = 4;  // warp bits of a register tile: tiles of 2^(9 + tile_wb) amplitudes
+    int tile_wb = 3;  // warp bits of a register tile
+    int tile_rb = 4;  // register bits: tiles of 2^(5 + tile_wb + tile_rb) amplitudes
     const wqc_gate* gates = nullptr;
     std::vector<Buffer> bufs;
     std::vector<Item> items;
@@ -543,7 +557,7 @@ struct Plan {
     // One register-tiled pass: the gates `g` (execution order) on a state of
     // `legs` legs whose targets outside positions 0-4 are `targets`.
     void emit_reg_pass(int id, int legs, const std::vector<Sched>& g, uint32_t targets) {
-        const int HB = tile_wb + 4;
+        const int HB = tile_wb + tile_rb;
         std::vector<int> hi;  // tensor positions of the high local bits, ascending
         for (int p = 5; p < legs; ++p)
             if (targets & (1u << p)) hi.push_back(p);
@@ -560,9 +574,9 @@ struct Plan {
         for (size_t i = 0; i < g.size(); ++i)
             if ((g[i].kind == kDense || g[i].kind == kPerm) && g[i].tgt >= 5) use[i] = hb_of(g[i].tgt);
         uint32_t regm = 0;
-        for (size_t i = 0; i < g.size() && __builtin_popcount(regm) < 4; ++i)
+        for (size_t i = 0; i < g.size() && __builtin_popcount(regm) < tile_rb; ++i)
             if (use[i] >= 0) regm |= 1u << use[i];
-        for (int b = 0; b < HB && __builtin_popcount(regm) < 4; ++b) regm |= 1u << b;
+        for (int b = 0; b < HB && __builtin_popcount(regm) < tile_rb; ++b) regm |= 1u << b;
         Item it{};
         it.kind = 2;
         it.buf = id;
@@ -588,7 +602,7 @@ struct Plan {
                 }
                 std::sort(next.begin(), next.end());
                 uint32_t nm = 0;
-                for (int k = 0; k < 4; ++k) nm |= 1u << next[size_t(k)].second;
+                for (int k = 0; k < tile_rb; ++k) nm |= 1u << next[size_t(k)].second;
                 RegOp x{};
                 x.code = uint32_t(kXchg);
                 x.x_reg = nm;
@@ -637,7 +651,7 @@ struct Plan {
     // a waiting gate, or that rounds while a rounding gate waits.  The waiting
     // gates keep their order.
     void flush_reg(Buffer& b, const std::vector<uint32_t>& wires, int id) {
-        const int cap = tile_wb + 4;
+        const int cap = tile_wb + tile_rb;
         std::vector<Sched> pending;
         for (uint32_t gi : b.pending) pending.push_back(classify(gates[gi], wires));
         while (!pending.empty()) {
@@ -669,7 +683,7 @@ struct Plan {
         Buffer& b = bufs[size_t(id)];
         if (b.pending.empty()) return;
         const int legs = b.legs;
-        if (legs >= 9 + tile_wb) {
+        if (legs >= 5 + tile_wb + tile_rb) {
             flush_reg(b, wires, id);
             gate_total += uint32_t(b.pending.size());
             b.pending.clear();
@@ -915,7 +929,7 @@ struct wqc_exact {
     int device = 0;
     int sm_count = 148;
     int pass_bits = kMaxPassBits;
-    int tile_bits = 12;  // register tiles of 2^12 amplitudes (256 threads x 16)
+    int tile_wb = 3, tile_rb = 4;  // register tiles: 2^tile_wb warps, 2^tile_rb amplitudes a thread
     cudaStream_t stream = nullptr;
     double2* arena = nullptr;
     uint64_t arena_bytes = 0;
@@ -998,10 +1012,10 @@ wqc_status wqc_exact_create(wqc_cuda_ctx* ctx, wqc_exact** out) {
         e = cudaFuncSetAttribute(exact_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sizeof(double2)) << kMaxPassBits);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(exact_pass_reg_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(exact_pass_reg_kernel<3, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sizeof(double2)) << 12);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(exact_pass_reg_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(exact_pass_reg_kernel<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sizeof(double2)) << 13);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ex->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -1027,7 +1041,8 @@ void wqc_exact_destroy(wqc_exact* ex) {
 wqc_status wqc_exact_set_tile_bits(wqc_exact* ex, int32_t bits) {
     if (!ex) return failx("null executor");
     if (bits != 12 && bits != 13) return failx("tile bits must be 12 or 13");
-    ex->tile_bits = bits;
+    ex->tile_wb = bits == 13 ? 4 : 3;
+    ex->tile_rb = 4;
     return WQC_OK;
 }
 
@@ -1073,7 +1088,8 @@ wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t n, const wqc_gate* gates, 
     Plan plan;
     plan.on = true;
     plan.pass_bits = ex->pass_bits;
-    plan.tile_wb = ex->tile_bits - 9;
+    plan.tile_wb = ex->tile_wb;
+    plan.tile_rb = ex->tile_rb;
     plan.gates = gates;
     Walker w(n, gates, gate_count, tree->node_count, &plan);
     uint64_t peak = 0;
@@ -1172,13 +1188,13 @@ wqc_status wqc_exact_contract(wqc_exact* ex, uint32_t n, const wqc_gate* gates, 
                 exact_pass_kernel<<<grid, kPassThreads, size_t(16) << it.hdr.local, st>>>(at(it.buf), it.hdr,
                                                                                            d_gates + it.gate_off);
             } else {
-                const int tile = 9 + plan.tile_wb;  // grid: one block per tile, 2^(legs - tile) tiles
+                const int tile = 5 + plan.tile_wb + plan.tile_rb;  // grid: one block per tile, 2^(legs - tile) tiles
                 const uint32_t grid = 1u << (it.legs - tile);
                 const size_t smem = it.xchg ? size_t(16) << tile : 0;
                 if (plan.tile_wb == 3)
-                    exact_pass_reg_kernel<3><<<grid, 256, smem, st>>>(at(it.buf), it.rhdr, d_ops + it.gate_off);
+                    exact_pass_reg_kernel<3, 4><<<grid, 256, smem, st>>>(at(it.buf), it.rhdr, d_ops + it.gate_off);
                 else
-                    exact_pass_reg_kernel<4><<<grid, 512, smem, st>>>(at(it.buf), it.rhdr, d_ops + it.gate_off);
+                    exact_pass_reg_kernel<4, 4><<<grid, 512, smem, st>>>(at(it.buf), it.rhdr, d_ops + it.gate_off);
             }
             if (time_it) {
                 cudaEventRecord(b, st);
