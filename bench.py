@@ -244,6 +244,124 @@ def precision_leg(W, torch, ctx, w, rule, steps: int, flush, fp64_value: float) 
     return out
 
 
+def measured_tf32_peak(torch) -> float:
+    """cuBLAS TF32 GEMM throughput (TFLOP/s, FP32 operands with TF32 tensor
+    math), best of 5 on 8192^3: the roofline of the tensor-core GEMM."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    try:
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            e1.synchronize()
+            best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+        del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+    return best
+
+
+def whole_circuit_profile(W, torch, ctx, w, rule, precision: int, flush) -> tuple[float, int, dict]:
+    """One untimed warm-up pass and one timed pass of the whole circuit from
+    |0...0> with per-kernel events: (ms, splits, kernel milliseconds)."""
+    m = W.CudaMps(w.n, w.chi, ctx=ctx, precision=precision)
+    m.set_split_rule(rule)
+    stream = torch.cuda.ExternalStream(m.stream())
+    ms = 0.0
+    for k in range(2):
+        m.reset()
+        m.reset_stats()
+        m.set_profiling(k == 1)
+        flush.fill_(float(np.random.random()))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.apply_gates(w.gates)
+        m.amplitude_at_compact_zero()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+    m.set_profiling(False)
+    st = m.kernel_stats()
+    splits = m.split_count()
+    m.close()
+    return ms, splits, st["milliseconds"]
+
+
+def tensor_core_leg(W, torch, ctx, w, rule, flush, gemm_only: bool = False) -> dict:
+    """The tcgen05 complex GEMM (wqc_tc_zgemm: 3xTF32 split products, FP32
+    accumulation in tensor memory, TMA-fed) on 4096^3 against cuBLAS TF32
+    measured here, then the tensor-core form (WQC_PRECISION_TF32X3: every
+    merge on that GEMM) on the whole headline circuit beside the plain form,
+    and its error against FP64 on the 16-qubit chi 32 brickwork."""
+    from wqc_cuda import tc as T
+
+    peak = measured_tf32_peak(torch)
+    rng = np.random.default_rng(2024)
+    n = 4096
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    b = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    reps = 10
+    c, ms = T.zgemm(a, b, reps=reps, ctx=ctx)
+    rows = rng.choice(n, 64, replace=False)
+    ref = a[rows] @ b
+    err = float(np.linalg.norm(c[rows] - ref) / np.linalg.norm(ref))
+    del a, b, c
+    tensor = 24.0 * n ** 3 / (ms * 1e-3) / 1e12  # 3 products x 2 flops x m x 2n x 2k of the real embedding
+    out = {
+        "gemm": {
+            "shape": f"complex {n} x {n} x {n}, operands resident, {reps} launches",
+            "kernel_ms": ms,
+            "complex_tflops": 8.0 * n ** 3 / (ms * 1e-3) / 1e12,
+            "roofline": {"bound": "tensor", "achieved": tensor, "peak": peak, "unit": "TFLOP/s",
+                         "frac": tensor / peak,
+                         "peak_source": "cuBLAS TF32 GEMM (torch.matmul, FP32 8192^3, TF32 math) measured in this run",
+                         "work": "24 m n k: three TF32 products (lo*hi, hi*lo, hi*hi) of the m x 2k by 2k x 2n "
+                                 "real embedding"},
+            "rel_err_vs_fp64": err,
+            "error_sample": "64 random rows against numpy FP64",
+        },
+    }
+    if gemm_only:
+        return out
+    fp64_ms, fp64_splits, fp64_k = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_FP64, flush)
+    tc_ms, tc_splits, tc_k = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_TF32X3, flush)
+    w0 = C.config0()
+    amps, recs = [], []
+    for prec in (W.PRECISION_FP64, W.PRECISION_TF32X3):
+        m0 = W.CudaMps(w0.n, w0.chi, ctx=ctx, precision=prec)
+        m0.apply_gates(w0.gates)
+        amps.append(m0.amplitude_at_compact_zero())
+        recs.append(m0.split_records())
+        m0.close()
+    out["form"] = {
+        "form": "WQC_PRECISION_TF32X3: every merge on the tcgen05 GEMM (theta in FP32-level precision, the 4x4 "
+                "gate in FP64), the precision form's two-phase Jacobi, singular values below 1e-6 of the largest "
+                "counted as zero",
+        "workload": "whole circuit from |0...0>, one timed pass per form with per-kernel events",
+        "value": tc_splits / (tc_ms * 1e-3),
+        "fp64_value": fp64_splits / (fp64_ms * 1e-3),
+        "unit": UNIT,
+        "merge_ms": tc_k["merge_gate"],
+        "fp64_merge_ms": fp64_k["merge_gate"],
+        "splits": tc_splits,
+        "fp64_splits": fp64_splits,
+        "amp_rel_err_vs_fp64": abs(amps[1] - amps[0]) / abs(amps[0]),
+        "kept_chi_differs": int(np.count_nonzero(recs[0]["chi"] != recs[1]["chi"])) if len(recs[0]) == len(recs[1])
+        else None,
+        "error_workload": f"{w0.name}: {w0.n} qubits, chi_max {w0.chi}, against the plain FP64 form",
+    }
+    return out
+
+
 def oracle_gradient_sample(n, chi, lists, labels, coeffs, budget_s: float, threads: int):
     """CPU leg of the differentiation form: threads run whole shifted circuits
     (and the observable) on the oracle until `budget_s`; returns (circuits
@@ -961,6 +1079,13 @@ def run_cuda(args) -> None:
     w = workload(args.workload, args.depth)
     g0, windows = timed_windows(w, SATURATED_LAYERS.get(args.workload, 0), args.steps)
     rule = W.SPLIT_RULE_EXACT if args.split_rule == "exact" else W.SPLIT_RULE_REFERENCE
+    if args.tensor_core_only:
+        ctx = W.Context(local)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+        leg = tensor_core_leg(W, torch, ctx, w, rule, flush, gemm_only=args.tensor_core_only == "gemm")
+        if rank == 0:
+            print(json.dumps({"tensor_core": leg}), flush=True)
+        return
     ctx = W.Context(local)
     # Jacobi cluster sizes measured on this device (or loaded from the
     # fingerprinted cache), before any timed work.
@@ -1123,6 +1248,8 @@ def run_cuda(args) -> None:
                                                           0.0 if args.no_cpu_baseline else args.cpu_budget)
         if world == 1 and args.large_chi_leg:
             line["large_chi"] = large_chi_leg(W, torch, ctx, flush, 0.0 if args.no_cpu_baseline else args.cpu_budget)
+        if world == 1 and args.tensor_core_leg:
+            line["tensor_core"] = tensor_core_leg(W, torch, ctx, w, rule, flush)
         if world == 1 and args.precision_leg:
             line["precision_form"] = precision_leg(W, torch, ctx, w, rule, 2, flush, whole_splits / (whole_ms * 1e-3))
             if args.batch_slices > 0:
@@ -1168,6 +1295,10 @@ def main():
                     help="skip the 100-qubit chi 256 circuit run after the timed steps")
     ap.add_argument("--no-precision-leg", dest="precision_leg", action="store_false",
                     help="skip the precision-form (complex64 Jacobi) leg run after the timed steps")
+    ap.add_argument("--no-tensor-core-leg", dest="tensor_core_leg", action="store_false",
+                    help="skip the tcgen05 GEMM and the tensor-core form (WQC_PRECISION_TF32X3)")
+    ap.add_argument("--tensor-core-only", choices=("gemm", "form"), default=None,
+                    help="run only the tensor-core leg (gemm: the 4096^3 GEMM alone) and print it (for profiling)")
     ap.add_argument("--batch-slices", type=int, default=512,
                     help="slices of the batching-form leg run once after the timed steps (0 = skip)")
     args = ap.parse_args()

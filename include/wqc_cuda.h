@@ -50,7 +50,7 @@ enum wqc_status_code {
 /* Arithmetic of the split path. */
 enum wqc_precision {
     WQC_PRECISION_FP64 = 0, /* plain form: complex128 throughout */
-    WQC_PRECISION_FP32 = 1  /* precision form: each Jacobi SVD runs in two phases.  The
+    WQC_PRECISION_FP32 = 1, /* precision form: each Jacobi SVD runs in two phases.  The
                                first sweeps complex64 columns (FP32 dot products and
                                rotation updates, FP64 rotation parameters, tolerance and
                                convergence tests) that carry X V and the accumulated V;
@@ -59,6 +59,13 @@ enum wqc_precision {
                                sweeps finish from there (quadratic convergence: a few
                                sweeps).  Sites, merges, range finder, sort and cut stay
                                FP64, so results carry FP64-level error. */
+    WQC_PRECISION_TF32X3 = 2 /* tensor-core form: the precision form's Jacobi, with every
+                               two-site merge (theta = L R and the 4x4 gate) on the tcgen05
+                               tensor cores: operands split into TF32 hi and lo parts, the
+                               three products lo*hi + hi*lo + hi*hi accumulated in FP32
+                               in tensor memory, the gate applied in FP64 to the FP32
+                               product.  Each theta carries FP32-level error (about 1e-7
+                               relative), which the splits after it carry on. */
 };
 
 typedef struct wqc_cuda_ctx wqc_cuda_ctx;
@@ -537,6 +544,22 @@ typedef struct wqc_network_stats {
     uint32_t small;          /* small contractions, run one block each in level-batched launches */
 } wqc_network_stats;
 WQC_API wqc_status wqc_network_last_stats(wqc_network* net, wqc_network_stats* out);
+
+/* ------------------------------------------------------------------------
+ * Complex GEMM on the tcgen05 tensor cores: the product of the tensor-core
+ * form's two-site merge (mps.rs:812-831, the cpu_merge product; the webgpu
+ * backend's gemm.wgsl is its GPU counterpart), here on its own.
+ * C = A B with A m x k, B k x n, C m x n, row-major complex FP64 in host
+ * memory (re, im interleaved).  Each operand is split into two TF32 values
+ * (hi, lo = x - hi) and the three products lo*hi + hi*lo + hi*hi accumulate
+ * in FP32 in tensor memory (kind::tf32, operands TMA-loaded with the 128-byte
+ * swizzle): results carry FP32-level error, about 1e-6 of
+ * max_i |A_i| max_j |B_j| (row and column 2-norms).  The GEMM kernel runs
+ * `reps` times (0 counts as 1) on operands staged on the device once;
+ * *kernel_ms (may be NULL) receives the mean CUDA-event time of one launch.
+ * Sizes 1..16384. */
+WQC_API wqc_status wqc_tc_zgemm(wqc_cuda_ctx* ctx, uint32_t m, uint32_t n, uint32_t k, const double* a,
+                                const double* b, double* c, uint32_t reps, double* kernel_ms);
 
 #ifdef __cplusplus
 }

@@ -59,6 +59,7 @@ enum : int {
     kStatusNonFinite = 1 << 3,
     kStatusCancelled = 1 << 4,
     kStatusSvdCheck = 1 << 5,  // sum sigma^2 != ||X||_F^2 (svd_guard.rs:234-255)
+    kStatusDeviceTimeout = 1 << 6,  // a bounded wait on an mbarrier gave up
 };
 
 // ---------------------------------------------------------------------------

@@ -24,6 +24,7 @@
 #include "../../include/wqc_cuda.h"
 #include "common.cuh"
 #include "split_kernels.cuh"
+#include "tc_gemm.cuh"
 
 using namespace wqc;
 
@@ -212,7 +213,14 @@ struct wqc_mps {
     int n = 0, chi = 0;
     bool reject = false;
     bool exact_only = false;  // WQC_SPLIT_RULE_EXACT
-    bool fp32 = false;        // WQC_PRECISION_FP32: complex64 Jacobi columns
+    bool fp32 = false;        // WQC_PRECISION_FP32 or _TF32X3: complex64 Jacobi columns
+    // WQC_PRECISION_TF32X3: merges on the tensor cores (tc_gemm.cu), their
+    // operands staged per wave job as TF32 hi/lo planes under two tensor maps
+    bool tc = false;
+    float* tc_a = nullptr;
+    float* tc_b = nullptr;
+    int tc_rpad = 0, tc_npad = 0, tc_kpad = 0;
+    CUtensorMap tc_map_a{}, tc_map_b{};
     bool batch = false;       // made by wqc_batch_create: Jacobi clusters sized for throughput
     cudaStream_t stream = nullptr;
     // Second stream of a wave: the exact-path SVDs run there while the range
@@ -873,15 +881,32 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
         }
         const SplitJob* d_jobs = d_jobs_all + w.jobs_off;
         const int nj = w.njobs;
-        // Both forms end on FP64 columns: no singular value is FP32 noise.
-        const double noise_rel = 0.0;
+        // The plain and precision forms end on FP64 columns of an FP64 theta:
+        // no singular value is FP32 noise.  The tensor-core form's theta
+        // carries FP32-level error (~1e-7 of its norm), which shows as
+        // singular values of ~1e-8 of the largest where theta has none; those
+        // below 1e-6 of the largest count as zero.
+        const double noise_rel = m->tc ? 1e-6 : 0.0;
         {
             Timed t(m, 1);
             prepare_kernel<<<(nj + 127) / 128, 128, 0, m->stream>>>(d_jobs, m->d_state, nj, m->dev);
             count_launch(m, 1);
-            dim3 g((w.max_dr + 15) / 16, (w.max_dl + 15) / 16, nj);
-            merge_gate_kernel<<<g, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);
-            count_launch(m, 1);
+            if (m->tc) {
+                // one thread per complex value of L, one block per 32 K values of an N tile of R
+                const int a_blocks = std::max(1, (w.max_rows * m->chi + 255) / 256);
+                const dim3 gp(a_blocks + ((w.max_dr + 31) / 32) * (m->tc_kpad / kTcKBlock), nj);
+                tc_prep_merge_kernel<<<gp, 256, 0, m->stream>>>(d_jobs, m->d_state, m->dev, m->tc_a, m->tc_b,
+                                                                m->tc_rpad, m->tc_npad, m->tc_kpad, a_blocks);
+                count_launch(m, 1);
+                const dim3 g((w.max_dr + 31) / 32, (w.max_rows + kTcTileM - 1) / kTcTileM, nj);
+                CUDA_TRY(launch_tc_merge(m->tc_map_a, m->tc_map_b, g, m->stream,
+                                         TcMergeArgs{d_jobs, m->d_state, m->d_slots}, m->d_status));
+                count_launch(m, 1);
+            } else {
+                dim3 g((w.max_dr + 15) / 16, (w.max_dl + 15) / 16, nj);
+                merge_gate_kernel<<<g, 256, 0, m->stream>>>(d_jobs, m->d_state, m->d_slots, m->dev);
+                count_launch(m, 1);
+            }
         }
         auto launch_phase = [&](const Group& gr, const PhaseCfg& pc, int mode, int phase, bool fp32,
                                 cudaStream_t on) -> wqc_status {
@@ -1098,6 +1123,7 @@ wqc_status sync_status(wqc_mps* m) {
     if (st & kStatusTruncationRejected) return fail(WQC_ERR_TRUNCATION_REJECTED, "mps bond exceeded chi");
     if (st & kStatusNonFinite) return fail(WQC_ERR_SVD_FAILED, "SVD of a two-site matrix produced non-finite values");
     if (st & kStatusSvdCheck) return fail(WQC_ERR_SVD_FAILED, "SVD of a two-site matrix failed its check");
+    if (st & kStatusDeviceTimeout) return fail(WQC_ERR_DEVICE_TIMEOUT, "a tensor-core merge gave up waiting on its operands");
     if (st & kStatusJacobiNoConvergence) {
         const unsigned long long bits = (static_cast<unsigned long long>(static_cast<unsigned>(stv[3])) << 32) |
                                         static_cast<unsigned>(stv[4]);
@@ -1218,7 +1244,7 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
         total_n += ns[i];
         chi_cap = std::max(chi_cap, chis[i]);
     }
-    if (precision != WQC_PRECISION_FP64 && precision != WQC_PRECISION_FP32)
+    if (precision != WQC_PRECISION_FP64 && precision != WQC_PRECISION_FP32 && precision != WQC_PRECISION_TF32X3)
         return fail(WQC_ERR_INVALID, "unsupported precision form");
     if (total_n > (1L << 24)) return fail(WQC_ERR_INVALID, "too many sites");
     CUDA_TRY(cudaSetDevice(ctx->device));
@@ -1228,7 +1254,8 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     m->n = n;
     m->chi = chi_cap;
     m->reject = reject;
-    m->fp32 = precision == WQC_PRECISION_FP32;
+    m->fp32 = precision != WQC_PRECISION_FP64;
+    m->tc = precision == WQC_PRECISION_TF32X3;
     m->ub.assign(n > 0 ? n - 1 : 0, 1);
     m->site_chi.resize(n);
     m->site_slice.resize(n);
@@ -1263,7 +1290,7 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     // The staged Jacobi's workspace holds (R + 32) x R complex128 values: the
     // padded FP64 columns, or the precision form's complex64 columns with V
     // under them ((R + 32) x 2R complex64 values, the same bytes).
-    const bool fp32 = precision == WQC_PRECISION_FP32;
+    const bool fp32 = precision != WQC_PRECISION_FP64;
     auto no_cluster = [&](int M, int N) {
         return choose_cluster(nullptr, M, N, ctx->max_cluster, 1, ctx->sm_count, sizeof(double2), false) < 1 ||
                (fp32 &&
@@ -1297,7 +1324,18 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     size_t slot_pool_bytes = 0;
     for (size_t b = 0; b < m->bucket_chi.size(); ++b) slot_pool_bytes += bucket_bytes[b] * size_t(m->bucket_cap[b]);
     const size_t site_bytes = site_off[n] * sizeof(double2);
-    const uint64_t need = site_bytes + uint64_t(slot_pool_bytes);
+    // Tensor-core form: TF32 hi/lo planes of both merge operands for every job
+    // a wave can hold (one per slot), padded to whole tiles of the largest
+    // two-site matrix.
+    size_t tc_a_bytes = 0, tc_b_bytes = 0;
+    if (m->tc) {
+        m->tc_rpad = tc_rpad(2 * chi_cap);
+        m->tc_kpad = tc_kpad(chi_cap);
+        m->tc_npad = tc_npad(2 * chi_cap);
+        tc_a_bytes = size_t(2) * m->nslots * m->tc_rpad * m->tc_kpad * sizeof(float);
+        tc_b_bytes = size_t(2) * m->nslots * m->tc_npad * m->tc_kpad * sizeof(float);
+    }
+    const uint64_t need = site_bytes + uint64_t(slot_pool_bytes) + tc_a_bytes + tc_b_bytes;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "cudaMemGetInfo"));
     if (need > fr) return bail(fail_oom(need, fr));
@@ -1314,6 +1352,15 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     m->d_seg = static_cast<int*>(p);
     if (wqc_status st = dmalloc(m, &p, slot_pool_bytes)) return bail(st);
     m->slot_pool = static_cast<char*>(p);
+    if (m->tc) {
+        if (wqc_status st = dmalloc(m, &p, tc_a_bytes)) return bail(st);
+        m->tc_a = static_cast<float*>(p);
+        if (wqc_status st = dmalloc(m, &p, tc_b_bytes)) return bail(st);
+        m->tc_b = static_cast<float*>(p);
+        if (!tc_encode_planes(&m->tc_map_a, m->tc_a, m->tc_kpad, m->tc_rpad, 2 * m->nslots) ||
+            !tc_encode_planes(&m->tc_map_b, m->tc_b, m->tc_kpad, m->tc_npad, 2 * m->nslots))
+            return bail(fail(WQC_ERR_CUDA, "cuTensorMapEncodeTiled refused the merge operand planes"));
+    }
     if (wqc_status st = dmalloc(m, &p, m->nslots * sizeof(SlotBuffers))) return bail(st);
     m->d_slots = static_cast<SlotBuffers*>(p);
     if (wqc_status st = dmalloc(m, &p, m->nslots * sizeof(SplitState))) return bail(st);
@@ -1436,6 +1483,8 @@ void wqc_mps_destroy(wqc_mps* m) {
     dfree(m, m->d_site_ptr, 0);
     dfree(m, m->d_dl, 0);
     dfree(m, m->slot_pool, 0);
+    dfree(m, m->tc_a, 0);
+    dfree(m, m->tc_b, 0);
     dfree(m, m->d_slots, 0);
     dfree(m, m->d_state, 0);
     dfree(m, m->d_small, 0);

@@ -34,6 +34,7 @@ ERR_INVALID_QUBIT_COUNT = 10
 
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1
+PRECISION_TF32X3 = 2
 OVERLAP_ENV_LIMIT = 256  # mps.rs:1443-1448 (the STARK witness limit)
 SPLIT_RULE_REFERENCE = 0
 SPLIT_RULE_EXACT = 1
@@ -54,7 +55,7 @@ EXPORTS = (
     "wqc_exact_create", "wqc_exact_destroy", "wqc_exact_validate", "wqc_exact_measured_peak", "wqc_exact_contract",
     "wqc_exact_cancel", "wqc_exact_last_stats", "wqc_exact_set_tile_bits",
     "wqc_network_create", "wqc_network_destroy", "wqc_network_validate", "wqc_network_measured_peak",
-    "wqc_network_contract", "wqc_network_cancel", "wqc_network_last_stats",
+    "wqc_network_contract", "wqc_network_cancel", "wqc_network_last_stats", "wqc_tc_zgemm",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")

@@ -1,0 +1,38 @@
+"""The tcgen05 tensor-core complex GEMM (``wqc_tc_zgemm`` of
+include/wqc_cuda.h): C = A B with 3xTF32 split products and FP32
+accumulation, the product of the tensor-core form's two-site merge
+(src/tn/mps.rs:812-831) on its own."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import Context, _check, lib
+
+
+def _bind(L):
+    if getattr(L, "_tc_bound", False):
+        return L
+    P, U32 = ctypes.c_void_p, ctypes.c_uint32
+    L.wqc_tc_zgemm.argtypes = [P, U32, U32, U32, P, P, P, U32, ctypes.POINTER(ctypes.c_double)]
+    L._tc_bound = True
+    return L
+
+
+def zgemm(a, b, reps: int = 1, ctx: Context | None = None):
+    """(C, kernel_ms): C = a @ b for complex matrices a (m x k) and b (k x n)
+    on the tensor cores; kernel_ms is the mean device time of one GEMM launch
+    over `reps` launches."""
+    ctx = ctx or Context.shared()
+    L = _bind(lib())
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    b = np.ascontiguousarray(b, dtype=np.complex128)
+    if a.ndim != 2 or b.ndim != 2 or a.shape[1] != b.shape[0]:
+        raise ValueError(f"shapes {a.shape} and {b.shape} do not multiply")
+    m, k = a.shape
+    n = b.shape[1]
+    c = np.zeros((m, n), dtype=np.complex128)
+    ms = ctypes.c_double(0.0)
+    _check(L.wqc_tc_zgemm(ctx._h, m, n, k, a.ctypes.data, b.ctypes.data, c.ctypes.data, int(reps), ctypes.byref(ms)))
+    return c, ms.value
