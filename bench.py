@@ -269,11 +269,13 @@ def measured_tf32_peak(torch) -> float:
     return best
 
 
-def whole_circuit_profile(W, torch, ctx, w, rule, precision: int, flush) -> tuple[float, int, dict]:
+def whole_circuit_profile(W, torch, ctx, w, rule, precision: int, flush, merge: int = 0) -> tuple[float, int, dict]:
     """One untimed warm-up pass and one timed pass of the whole circuit from
     |0...0> with per-kernel events: (ms, splits, kernel milliseconds)."""
     m = W.CudaMps(w.n, w.chi, ctx=ctx, precision=precision)
     m.set_split_rule(rule)
+    if merge:
+        m.set_merge(merge)
     stream = torch.cuda.ExternalStream(m.stream())
     ms = 0.0
     for k in range(2):
@@ -330,9 +332,36 @@ def tensor_core_leg(W, torch, ctx, w, rule, flush, gemm_only: bool = False) -> d
             "error_sample": "64 random rows against numpy FP64",
         },
     }
+    # the same product from int8 digit slices (45 slice products, exact int32
+    # accumulation): FP64-level, on the integer tensor pipe
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    b = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    c, ms8 = T.zgemm(a, b, reps=5, ctx=ctx, form="int8")
+    ref = a[rows] @ b
+    err8 = float(np.linalg.norm(c[rows] - ref) / np.linalg.norm(ref))
+    del a, b, c
+    out["gemm_int8"] = {
+        "shape": f"complex {n} x {n} x {n}, operands resident, 5 launches",
+        "kernel_ms": ms8,
+        "complex_tflops": 8.0 * n ** 3 / (ms8 * 1e-3) / 1e12,
+        "int8_tops": 360.0 * n ** 3 / (ms8 * 1e-3) / 1e12,
+        "work": "360 m n k int8 ops: 45 digit-slice products of the m x 2k by 2k x 2n real embedding",
+        "rel_err_vs_fp64": err8,
+        "error_sample": "64 random rows against numpy FP64",
+    }
     if gemm_only:
         return out
     fp64_ms, fp64_splits, fp64_k = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_FP64, flush)
+    i8_ms, i8_splits, i8_k = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_FP64, flush,
+                                                   merge=W.MERGE_TC_INT8)
+    out["int8_merge"] = {
+        "form": "plain FP64 form with every merge from int8 digit slices on the tensor cores (WQC_MERGE_TC_INT8)",
+        "value": i8_splits / (i8_ms * 1e-3),
+        "fp64_value": fp64_splits / (fp64_ms * 1e-3),
+        "unit": UNIT,
+        "merge_ms": i8_k["merge_gate"],
+        "fp64_merge_ms": fp64_k["merge_gate"],
+    }
     tc_ms, tc_splits, tc_k = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_TF32X3, flush)
     w0 = C.config0()
     amps, recs = [], []

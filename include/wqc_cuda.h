@@ -197,6 +197,19 @@ WQC_API wqc_status wqc_mps_apply_layer(wqc_mps* mps, const wqc_gate* gates, uint
 enum wqc_split_rule { WQC_SPLIT_RULE_REFERENCE = 0, WQC_SPLIT_RULE_EXACT = 1 };
 WQC_API wqc_status wqc_mps_set_split_rule(wqc_mps* mps, int32_t rule);
 
+/* How the state performs its merges (merge_two_site_tensors / cpu_merge,
+ * mps.rs:484-514, 812-831, with the 4x4 of mps.rs:833-866; applies to merges
+ * enqueued afterwards).  FFMA (the default): tiled FP64 FMA.  TC_INT8: on the
+ * tcgen05 tensor cores from int8 digit slices (the Ozaki scheme): each row of
+ * L and each column of R scaled by a power of two, cut into 9 signed 7-bit
+ * digits (63 bits), the digit products exact in int32 in tensor memory and
+ * summed in FP64 -- FP64-level results (the dropped slice products lie below
+ * 2^-60 of the row and column maxima) from the integer tensor pipe.  The first TC_INT8 call
+ * allocates the digit planes of every split slot (WQC_ERR_OOM if they do not
+ * fit).  Not for the tensor-core form, whose merges are its TF32 path. */
+enum wqc_merge { WQC_MERGE_FFMA = 0, WQC_MERGE_TC_INT8 = 1 };
+WQC_API wqc_status wqc_mps_set_merge(wqc_mps* mps, int32_t merge);
+
 /* Host-only: how wqc_mps_apply_gates would schedule `gates` on n sites,
  * without a device.  For each split in program order, its left site and its
  * level (splits of one level run concurrently); *nsplits and *nlevels
@@ -560,6 +573,12 @@ WQC_API wqc_status wqc_network_last_stats(wqc_network* net, wqc_network_stats* o
  * Sizes 1..16384. */
 WQC_API wqc_status wqc_tc_zgemm(wqc_cuda_ctx* ctx, uint32_t m, uint32_t n, uint32_t k, const double* a,
                                 const double* b, double* c, uint32_t reps, double* kernel_ms);
+
+/* The same product from int8 digit slices on the tensor cores (kind::i8,
+ * the scheme of WQC_MERGE_TC_INT8): FP64-level results.  m, n in 1..8192,
+ * k in 1..4096 (the int32 accumulators' bound). */
+WQC_API wqc_status wqc_tc_zgemm_int8(wqc_cuda_ctx* ctx, uint32_t m, uint32_t n, uint32_t k, const double* a,
+                                     const double* b, double* c, uint32_t reps, double* kernel_ms);
 
 #ifdef __cplusplus
 }

@@ -44,12 +44,15 @@ def assert_shapes_exact(got, ref):
         assert bad.size == 0, f"{k} differs at splits {bad[:10]}"
 
 
-def test_config1_exact_rule_at_full_size(cuda_ctx):
+@pytest.mark.parametrize("merge", [W.MERGE_FFMA, W.MERGE_TC_INT8], ids=["ffma_merge", "tc_int8_merge"])
+def test_config1_exact_rule_at_full_size(cuda_ctx, merge):
+    """Also with every merge on the tensor cores from int8 digit slices
+    (WQC_MERGE_TC_INT8): the same bar as the FP64 FMA merge."""
     fx = fixture("config1_exact.npz")
     dr = fixture("config1_drift.npz")
     w = C.config1()
     assert (w.n, w.chi, w.seed) == (int(fx["n"]), int(fx["chi"]), int(fx["seed"]))
-    m = W.run(w.n, w.chi, w.gates, ctx=cuda_ctx, rule=W.SPLIT_RULE_EXACT)
+    m = W.run(w.n, w.chi, w.gates, ctx=cuda_ctx, rule=W.SPLIT_RULE_EXACT, merge=merge)
     rec, ref = m.split_records(), fx["records"]
     assert_shapes_exact(rec, ref)
     assert np.array_equal(m.bond_dims(), fx["bond_dims"])

@@ -221,6 +221,12 @@ struct wqc_mps {
     float* tc_b = nullptr;
     int tc_rpad = 0, tc_npad = 0, tc_kpad = 0;
     CUtensorMap tc_map_a{}, tc_map_b{};
+    // WQC_MERGE_TC_INT8 (wqc_mps_set_merge): merges from int8 digit slices
+    // on the tensor cores (tc_ozaki.cu), staged per wave job
+    bool oz = false;
+    void* oz_pool = nullptr;
+    size_t oz_bytes = 0;
+    OzPlanes oz_planes;
     bool batch = false;       // made by wqc_batch_create: Jacobi clusters sized for throughput
     cudaStream_t stream = nullptr;
     // Second stream of a wave: the exact-path SVDs run there while the range
@@ -891,7 +897,18 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
             Timed t(m, 1);
             prepare_kernel<<<(nj + 127) / 128, 128, 0, m->stream>>>(d_jobs, m->d_state, nj, m->dev);
             count_launch(m, 1);
-            if (m->tc) {
+            if (m->oz) {
+                // rows of L by warps, N tiles of R (8 values of b) by blocks
+                const int a_blocks = std::max(1, (w.max_rows + 7) / 8);
+                const int ntiles = (w.max_dr + 7) / 8;
+                oz_prep_merge_kernel<<<dim3(a_blocks + ntiles, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->dev,
+                                                                                         m->oz_planes, a_blocks);
+                count_launch(m, 1);
+                const dim3 g(ntiles, (w.max_rows + kOzTileM - 1) / kOzTileM, nj);
+                CUDA_TRY(launch_oz_merge(m->oz_planes, g, m->stream, TcMergeArgs{d_jobs, m->d_state, m->d_slots},
+                                         m->d_status));
+                count_launch(m, 1);
+            } else if (m->tc) {
                 // one thread per complex value of L, one block per 32 K values of an N tile of R
                 const int a_blocks = std::max(1, (w.max_rows * m->chi + 255) / 256);
                 const dim3 gp(a_blocks + ((w.max_dr + 31) / 32) * (m->tc_kpad / kTcKBlock), nj);
@@ -1485,6 +1502,7 @@ void wqc_mps_destroy(wqc_mps* m) {
     dfree(m, m->slot_pool, 0);
     dfree(m, m->tc_a, 0);
     dfree(m, m->tc_b, 0);
+    dfree(m, m->oz_pool, 0);
     dfree(m, m->d_slots, 0);
     dfree(m, m->d_state, 0);
     dfree(m, m->d_small, 0);
@@ -1719,6 +1737,31 @@ wqc_status wqc_mps_set_split_rule(wqc_mps* m, int32_t rule) {
     if (!m) return fail(WQC_ERR_INVALID, "null argument");
     if (rule != WQC_SPLIT_RULE_REFERENCE && rule != WQC_SPLIT_RULE_EXACT) return fail(WQC_ERR_INVALID, "unknown split rule");
     m->exact_only = rule == WQC_SPLIT_RULE_EXACT;
+    return WQC_OK;
+}
+
+wqc_status wqc_mps_set_merge(wqc_mps* m, int32_t merge) {
+    if (!m) return fail(WQC_ERR_INVALID, "null argument");
+    if (merge != WQC_MERGE_FFMA && merge != WQC_MERGE_TC_INT8) return fail(WQC_ERR_INVALID, "unknown merge");
+    if (m->tc) return fail(WQC_ERR_INVALID, "the tensor-core form merges on its own TF32 path");
+    CUDA_TRY(cudaSetDevice(m->ctx->device));
+    CUDA_TRY(cudaStreamSynchronize(m->stream));  // no enqueued merge still reads the planes
+    if (merge == WQC_MERGE_TC_INT8 && !m->oz_pool) {
+        const int rpad = oz_rpad(2 * m->chi), npad = oz_npad(2 * m->chi), kpad = oz_kpad(m->chi);
+        const size_t bytes = oz_planes_bytes(m->nslots, rpad, npad, kpad);
+        size_t fr = 0, tot = 0;
+        CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+        if (bytes > fr) return fail_oom(bytes, fr);
+        void* p = nullptr;
+        if (wqc_status st = dmalloc(m, &p, bytes)) return st;
+        if (!oz_planes_init(&m->oz_planes, p, m->nslots, rpad, npad, kpad)) {
+            dfree(m, p, bytes);
+            return fail(WQC_ERR_CUDA, "cuTensorMapEncodeTiled refused the merge digit planes");
+        }
+        m->oz_pool = p;
+        m->oz_bytes = bytes;
+    }
+    m->oz = merge == WQC_MERGE_TC_INT8;
     return WQC_OK;
 }
 

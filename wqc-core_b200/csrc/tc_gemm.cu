@@ -4,7 +4,7 @@
 // exposed alone as wqc_tc_zgemm.  The layout of operands and tiles is
 // described in tc_gemm.cuh.
 //
-// Every wait on an mbarrier is bounded (kTcWaitNs); a wait that gives up sets
+// Every wait on an mbarrier is bounded (ptx::kWaitNs); a wait that gives up sets
 // kStatusDeviceTimeout, the thread stops issuing work, and the block still
 // waits (bounded) for what it issued and frees its tensor memory.
 #include <cudaTypedefs.h>
@@ -17,78 +17,21 @@
 #include "../../include/wqc_cuda.h"
 #include "split_kernels.cuh"
 #include "tc_gemm.cuh"
+#include "tc_ptx.cuh"
 
 namespace wqc {
 
 namespace {
 
-constexpr unsigned long long kTcWaitNs = 1000000000ull;  // 1 s per wait
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Wait until the phase of parity `parity` has completed; false after
-// kTcWaitNs (or an iteration bound) without it.
-__device__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    if (mbar_try(bar, parity)) return true;
-    const unsigned long long t0 = globaltimer_ns();
-    for (int i = 0; i < (1 << 26); ++i) {
-        if (mbar_try(bar, parity)) return true;
-        if ((i & 63) == 63 && globaltimer_ns() - t0 > kTcWaitNs) return false;
-    }
-    return false;
-}
-
-// 3-D tiled TMA load of one box into shared memory, completing on `bar`.
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
-            "r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
-        : "memory");
-}
-
-// Shared-memory matrix descriptor of a K-major operand tile with the 128-byte
-// swizzle: rows of 128 bytes, 8-row groups 1024 bytes apart (stride byte
-// offset), leading byte offset unused by this layout (1), descriptor version 1
-// (bits 46-47), layout type 2 = 128-byte swizzle (bits 61-63).
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
-    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t(1) << 16) | (uint64_t(1024 >> 4) << 32) | (uint64_t(1) << 46) |
-           (uint64_t(2) << 61);
-}
+using namespace ptx;
 
 // Instruction descriptor of kind::tf32: FP32 accumulator (bits 4-5 = 1), A
 // and B TF32 (bits 7-9, 10-12 = 2), both K-major, N >> 3 at bits 17-22, M >> 4
 // at bits 24-28.
 constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(kTcTileN >> 3) << 17) |
                               (uint32_t(kTcTileM >> 4) << 24);
+
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) { return umma_desc_kmajor<128>(addr); }
 
 __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
     asm volatile(
@@ -99,41 +42,29 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint6
         : "memory");
 }
 
-// Arrive on `bar` once every tcgen05 operation this thread issued so far has
-// completed.
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 // Tensor-memory columns: the even-K-block hi*hi accumulator at 0, the odd
 // one at kTcAccOdd, the lo*hi + hi*lo accumulator at kTcAccSmall (the
 // allocation is a power of two of at least 32 columns).
 constexpr uint32_t kTcAccOdd = kTcTileN, kTcAccSmall = 2 * kTcTileN;
 constexpr uint32_t kTcTmemCols = 512;
 
+__device__ __forceinline__ void tmem_ld16f(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    tmem_ld16(taddr, r);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // Sixteen accumulator columns at `taddr`, the three accumulators summed in
 // FP64 (`odd`: the second hi*hi accumulator holds a part).
 __device__ __forceinline__ void tmem_sum16(uint32_t taddr, bool odd, double* v) {
     float a[16], b[16];
-    tmem_ld16(taddr + kTcAccSmall, a);
-    tmem_ld16(taddr, b);
+    tmem_ld16f(taddr + kTcAccSmall, a);
+    tmem_ld16f(taddr, b);
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = double(b[i]) + double(a[i]);
     if (odd) {
-        tmem_ld16(taddr + kTcAccOdd, b);
+        tmem_ld16f(taddr + kTcAccOdd, b);
 #pragma unroll
         for (int i = 0; i < 16; ++i) v[i] += double(b[i]);
     }
@@ -312,12 +243,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                     "r"(kTcTmemCols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), kTcTmemCols);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -435,7 +361,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
+        tmem_dealloc(tmem, kTcTmemCols);
 }
 
 // ---------------------------------------------------------------------------

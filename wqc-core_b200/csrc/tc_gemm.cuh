@@ -70,4 +70,69 @@ cudaError_t launch_tc_merge(const CUtensorMap& ma, const CUtensorMap& mb, dim3 g
 cudaError_t launch_tc_plain(const CUtensorMap& ma, const CUtensorMap& mb, dim3 grid, cudaStream_t s,
                             const TcPlainArgs& args, int* status);
 
+// ---------------------------------------------------------------------------
+// FP64-accurate complex GEMM from int8 slices (the Ozaki scheme) on the
+// tcgen05 tensor cores, kind::i8 (tc_ozaki.cu).  Each row r of A (the real
+// embedding, as above) is scaled by 2^-e_r so that its largest entry lies in
+// [1/2, 1), each real column c of B2 by 2^-f_c, and every scaled value x is
+// cut into kOzSlices = 9 signed 7-bit digits, x = sum_p d_p 2^-7(p+1) + eps
+// with |eps| < 2^-63 (digits by truncation: |d_p| <= 127, the sign of x).
+// The slice products A_p B_q are exact in int32; those with p + q = d share
+// accumulator d (at most 9 products of K <= 8192 terms of |d_p e_q| <= 127^2:
+// below 2^31), and the products with p + q >= kOzSlices are dropped (all
+// together below 2^-60 of the two scales).  The epilogue sums the
+// accumulators in FP64, C[r][c] = 2^(e_r + f_c - 14) sum_d acc_d 2^-7d, so
+// the FP64 rounding of that sum is the error that remains.
+//
+// Staging: digit planes [job][slice][Rpad][Kpad] (A) and [job][slice][Npad]
+// [Kpad] (B, one row per real output column), int8, K innermost, zero beyond
+// the problem; exponents e [job][Rpad] and f [job][Npad / 2] (one per complex
+// output column: both real columns of a complex column have the same B2
+// column maximum).  TMA loads 64-byte x 128-row (A) and 64-byte x 64-row (B)
+// boxes with the 64-byte swizzle; one thread issues the 45 MMAs (M = 128,
+// N = 32, K = 32 bytes) of each 32-byte K step into 9 int32 accumulators in
+// tensor memory (9 x 32 of its 512 columns: nine accumulators of 64 columns
+// would not fit, hence the narrow tile).
+// ---------------------------------------------------------------------------
+constexpr int kOzSlices = 9;                                      // digits per operand: 63 bits
+constexpr int kOzTileM = 128;                                     // rows of a CTA tile
+constexpr int kOzTileN = 32;                                      // real columns of a CTA tile (16 complex)
+constexpr int kOzTileC = kOzTileN / 2;                            // complex columns of a CTA tile
+constexpr int kOzKBlock = 64;                                     // int8 K values per stage (64-byte rows)
+constexpr int kOzStages = 2;
+constexpr int kOzThreads = 128;
+constexpr int kOzABox = kOzTileM * kOzKBlock;                     // one A slice's box: 8 KB
+constexpr int kOzBBox = kOzTileN * kOzKBlock;                     // one B slice's box: 2 KB
+constexpr int kOzStageBytes = kOzSlices * (kOzABox + kOzBBox);    // 90 KB
+constexpr int kOzSmemBytes = kOzStages * kOzStageBytes + 1024;    // + alignment of the swizzled tiles
+
+__host__ __device__ inline int oz_kpad(int k) { return ((2 * k + kOzKBlock - 1) / kOzKBlock) * kOzKBlock; }
+__host__ __device__ inline int oz_rpad(int m) { return ((m + kOzTileM - 1) / kOzTileM) * kOzTileM; }
+__host__ __device__ inline int oz_npad(int n) { return ((2 * n + kOzTileN - 1) / kOzTileN) * kOzTileN; }
+
+// Staging of one set of jobs: digit planes, exponents and their tensor maps.
+struct OzPlanes {
+    int8_t* a = nullptr;   // [jobs][kOzSlices][rpad][kpad]
+    int8_t* b = nullptr;   // [jobs][kOzSlices][npad][kpad]
+    int* ea = nullptr;     // [jobs][rpad]
+    int* eb = nullptr;     // [jobs][npad / 2]
+    int rpad = 0, npad = 0, kpad = 0, jobs = 0;
+    CUtensorMap map_a{}, map_b{};
+};
+// Bytes of the staging for `jobs` problems up to rpad x kpad times kpad x npad.
+size_t oz_planes_bytes(int jobs, int rpad, int npad, int kpad);
+// Carve the staging out of `base` (oz_planes_bytes long, 256-byte aligned)
+// and encode its tensor maps; false if the driver refuses a map.
+bool oz_planes_init(OzPlanes* P, void* base, int jobs, int rpad, int npad, int kpad);
+
+// Stage the merge operands of every job of a wave (grid: a_blocks + N tiles
+// of 8 values of b, jobs); a_blocks blocks take 8 rows of A each in turn.
+__global__ void oz_prep_merge_kernel(const SplitJob* jobs, const SplitState* st, DeviceMps mps, OzPlanes P,
+                                     int a_blocks);
+cudaError_t launch_oz_merge(const OzPlanes& P, dim3 grid, cudaStream_t s, const TcMergeArgs& args, int* status);
+// Plain problems (wqc_tc_zgemm_int8).
+__global__ void oz_prep_plain_kernel(const double2* A, const double2* B, int m, int n, int k, OzPlanes P,
+                                     int a_blocks);
+cudaError_t launch_oz_plain(const OzPlanes& P, dim3 grid, cudaStream_t s, const TcPlainArgs& args, int* status);
+
 }  // namespace wqc

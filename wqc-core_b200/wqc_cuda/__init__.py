@@ -35,6 +35,8 @@ ERR_INVALID_QUBIT_COUNT = 10
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1
 PRECISION_TF32X3 = 2
+MERGE_FFMA = 0
+MERGE_TC_INT8 = 1
 OVERLAP_ENV_LIMIT = 256  # mps.rs:1443-1448 (the STARK witness limit)
 SPLIT_RULE_REFERENCE = 0
 SPLIT_RULE_EXACT = 1
@@ -55,7 +57,7 @@ EXPORTS = (
     "wqc_exact_create", "wqc_exact_destroy", "wqc_exact_validate", "wqc_exact_measured_peak", "wqc_exact_contract",
     "wqc_exact_cancel", "wqc_exact_last_stats", "wqc_exact_set_tile_bits",
     "wqc_network_create", "wqc_network_destroy", "wqc_network_validate", "wqc_network_measured_peak",
-    "wqc_network_contract", "wqc_network_cancel", "wqc_network_last_stats", "wqc_tc_zgemm",
+    "wqc_network_contract", "wqc_network_cancel", "wqc_network_last_stats", "wqc_tc_zgemm", "wqc_tc_zgemm_int8", "wqc_mps_set_merge",
 )
 
 KERNEL_KINDS = ("jacobi_svd", "merge_gate", "range_finder", "one_qubit", "cut_absorb")
@@ -121,6 +123,7 @@ def lib():
         L.wqc_mps_apply_2q_routed.argtypes = [P, U32, U32, D]
         L.wqc_mps_apply_layer.argtypes = [P, P, U32]
         L.wqc_mps_set_split_rule.argtypes = [P, ctypes.c_int32]
+        L.wqc_mps_set_merge.argtypes = [P, ctypes.c_int32]
         L.wqc_mps_synchronize.argtypes = [P]
         L.wqc_mps_cancel.argtypes = [P]
         L.wqc_mps_cancel.restype = None
@@ -345,6 +348,11 @@ class CudaMps:
     # --- reads ---------------------------------------------------------------
     def set_split_rule(self, rule: int) -> None:
         _check(lib().wqc_mps_set_split_rule(self._h, rule))
+
+    def set_merge(self, merge: int) -> None:
+        """MERGE_FFMA (FP64 FMA tiles) or MERGE_TC_INT8 (int8 digit slices on
+        the tcgen05 tensor cores, FP64-level) for the merges that follow."""
+        _check(lib().wqc_mps_set_merge(self._h, merge))
 
     def synchronize(self) -> None:
         _check(lib().wqc_mps_synchronize(self._h))
@@ -639,9 +647,12 @@ CZ4 = _mat4([((0, 0, 0, 0), 1), ((0, 1, 0, 1), 1), ((1, 0, 1, 0), 1), ((1, 1, 1,
 SWAP4 = _mat4([((0, 0, 0, 0), 1), ((0, 1, 1, 0), 1), ((1, 0, 0, 1), 1), ((1, 1, 1, 1), 1)])
 
 
-def run(n: int, chi: int, gates: np.ndarray, ctx: Context | None = None, rule: int = SPLIT_RULE_REFERENCE) -> CudaMps:
+def run(n: int, chi: int, gates: np.ndarray, ctx: Context | None = None, rule: int = SPLIT_RULE_REFERENCE,
+        merge: int = MERGE_FFMA) -> CudaMps:
     m = CudaMps(n, chi, ctx=ctx)
     m.set_split_rule(rule)
+    if merge != MERGE_FFMA:
+        m.set_merge(merge)
     m.apply_gates(gates)
     return m
 
