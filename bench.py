@@ -269,12 +269,12 @@ def measured_tf32_peak(torch) -> float:
     return best
 
 
-def whole_circuit_profile(W, torch, ctx, w, rule, precision: int, flush, merge: int = 0) -> tuple[float, int, dict]:
+def whole_circuit_profile(W, torch, ctx, w, rule, precision: int, flush, merge=None) -> tuple[float, int, dict]:
     """One untimed warm-up pass and one timed pass of the whole circuit from
     |0...0> with per-kernel events: (ms, splits, kernel milliseconds)."""
     m = W.CudaMps(w.n, w.chi, ctx=ctx, precision=precision)
     m.set_split_rule(rule)
-    if merge:
+    if merge is not None:
         m.set_merge(merge)
     stream = torch.cuda.ExternalStream(m.stream())
     ms = 0.0
@@ -351,16 +351,18 @@ def tensor_core_leg(W, torch, ctx, w, rule, flush, gemm_only: bool = False) -> d
     }
     if gemm_only:
         return out
-    fp64_ms, fp64_splits, fp64_k = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_FP64, flush)
+    fp64_ms, fp64_splits, fp64_k = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_FP64, flush,
+                                                         merge=W.MERGE_FFMA)
     i8_ms, i8_splits, i8_k = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_FP64, flush,
                                                    merge=W.MERGE_TC_INT8)
     out["int8_merge"] = {
-        "form": "plain FP64 form with every merge from int8 digit slices on the tensor cores (WQC_MERGE_TC_INT8)",
+        "form": "plain FP64 form with every merge from int8 digit slices on the tensor cores (WQC_MERGE_TC_INT8, "
+                "the single-state default)",
         "value": i8_splits / (i8_ms * 1e-3),
-        "fp64_value": fp64_splits / (fp64_ms * 1e-3),
+        "ffma_value": fp64_splits / (fp64_ms * 1e-3),
         "unit": UNIT,
         "merge_ms": i8_k["merge_gate"],
-        "fp64_merge_ms": fp64_k["merge_gate"],
+        "ffma_merge_ms": fp64_k["merge_gate"],
     }
     tc_ms, tc_splits, tc_k = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_TF32X3, flush)
     w0 = C.config0()
@@ -381,6 +383,7 @@ def tensor_core_leg(W, torch, ctx, w, rule, flush, gemm_only: bool = False) -> d
         "unit": UNIT,
         "merge_ms": tc_k["merge_gate"],
         "fp64_merge_ms": fp64_k["merge_gate"],
+        "fp64_merge": "FP64 FMA tiles",
         "splits": tc_splits,
         "fp64_splits": fp64_splits,
         "amp_rel_err_vs_fp64": abs(amps[1] - amps[0]) / abs(amps[0]),
@@ -1207,7 +1210,8 @@ def run_cuda(args) -> None:
             "vs_baseline": None,
             "dtype": "f64",
             "data": "synthetic (seeded generator, same circuit every run)",
-            "config": workload_config(w, args.split_rule, g0, windows),
+            "config": dict(workload_config(w, args.split_rule, g0, windows),
+                           merge="int8 digit slices on the tcgen05 tensor cores, FP64-level (the state default)"),
             "e2e": {
                 "value": e2e,
                 "unit": UNIT,

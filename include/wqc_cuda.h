@@ -57,8 +57,9 @@ enum wqc_precision {
                                V is then made orthonormal to FP64 rounding (two
                                Newton-Schulz steps) and X V formed in FP64, and FP64
                                sweeps finish from there (quadratic convergence: a few
-                               sweeps).  Sites, merges, range finder, sort and cut stay
-                               FP64, so results carry FP64-level error. */
+                               sweeps).  Sites, range finder, sort and cut stay FP64 and
+                               merges FP64-level (wqc_mps_set_merge), so results carry
+                               FP64-level error. */
     WQC_PRECISION_TF32X3 = 2 /* tensor-core form: the precision form's Jacobi, with every
                                two-site merge (theta = L R and the 4x4 gate) on the tcgen05
                                tensor cores: operands split into TF32 hi and lo parts, the
@@ -199,14 +200,18 @@ WQC_API wqc_status wqc_mps_set_split_rule(wqc_mps* mps, int32_t rule);
 
 /* How the state performs its merges (merge_two_site_tensors / cpu_merge,
  * mps.rs:484-514, 812-831, with the 4x4 of mps.rs:833-866; applies to merges
- * enqueued afterwards).  FFMA (the default): tiled FP64 FMA.  TC_INT8: on the
+ * enqueued afterwards).  FFMA: tiled FP64 FMA (the default of batches).
+ * TC_INT8 (the default of states from wqc_mps_create, except the tensor-core
+ * form): on the
  * tcgen05 tensor cores from int8 digit slices (the Ozaki scheme): each row of
  * L and each column of R scaled by a power of two, cut into 9 signed 7-bit
  * digits (63 bits), the digit products exact in int32 in tensor memory and
  * summed in FP64 -- FP64-level results (the dropped slice products lie below
- * 2^-60 of the row and column maxima) from the integer tensor pipe.  The first TC_INT8 call
- * allocates the digit planes of every split slot (WQC_ERR_OOM if they do not
- * fit).  Not for the tensor-core form, whose merges are its TF32 path. */
+ * 2^-60 of the row and column maxima) from the integer tensor pipe.  The
+ * digit planes of every split slot are allocated with the state when
+ * TC_INT8 is its default, else by the first TC_INT8 call (WQC_ERR_OOM if
+ * they do not fit).  Not for the tensor-core form, whose merges are its TF32
+ * path. */
 enum wqc_merge { WQC_MERGE_FFMA = 0, WQC_MERGE_TC_INT8 = 1 };
 WQC_API wqc_status wqc_mps_set_merge(wqc_mps* mps, int32_t merge);
 

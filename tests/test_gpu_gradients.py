@@ -33,6 +33,7 @@ def test_batch_expectations_equal_single_state_ones(cuda_ctx):
     got = b.expectations(labels, coeffs)
     for s, g in enumerate((gates, gates[: len(gates) // 2])):
         m = W.CudaMps(8, 16, ctx=cuda_ctx)
+        m.set_merge(W.MERGE_FFMA)  # the batch's merges: bit for bit only on the same merge path
         m.apply_gates(g)
         assert got[s] == m.expectation(labels, coeffs)
 

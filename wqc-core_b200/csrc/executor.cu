@@ -306,6 +306,40 @@ struct wqc_mps {
 
 namespace {
 
+wqc_status dmalloc(wqc_mps* m, void** p, size_t bytes);
+
+// Digit planes of the int8-slice merges for every split slot of the state.
+size_t oz_state_bytes(const wqc_mps* m) {
+    return oz_planes_bytes(m->nslots, oz_rpad(2 * m->chi), oz_npad(2 * m->chi), oz_kpad(m->chi));
+}
+
+}  // namespace
+
+// Merges from int8 digit slices from now on: allocate the digit planes of
+// every split slot the first time (WQC_ERR_OOM if they do not fit).
+static wqc_status oz_enable(wqc_mps* m) {
+    if (!m->oz_pool) {
+        const int rpad = oz_rpad(2 * m->chi), npad = oz_npad(2 * m->chi), kpad = oz_kpad(m->chi);
+        const size_t bytes = oz_state_bytes(m);
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return fail(WQC_ERR_CUDA, "cudaMemGetInfo");
+        if (bytes > fr) return fail_oom(bytes, fr);
+        void* p = nullptr;
+        if (wqc_status st = dmalloc(m, &p, bytes)) return st;
+        if (!oz_planes_init(&m->oz_planes, p, m->nslots, rpad, npad, kpad)) {
+            cudaFree(p);
+            m->bytes_now -= bytes;
+            return fail(WQC_ERR_CUDA, "cuTensorMapEncodeTiled refused the merge digit planes");
+        }
+        m->oz_pool = p;
+        m->oz_bytes = bytes;
+    }
+    m->oz = true;
+    return WQC_OK;
+}
+
+namespace {
+
 wqc_status dmalloc(wqc_mps* m, void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
@@ -1248,7 +1282,8 @@ uint64_t wqc_mps_workspace_bytes(uint32_t n, uint32_t chi) {
 }
 
 static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, const std::vector<int>& chis,
-                               int32_t precision, bool reject, int nslots_req, wqc_mps** out) {
+                               int32_t precision, bool reject, int nslots_req, wqc_mps** out,
+                               bool single_state = false) {
     if (!ctx || !out) return fail(WQC_ERR_INVALID, "null argument");
     if (ns.empty()) return fail(WQC_ERR_INVALID, "no slices");
     long total_n = 0;
@@ -1352,7 +1387,13 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
         tc_a_bytes = size_t(2) * m->nslots * m->tc_rpad * m->tc_kpad * sizeof(float);
         tc_b_bytes = size_t(2) * m->nslots * m->tc_npad * m->tc_kpad * sizeof(float);
     }
-    const uint64_t need = site_bytes + uint64_t(slot_pool_bytes) + tc_a_bytes + tc_b_bytes;
+    // States from wqc_mps_create merge from int8 digit slices on the tensor
+    // cores by default (FP64-level, wqc_mps_set_merge); batches (a batch of
+    // one included) keep FMA merges, whose many slots would each need digit
+    // planes.
+    const bool oz_default = single_state && !m->tc;
+    const uint64_t need = site_bytes + uint64_t(slot_pool_bytes) + tc_a_bytes + tc_b_bytes +
+                          (oz_default ? oz_state_bytes(m) : 0);
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "cudaMemGetInfo"));
     if (need > fr) return bail(fail_oom(need, fr));
@@ -1387,6 +1428,8 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
     m->d_small = static_cast<double2*>(p);
     m->d_counters = reinterpret_cast<unsigned long long*>(m->d_small + small - 4);
     if (cudaMemset(m->d_small, 0, small * sizeof(double2)) != cudaSuccess) return bail(fail(WQC_ERR_CUDA, "memset"));
+    if (oz_default)
+        if (wqc_status st = oz_enable(m)) return bail(st);
     if (ns.size() == 1) {  // the trace feeders' environment cache (single states)
         const size_t env_bytes = 2 * size_t(n) * chi_cap * sizeof(double2) + size_t(n) * 2 * sizeof(double2) +
                                  size_t(n) * sizeof(int);
@@ -1461,7 +1504,7 @@ static wqc_status create_state(wqc_cuda_ctx* ctx, const std::vector<int>& ns, co
 
 wqc_status wqc_mps_create(wqc_cuda_ctx* ctx, uint32_t n, uint32_t chi, int32_t precision, uint8_t reject,
                           wqc_mps** out) {
-    return create_state(ctx, {int(n)}, {int(chi)}, precision, reject != 0, 0, out);
+    return create_state(ctx, {int(n)}, {int(chi)}, precision, reject != 0, 0, out, true);
 }
 
 wqc_status wqc_batch_create(wqc_cuda_ctx* ctx, uint32_t count, const uint32_t* qubit_counts,
@@ -1746,22 +1789,8 @@ wqc_status wqc_mps_set_merge(wqc_mps* m, int32_t merge) {
     if (m->tc) return fail(WQC_ERR_INVALID, "the tensor-core form merges on its own TF32 path");
     CUDA_TRY(cudaSetDevice(m->ctx->device));
     CUDA_TRY(cudaStreamSynchronize(m->stream));  // no enqueued merge still reads the planes
-    if (merge == WQC_MERGE_TC_INT8 && !m->oz_pool) {
-        const int rpad = oz_rpad(2 * m->chi), npad = oz_npad(2 * m->chi), kpad = oz_kpad(m->chi);
-        const size_t bytes = oz_planes_bytes(m->nslots, rpad, npad, kpad);
-        size_t fr = 0, tot = 0;
-        CUDA_TRY(cudaMemGetInfo(&fr, &tot));
-        if (bytes > fr) return fail_oom(bytes, fr);
-        void* p = nullptr;
-        if (wqc_status st = dmalloc(m, &p, bytes)) return st;
-        if (!oz_planes_init(&m->oz_planes, p, m->nslots, rpad, npad, kpad)) {
-            dfree(m, p, bytes);
-            return fail(WQC_ERR_CUDA, "cuTensorMapEncodeTiled refused the merge digit planes");
-        }
-        m->oz_pool = p;
-        m->oz_bytes = bytes;
-    }
-    m->oz = merge == WQC_MERGE_TC_INT8;
+    if (merge == WQC_MERGE_TC_INT8) return oz_enable(m);
+    m->oz = false;
     return WQC_OK;
 }
 

@@ -48,16 +48,25 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
+// Exponent of a row or column holding a NaN or an infinity: no finite
+// exponent comes near it, and the epilogue turns its entries into NaN, so a
+// non-finite site still reaches the SVD's non-finite check.
+constexpr int kOzNonFinite = 1 << 20;
+
 // Exponent e with max * 2^-e in [1/2, 1) (0 for max = 0).
-__device__ __forceinline__ int scale_exponent(double mx) {
+__device__ __forceinline__ int scale_exponent(double mx, bool nonfinite) {
+    if (nonfinite) return kOzNonFinite;
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);
     return e;
 }
 
-// The kOzSlices digits of x * 2^-e (|x| 2^-e < 1), by truncation: exact.
+__device__ __forceinline__ bool nonfinite2(double2 v) { return !(isfinite(v.x) && isfinite(v.y)); }
+
+// The kOzSlices digits of x * 2^-e (|x| 2^-e < 1), by truncation: exact
+// (all zero for a non-finite row or column).
 __device__ __forceinline__ void digits(double x, int e, int* d) {
-    double v = ldexp(x, -e);
+    double v = e == kOzNonFinite ? 0.0 : ldexp(x, -e);
 #pragma unroll
     for (int p = 0; p < kOzSlices; ++p) {
         v *= 128.0;
@@ -109,11 +118,13 @@ __device__ void oz_stage(const OzSource& src, const OzPlanes& P, int j, int a_bl
         int8_t* A = P.a + size_t(j) * kOzSlices * a_plane;
         for (int r = blockIdx.x * (blockDim.x / 32) + warp; r < mrows; r += a_blocks * (blockDim.x / 32)) {
             double mx = 0.0;
+            bool bad = false;
             for (int g = lane; g < gpad; g += 32) {
                 const double2 v = src.a(r, g);
                 mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+                bad |= nonfinite2(v);
             }
-            const int e = scale_exponent(warp_max(mx));
+            const int e = scale_exponent(warp_max(mx), __any_sync(0xffffffffu, bad));
             if (lane == 0) P.ea[size_t(j) * P.rpad + r] = e;
             for (int g = lane; g < gpad; g += 32) {
                 const double2 v = src.a(r, g);
@@ -133,22 +144,30 @@ __device__ void oz_stage(const OzSource& src, const OzPlanes& P, int j, int a_bl
     if (nt >= src.ntiles()) return;  // uniform over the block
     constexpr int kSub = 256 / kOzTileC;  // threads splitting g per column in the maxima pass
     __shared__ double colmax[kSub][kOzTileC];
+    __shared__ int colbad[kSub][kOzTileC];
     __shared__ int fexp[kOzTileC];
     __shared__ double2 tile[kOzKBlock / 2][kOzTileC + 1];  // [g - g0][q]
     {
         const int q = tid % kOzTileC, gsub = tid / kOzTileC;
         double mx = 0.0;
+        bool bad = false;
         for (int g = gsub; g < src.k; g += kSub) {
             const double2 v = src.b(g, nt, q);
             mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+            bad |= nonfinite2(v);
         }
         colmax[gsub][q] = mx;
+        colbad[gsub][q] = bad ? 1 : 0;
     }
     __syncthreads();
     if (tid < kOzTileC) {
         double mx = 0.0;
-        for (int w = 0; w < kSub; ++w) mx = fmax(mx, colmax[w][tid]);
-        const int f = scale_exponent(mx);
+        bool bad = false;
+        for (int w = 0; w < kSub; ++w) {
+            mx = fmax(mx, colmax[w][tid]);
+            bad |= colbad[w][tid] != 0;
+        }
+        const int f = scale_exponent(mx, bad);
         fexp[tid] = f;
         P.eb[size_t(j) * (P.npad / 2) + nt * kOzTileC + tid] = f;
     }
@@ -303,6 +322,11 @@ __global__ void __launch_bounds__(kOzThreads, 1)
         const int row = row0 + warp * 32 + lane;
         const int er = row < rows ? ea_all[size_t(j) * rpad + row] : 0;
         const int* eb = eb_all + size_t(j) * (npad / 2) + nt * kOzTileC;
+        // 2^(e_r + f_c - 14) x, or NaN where the row or column held a non-finite value
+        auto scaled = [&](double x, int f) {
+            return (er == kOzNonFinite || f == kOzNonFinite) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                             : ldexp(x, er + f - 14);
+        };
         // sum_d acc_d 2^-7d over 16 columns from `col`, by Horner from the last d
         auto combine = [&](int col, double* v) {
             uint32_t r[16];
@@ -334,9 +358,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
             combine(16, v1);
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                const int s0 = er + eb[i] - 14, s1 = er + eb[8 + i] - 14;
-                const double2 o0 = cmake(ldexp(v0[2 * i], s0), ldexp(v0[2 * i + 1], s0));
-                const double2 o1 = cmake(ldexp(v1[2 * i], s1), ldexp(v1[2 * i + 1], s1));
+                const int f0 = eb[i], f1 = eb[8 + i];
+                const double2 o0 = cmake(scaled(v0[2 * i], f0), scaled(v0[2 * i + 1], f0));
+                const double2 o1 = cmake(scaled(v1[2 * i], f1), scaled(v1[2 * i + 1], f1));
                 const double2 p0 = cmake(__shfl_xor_sync(0xffffffffu, o0.x, 1), __shfl_xor_sync(0xffffffffu, o0.y, 1));
                 const double2 p1 = cmake(__shfl_xor_sync(0xffffffffu, o1.x, 1), __shfl_xor_sync(0xffffffffu, o1.y, 1));
                 const double2 t00 = s_own ? p0 : o0, t01 = s_own ? p1 : o1;
@@ -363,9 +387,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
                     const int q = 8 * c + i, col = nt * kOzTileC + q;
-                    const int sc = er + eb[q] - 14;
                     if (row_ok && col < args.n)
-                        args.C[size_t(row) * args.ldc + col] = cmake(ldexp(v[2 * i], sc), ldexp(v[2 * i + 1], sc));
+                        args.C[size_t(row) * args.ldc + col] = cmake(scaled(v[2 * i], eb[q]), scaled(v[2 * i + 1], eb[q]));
                 }
             }
         }

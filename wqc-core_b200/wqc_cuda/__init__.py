@@ -648,10 +648,12 @@ SWAP4 = _mat4([((0, 0, 0, 0), 1), ((0, 1, 1, 0), 1), ((1, 0, 0, 1), 1), ((1, 1, 
 
 
 def run(n: int, chi: int, gates: np.ndarray, ctx: Context | None = None, rule: int = SPLIT_RULE_REFERENCE,
-        merge: int = MERGE_FFMA) -> CudaMps:
+        merge: int | None = None) -> CudaMps:
+    """A state with the gates applied; `merge` (MERGE_*) overrides the
+    default merge (int8 digit slices on the tensor cores for single states)."""
     m = CudaMps(n, chi, ctx=ctx)
     m.set_split_rule(rule)
-    if merge != MERGE_FFMA:
+    if merge is not None:
         m.set_merge(merge)
     m.apply_gates(gates)
     return m
