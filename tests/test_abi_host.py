@@ -64,6 +64,7 @@ def test_bindings_reach_the_library_with_a_null_state():
         lambda: fake.sample([0, 2], 3, 7),
         lambda: fake.sample_counts([(0, 0)], 1, 3, 7),
         lambda: fake.expectation(["ZZZZ"], [1.0]),
+        lambda: fake.set_merge(W.MERGE_TC_INT8),
     ]
     for call in calls:
         with pytest.raises(W.WqcCudaError) as e:
@@ -75,6 +76,25 @@ def test_bindings_reach_the_library_with_a_null_state():
     with pytest.raises(W.WqcCudaError) as e:
         fake.sample_counts([(0, 2)], 2, 3, 7)
     assert e.value.code == W.ERR_INVALID and "classical bit index 2" in str(e.value)
+
+
+def test_tensor_core_gemms_reject_a_null_context_before_device_work():
+    """wqc_tc_zgemm and wqc_tc_zgemm_int8 check their arguments on the host:
+    a null context is refused without touching a device."""
+    import numpy as np
+
+    from wqc_cuda import tc as T
+
+    class NoCtx:
+        _h = None
+
+    a, b = np.ones((3, 2), dtype=complex), np.ones((2, 4), dtype=complex)
+    for form in ("tf32x3", "int8"):
+        with pytest.raises(W.WqcCudaError) as e:
+            T.zgemm(a, b, ctx=NoCtx(), form=form)
+        assert e.value.code == W.ERR_INVALID and "null" in str(e.value)
+    with pytest.raises(ValueError):
+        T.zgemm(a, b, ctx=NoCtx(), form="fp16")
 
 
 def test_workspace_bytes_matches_reference_formula():
