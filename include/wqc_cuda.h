@@ -580,7 +580,13 @@ WQC_API wqc_status wqc_tc_zgemm(wqc_cuda_ctx* ctx, uint32_t m, uint32_t n, uint3
                                 const double* b, double* c, uint32_t reps, double* kernel_ms);
 
 /* The same product from int8 digit slices on the tensor cores (kind::i8,
- * the scheme of WQC_MERGE_TC_INT8): FP64-level results.  m, n in 1..8192,
+ * the scheme of WQC_MERGE_TC_INT8).  Each entry lies within 2^-49 2k of the
+ * product of its row's largest |re|, |im| in A and its column's in B: FP64
+ * level wherever the terms of a dot product are not far below those maxima.
+ * Where a row's large entries meet a column's small ones along k, the result
+ * is small against the maxima and loses relative accuracy (FP64 FMA would
+ * not); the merge's operands, L = U sqrt(S) and R = sqrt(S) V^H, shrink
+ * together along k and keep FP64-level relative error.  m, n in 1..8192,
  * k in 1..4096 (the int32 accumulators' bound). */
 WQC_API wqc_status wqc_tc_zgemm_int8(wqc_cuda_ctx* ctx, uint32_t m, uint32_t n, uint32_t k, const double* a,
                                      const double* b, double* c, uint32_t reps, double* kernel_ms);
