@@ -9,10 +9,8 @@
 // waits (bounded) for what it issued and frees its tensor memory.
 #include <cudaTypedefs.h>
 
-#include <cstring>
 #include <mutex>
 #include <string>
-#include <vector>
 
 #include "../../include/wqc_cuda.h"
 #include "split_kernels.cuh"
