@@ -1111,6 +1111,15 @@ def run_cuda(args) -> None:
     w = workload(args.workload, args.depth)
     g0, windows = timed_windows(w, SATURATED_LAYERS.get(args.workload, 0), args.steps)
     rule = W.SPLIT_RULE_EXACT if args.split_rule == "exact" else W.SPLIT_RULE_REFERENCE
+    if args.tensor_core_only == "merge":
+        ctx = W.Context(local)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+        ms, splits, kms = whole_circuit_profile(W, torch, ctx, w, rule, W.PRECISION_FP64, flush,
+                                                merge=W.MERGE_TC_INT8)
+        if rank == 0:
+            print(json.dumps({"int8_merge_pass": {"ms": ms, "splits": splits, "merge_ms": kms["merge_gate"]}}),
+                  flush=True)
+        return
     if args.tensor_core_only:
         ctx = W.Context(local)
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -1330,8 +1339,9 @@ def main():
                     help="skip the precision-form (complex64 Jacobi) leg run after the timed steps")
     ap.add_argument("--no-tensor-core-leg", dest="tensor_core_leg", action="store_false",
                     help="skip the tcgen05 GEMM and the tensor-core form (WQC_PRECISION_TF32X3)")
-    ap.add_argument("--tensor-core-only", choices=("gemm", "form"), default=None,
-                    help="run only the tensor-core leg (gemm: the 4096^3 GEMM alone) and print it (for profiling)")
+    ap.add_argument("--tensor-core-only", choices=("gemm", "form", "merge"), default=None,
+                    help="run only the tensor-core leg (gemm: the 4096^3 GEMMs alone; merge: one pass of the "
+                         "circuit with the int8-slice merges) and print it (for profiling)")
     ap.add_argument("--batch-slices", type=int, default=512,
                     help="slices of the batching-form leg run once after the timed steps (0 = skip)")
     args = ap.parse_args()
