@@ -935,8 +935,9 @@ wqc_status launch_plan(wqc_mps* m, Plan& plan) {
                 // rows of L by warps, N tiles of R (8 values of b) by blocks
                 const int a_blocks = std::max(1, (w.max_rows + 7) / 8);
                 const int ntiles = (w.max_dr + 7) / 8;
-                oz_prep_merge_kernel<<<dim3(a_blocks + ntiles, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->dev,
-                                                                                         m->oz_planes, a_blocks);
+                const int b_blocks = ntiles * (m->oz_planes.kpad / kOzKBlock);
+                oz_prep_merge_kernel<<<dim3(a_blocks + b_blocks, nj), 256, 0, m->stream>>>(d_jobs, m->d_state, m->dev,
+                                                                                           m->oz_planes, a_blocks);
                 count_launch(m, 1);
                 const dim3 g(ntiles, (w.max_rows + kOzTileM - 1) / kOzTileM, nj);
                 CUDA_TRY(launch_oz_merge(m->oz_planes, g, m->stream, TcMergeArgs{d_jobs, m->d_state, m->d_slots},

@@ -126,7 +126,8 @@ size_t oz_planes_bytes(int jobs, int rpad, int npad, int kpad);
 bool oz_planes_init(OzPlanes* P, void* base, int jobs, int rpad, int npad, int kpad);
 
 // Stage the merge operands of every job of a wave (grid: a_blocks + N tiles
-// of 8 values of b, jobs); a_blocks blocks take 8 rows of A each in turn.
+// of 8 values of b x kpad / 64 K chunks, jobs); a_blocks blocks take 8 rows
+// of A each in turn.
 __global__ void oz_prep_merge_kernel(const SplitJob* jobs, const SplitState* st, DeviceMps mps, OzPlanes P,
                                      int a_blocks);
 cudaError_t launch_oz_merge(const OzPlanes& P, dim3 grid, cudaStream_t s, const TcMergeArgs& args, int* status);

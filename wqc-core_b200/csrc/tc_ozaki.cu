@@ -106,9 +106,11 @@ struct OzSource {
 };
 
 // Stage one job: blocks [0, a_blocks) take rows of A (one warp per row, 8
-// rows a block in turn); block a_blocks + nt takes N tile nt of B (column
-// maxima over all K first, then 32 values of g at a time through shared
-// memory, written as 4-byte runs of K per plane row).
+// rows a block in turn); block a_blocks + nt * (kpad / 64) + kc takes K
+// chunk kc (32 values of g) of N tile nt of B: the tile's column maxima over
+// all K first (every chunk's block computes them: R is small and in L2),
+// then its chunk through shared memory, written as 4-byte runs of K per
+// plane row.
 __device__ void oz_stage(const OzSource& src, const OzPlanes& P, int j, int a_blocks) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int kx_end = min(oz_kpad(src.k), P.kpad);
@@ -140,8 +142,9 @@ __device__ void oz_stage(const OzSource& src, const OzPlanes& P, int j, int a_bl
         }
         return;
     }
-    const int nt = int(blockIdx.x) - a_blocks;
-    if (nt >= src.ntiles()) return;  // uniform over the block
+    const int kchunks = P.kpad / kOzKBlock;
+    const int nt = (int(blockIdx.x) - a_blocks) / kchunks, kc = (int(blockIdx.x) - a_blocks) % kchunks;
+    if (nt >= src.ntiles() || kc * kOzKBlock >= kx_end) return;  // uniform over the block
     constexpr int kSub = 256 / kOzTileC;  // threads splitting g per column in the maxima pass
     __shared__ double colmax[kSub][kOzTileC];
     __shared__ int colbad[kSub][kOzTileC];
@@ -169,11 +172,11 @@ __device__ void oz_stage(const OzSource& src, const OzPlanes& P, int j, int a_bl
         }
         const int f = scale_exponent(mx, bad);
         fexp[tid] = f;
-        P.eb[size_t(j) * (P.npad / 2) + nt * kOzTileC + tid] = f;
+        if (kc == 0) P.eb[size_t(j) * (P.npad / 2) + nt * kOzTileC + tid] = f;
     }
     __syncthreads();
     int8_t* B = P.b + size_t(j) * kOzSlices * b_plane;
-    for (int kc = 0; kc * kOzKBlock < kx_end; ++kc) {
+    {
         const int g0 = kc * (kOzKBlock / 2);
         for (int e = tid; e < (kOzKBlock / 2) * kOzTileC; e += blockDim.x)
             tile[e / kOzTileC][e % kOzTileC] = src.b(g0 + e / kOzTileC, nt, e % kOzTileC);
@@ -526,7 +529,7 @@ WQC_API wqc_status wqc_tc_zgemm_int8(wqc_cuda_ctx* ctx, uint32_t m, uint32_t n, 
         return cuda_fail("cudaMemcpyAsync(int8-slice GEMM operands)", e);
     const int a_blocks = std::min(1184, (rpad + 7) / 8);
     const int ntiles = (int(n) + kOzTileC - 1) / kOzTileC;
-    oz_prep_plain_kernel<<<a_blocks + ntiles, 256, 0, s>>>(static_cast<const double2*>(dA),
+    oz_prep_plain_kernel<<<a_blocks + ntiles * (kpad / kOzKBlock), 256, 0, s>>>(static_cast<const double2*>(dA),
                                                            static_cast<const double2*>(dB), int(m), int(n), int(k), P,
                                                            a_blocks);
     if ((e = cudaGetLastError())) return cuda_fail("int8-slice GEMM staging", e);
